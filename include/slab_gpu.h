@@ -1,0 +1,186 @@
+/* slab_gpu.h -- C ABI of libslab_gpu.so, the B200 (sm_100a) engine for the
+ * Slab-Pro depth-averaged material point method (MPM) time step.
+ *
+ * The reference (ALMO-SLF-ETH/Slab-Pro) has no plugin or FFI interface: its
+ * boundary is the C++ class Simulation<T,TV2> (src/simulation.hpp:27-354),
+ * whose simulate() (src/simulation.cpp:484-522) runs the step loop on the
+ * host. This header is the interface that loop is replaced by. Each entry
+ * point below names the reference code it stands in for. The C++ class in
+ * slab-pro_b200/csrc/simulation.hpp keeps the reference's public Simulation
+ * API and calls these functions from its simulate().
+ *
+ * Conventions
+ *  - Plain C types only; every pointer argument is a host pointer unless the
+ *    name says otherwise. The caller owns host buffers, a context owns its
+ *    device memory.
+ *  - Arrays follow the reference layouts (src/data_arrays.hpp:22-98):
+ *    particle positions and velocities are interleaved (x0,y0,x1,y1,...) like
+ *    std::vector<Eigen::Vector2d>; scalar particle fields are separate arrays;
+ *    grid/terrain fields are flattened i*Ny + j (src/tools.hpp:172-174), with
+ *    node (i,j) at (i*dx, j*dx).
+ *  - Every function returns a slab_status. On error, slab_last_error() gives a
+ *    message. The C++ wrapper rethrows non-OK codes as std::runtime_error,
+ *    matching how the reference reports errors (src/main.cpp:52-55).
+ *  - One context per host thread; contexts are not internally locked.
+ */
+#ifndef SLAB_GPU_H
+#define SLAB_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum slab_status {
+    SLAB_OK = 0,
+    SLAB_E_ARG = 1,       /* invalid argument or size */
+    SLAB_E_CUDA = 2,      /* CUDA runtime error (message has details) */
+    SLAB_E_OOM = 3,       /* device allocation failed / capacity exceeded */
+    SLAB_E_DOMAIN = 4,    /* a particle's 3x3 stencil left the terrain */
+    SLAB_E_NONFINITE = 5, /* NaN/Inf in particle or grid state */
+    SLAB_E_TIMEOUT = 6,   /* a bounded device-side wait gave up */
+    SLAB_E_STATE = 7,     /* call out of order (e.g. advance before upload) */
+    SLAB_E_NOTFOUND = 8   /* unknown scenario / request id */
+} slab_status;
+
+/* Basal friction laws, src/tools.hpp:37,62-84 */
+typedef enum slab_friction_type { SLAB_COULOMB = 0, SLAB_VOELLMY = 1, SLAB_MU_I = 2 } slab_friction_type;
+
+/* Arithmetic of the step loop.
+ *  FP64_PLAIN: state and arithmetic in FP64, particles in upload order,
+ *              atomicAdd(double) P2G scatter. The drop-in twin of the
+ *              reference loop and the comparison baseline.
+ *  FP32_SPLIT: positions as int32 cell index + FP32 in-cell offset, FP32
+ *              particle/grid state, deterministic atomic-free P2G over
+ *              cell-sorted particles in sparse 16x16-cell tiles. FP64 only for
+ *              terrain metric terms, conservation sums, time and dt. */
+typedef enum slab_precision { SLAB_FP64_PLAIN = 0, SLAB_FP32_SPLIT = 1 } slab_precision;
+
+/* Friction parameters, src/tools.hpp:62-84 (struct Friction). */
+typedef struct slab_friction {
+    int32_t type; /* slab_friction_type */
+    int32_t pad_;
+    double coulomb_mu;
+    double voellmy_mu, voellmy_xi;
+    double mu_1, mu_2, I0, d, phi;
+} slab_friction;
+
+/* Simulation parameters read by Simulation::loadFromJSON
+ * (src/simulation.cpp:118-208), plus the engine's precision. */
+typedef struct slab_params {
+    double gravity, rho;
+    double C_cfl, dt_max, flip_ratio;
+    double output_dt, total_time;
+    slab_friction friction;
+    int32_t precision; /* slab_precision */
+    int32_t pad_;
+} slab_params;
+
+/* The terrain Grid of the reference (src/data_arrays.hpp:49-93,
+ * src/complex_terrain.cpp:31-65): Nx x Ny nodes at spacing dx; the origin
+ * offsets only matter for georeferenced output. */
+typedef struct slab_terrain_desc {
+    int32_t Nx, Ny;
+    double dx;
+    double xllcorner, yllcorner;
+} slab_terrain_desc;
+
+/* The remeshed grid the reference writes at every frame
+ * (src/simulation.cpp:584-642, src/save_function.cpp:96-226). The caller sets
+ * the pointers (capacity given in cap_nodes); the call fills Nx, Ny, i_off,
+ * j_off and the arrays (flattened i*Ny + j over the Nx x Ny box). */
+typedef struct slab_grid_view {
+    int32_t Nx, Ny, i_off, j_off;
+    int64_t cap_nodes;
+    double* h;
+    double* mass;
+    double* v;  /* interleaved vx,vy */
+    double* vz;
+} slab_grid_view;
+
+typedef struct slab_ctx slab_ctx;
+
+/* Create a context on the current CUDA device over terrain z[i*Ny+j].
+ * Computes the terrain metric terms once, in FP64
+ * (Simulation::terrainGradients / terrainTheta, src/complex_terrain.cpp:84-111)
+ * and zeroes h_max / v_max2 (src/simulation.cpp:255-256). */
+slab_status slab_create(const slab_terrain_desc* terrain, const double* z, slab_ctx** out);
+
+/* Set the physical/numerical parameters (members filled by
+ * Simulation::loadFromJSON, src/simulation.cpp:118-208). Must precede
+ * slab_upload_particles. */
+slab_status slab_set_params(slab_ctx* ctx, const slab_params* params);
+
+/* Use this CUDA stream (a cudaStream_t) for every later call; NULL = the
+ * context's own stream. */
+slab_status slab_set_stream(slab_ctx* ctx, void* cuda_stream);
+
+/* Upload the particle set built by Simulation::initializeParticles
+ * (src/simulation.cpp:259-476) -- the arrays of class Particles
+ * (src/data_arrays.hpp:22-47). theta is derived on the device. Resets time,
+ * dt and frame to zero. */
+slab_status slab_upload_particles(slab_ctx* ctx, int32_t Np, const double* x_xy, const double* v_xy, const double* vz, const double* h,
+                                  const double* A, const double* mass, const double* z);
+
+/* simulate()'s t=0 pass (src/simulation.cpp:493-495): remesh, P2G and the
+ * grid update with dt = 0, which normalises the grid fields for frame 0 and
+ * seeds h_max. */
+slab_status slab_initial_pass(slab_ctx* ctx);
+
+/* Run iterations of simulate()'s loop (src/simulation.cpp:500-510, each one
+ * Simulation::advanceStep, src/simulation.cpp:524-563, then time += dt) until
+ * the next output frame is reached or time >= total_time. time and dt are
+ * computed on the device exactly as Simulation::updateDt
+ * (src/simulation.cpp:565-582), including the snap onto the frame time.
+ * Outputs (any may be NULL): time after the last step, frame counter, and the
+ * number of steps taken. */
+slab_status slab_advance_to_frame(slab_ctx* ctx, double* time_out, int32_t* frame_out, int64_t* steps_out);
+
+/* Run up to nsteps iterations of the same loop without stopping at frames
+ * (frames still snap dt and bump the frame counter); stops early at
+ * total_time. For benchmarks and tests. */
+slab_status slab_advance_steps(slab_ctx* ctx, int64_t nsteps, int64_t* steps_out);
+
+/* Copy the particle state back in the upload order (the reference reorders
+ * particles every 50 steps, src/simulation.cpp:540; the engine keeps stable
+ * ids instead). Any pointer may be NULL. A = mass/(h*rho) as in G2P
+ * (src/simulation.cpp:938). z and vz are the values of the last step's G2P. */
+slab_status slab_download_particles(slab_ctx* ctx, double* x_xy, double* v_xy, double* vz, double* h, double* A, double* mass, double* z);
+
+/* The grid fields of the last step over the reference's remeshed bounding
+ * box (src/simulation.cpp:603-612). */
+slab_status slab_download_grid(slab_ctx* ctx, slab_grid_view* view);
+
+/* Full-terrain maxima (Grid::h_max, Grid::v_max2), as written by
+ * Simulation::saveMaxData (src/save_function.cpp:228-291). Nx*Ny each. */
+slab_status slab_download_max(slab_ctx* ctx, double* h_max, double* v_max2);
+
+/* Diagnostics, all FP64: out[0] = total particle mass, out[1] = total grid
+ * mass of the last step, out[2..3] = particle momentum (x, y). */
+slab_status slab_conservation(slab_ctx* ctx, double out[4]);
+
+/* time, dt, frame and steps so far (Simulation members time, dt, frame). */
+slab_status slab_get_state(slab_ctx* ctx, double* time, double* dt, int32_t* frame, int64_t* steps);
+
+/* Device-time breakdown of the last advance call in milliseconds, per kernel
+ * family: out[0] dt/control, [1] bin/sort, [2] P2G, [3] grid update, [4] G2P.
+ * Mirrors the reference's per-phase timers (src/simulation.cpp:512-519).
+ * Enabled by slab_set_profiling(ctx, 1); adds event records per step. */
+slab_status slab_set_profiling(slab_ctx* ctx, int32_t on);
+slab_status slab_get_phase_times(slab_ctx* ctx, double out[5]);
+
+/* Number of kernels this context has launched since creation. */
+int64_t slab_kernel_launches(const slab_ctx* ctx);
+
+const char* slab_last_error(const slab_ctx* ctx);
+void slab_destroy(slab_ctx* ctx);
+
+/* Library version string and status-code names. */
+const char* slab_version(void);
+const char* slab_status_name(slab_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLAB_GPU_H */

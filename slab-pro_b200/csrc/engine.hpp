@@ -1,0 +1,80 @@
+// Host-side engine: the context behind the C ABI and the interface of the two
+// step-loop implementations (plain FP64, split FP32).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "slab_gpu.h"
+
+namespace slab {
+
+// Thrown inside the library, turned into a slab_status at the C boundary.
+struct Error {
+    slab_status code;
+    std::string msg;
+};
+
+#define SLAB_CUDA(call)                                                                                     \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess)                                                                              \
+            throw ::slab::Error{e_ == cudaErrorMemoryAllocation ? SLAB_E_OOM : SLAB_E_CUDA,                 \
+                                std::string(#call) + ": " + cudaGetErrorString(e_)};                        \
+    } while (0)
+
+template <typename T> T* dmalloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{SLAB_E_OOM, "cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed: " + cudaGetErrorString(e)};
+    }
+    return static_cast<T*>(p);
+}
+
+struct DFree {
+    void operator()(void* p) const { cudaFree(p); }
+};
+template <typename T> using dptr = std::unique_ptr<T, DFree>;
+template <typename T> dptr<T> dalloc(size_t n) { return dptr<T>(dmalloc<T>(n)); }
+
+// Terrain metric terms shared by both paths, computed once on the device in
+// FP64 (Simulation::terrainGradients / terrainTheta,
+// src/complex_terrain.cpp:84-111).
+struct Terrain {
+    int Nx = 0, Ny = 0;
+    double dx = 0, xll = 0, yll = 0;
+    dptr<double> z;        // Nx*Ny
+    dptr<double2> grad;    // cell gradient stored at the bottom-left node
+    dptr<double> cos_t;    // cos(atan|grad|)
+    dptr<float4> dem32;    // FP32 copy for the split path: gx, gy, cos(theta), z
+};
+
+struct Path {
+    virtual ~Path() = default;
+    virtual void upload(int Np, const double* x, const double* v, const double* vz, const double* h, const double* A, const double* m,
+                        const double* z) = 0;
+    virtual void initial_pass() = 0;
+    // enqueue up to `chunk` steps; the device control block decides which run
+    virtual void enqueue_steps(int chunk) = 0;
+    virtual void download_particles(double* x, double* v, double* vz, double* h, double* A, double* m, double* z) = 0;
+    virtual void download_grid(slab_grid_view* view) = 0;
+    virtual void download_max(double* h_max, double* v_max2) = 0;
+    virtual void conservation(double out[4]) = 0;
+    virtual int64_t launches() const = 0;
+    virtual void phase_times(double out[5]) { for (int k = 0; k < 5; ++k) out[k] = 0; }
+    virtual void set_profiling(bool) {}
+};
+
+std::unique_ptr<Path> make_plain64(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d_ctl, Ctl* h_ctl);
+std::unique_ptr<Path> make_split32(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d_ctl, Ctl* h_ctl);
+
+void compute_terrain_metrics(Terrain& t, cudaStream_t s);
+
+}  // namespace slab

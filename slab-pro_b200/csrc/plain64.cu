@@ -1,0 +1,488 @@
+// Plain single-scenario FP64 step loop (kernels P0-P5). Compiled with
+// -fmad=false: every multiply and add is the IEEE operation the reference
+// performs, so the only differences from the reference are the order of the
+// P2G atomic sums and the last bit of CUDA's cos/atan.
+//
+// Layout: particles FP64 SoA in upload order; node fields dense over the
+// whole terrain (i*Ny + j). The grid box of each step is the reference's
+// remesh box (src/simulation.cpp:584-642) computed on the device; it bounds
+// the grid-update work and the accumulator zeroing, which replaces the
+// reference's per-step reallocation.
+#include <algorithm>
+#include <cstring>
+
+#include "engine.hpp"
+
+namespace slab {
+namespace {
+
+struct P64 {
+    double2 *x, *v;
+    double *vz, *h, *A, *m, *z;
+};
+
+struct N64 {
+    double *m, *px, *py, *pvz, *hm, *Fx, *Fy;  // P2G accumulators (zero between steps)
+    double2 *v, *flip;                          // grid velocity and FLIP increment of the last step
+    double *out_h, *out_m, *out_vz;             // normalised grid fields for output frames
+    double *h_max, *v_max2;                     // Grid::h_max / Grid::v_max2 of the terrain
+};
+
+struct Phys {
+    double g, rho, flip_ratio, one_over_dx, dx;
+    int fric;
+    double mu_c, mu_v, xi, mu1, mu2, I0, d, phi;
+    int Nx, Ny;
+};
+
+// quadratic B-spline and derivative in the reference's form (src/tools.hpp:119-140)
+__device__ __forceinline__ double Nq(double u) {
+    const double a = fabs(u);
+    if (a < 0.5) return 0.75 - a * a;
+    if (a < 1.5) return 0.5 * (1.5 - a) * (1.5 - a);
+    return 0.0;
+}
+__device__ __forceinline__ double dNq(double u) {
+    const double a = fabs(u);
+    if (a < 0.5) return -2.0 * u;
+    if (a < 1.5) return u - 1.5 * (double)((0.0 < u) - (u < 0.0));
+    return 0.0;
+}
+
+__device__ __forceinline__ void stencil_weights(const Phys& P, double xp, int base, double w[3], double dw[3]) {
+    for (int d = 0; d < 3; ++d) {
+        const double u = (xp - (double)(base + d) * P.dx) * P.one_over_dx;
+        w[d] = Nq(u);
+        dw[d] = dNq(u) * P.one_over_dx;
+    }
+}
+
+__global__ void k64_begin(Ctl* c, int Nx, int Ny) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) ctl_begin(c, Nx, Ny);
+}
+__global__ void k64_begin_t0(Ctl* c, int Nx, int Ny) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) ctl_begin_t0(c, Nx, Ny);
+}
+
+// P2G (src/simulation.cpp:726-798) with atomicAdd(double) scatter. Slope
+// terms of the particle's containing cell (src/complex_terrain.cpp:113-130).
+__global__ void __launch_bounds__(256) k64_p2g(const Ctl* __restrict__ c, P64 p, N64 n, const double2* __restrict__ grad,
+                                               const double* __restrict__ cos_t, Phys P, int Np) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Np || !c->active) return;
+    const double2 x = p.x[q], v = p.v[q];
+    const double h = p.h[q], A = p.A[q], m = p.m[q];
+    const double vmx = v.x * m, vmy = v.y * m;
+    const double vzm = p.vz[q] * m, hm = h * m, hA = h * A;
+    const int ib = (int)floor(x.x * P.one_over_dx - 0.5), jb = (int)floor(x.y * P.one_over_dx - 0.5);
+    const int cell = (int)floor(x.x * P.one_over_dx) * P.Ny + (int)floor(x.y * P.one_over_dx);
+    const double2 gr = grad[cell];
+    const double ct = cos_t[cell];
+    const double coeff = -m * P.g * ct * ct;
+    const double mbx = coeff * gr.x, mby = coeff * gr.y;
+    const double s00 = -0.5 * P.rho * P.g * ct * ct * h;
+    double wx[3], wy[3], dwx[3], dwy[3];
+    stencil_weights(P, x.x, ib, wx, dwx);
+    stencil_weights(P, x.y, jb, wy, dwy);
+#pragma unroll
+    for (int di = 0; di < 3; ++di) {
+#pragma unroll
+        for (int dj = 0; dj < 3; ++dj) {
+            const double w = wx[di] * wy[dj];
+            if (w > 3e-3) {
+                const double gwx = dwx[di] * wy[dj], gwy = dwy[dj] * wx[di];
+                const int64_t k = (int64_t)(ib + di) * P.Ny + (jb + dj);
+                atomicAdd(n.m + k, m * w);
+                atomicAdd(n.px + k, vmx * w);
+                atomicAdd(n.py + k, vmy * w);
+                atomicAdd(n.pvz + k, vzm * w);
+                atomicAdd(n.hm + k, hm * w);
+                atomicAdd(n.Fx + k, mbx * w - hA * (s00 * gwx + 0.0 * gwy));
+                atomicAdd(n.Fy + k, mby * w - hA * (s00 * gwy + 0.0 * gwx));
+            }
+        }
+    }
+}
+
+// computeGridVelocity (src/simulation.cpp:800-875) over the remesh box, then
+// the accumulators are zeroed for the next step.
+__global__ void __launch_bounds__(256) k64_grid(const Ctl* __restrict__ c, N64 n, const double2* __restrict__ grad,
+                                                const double* __restrict__ cos_t, Phys P) {
+    if (!c->active) return;
+    const int i0 = c->box[0], j0 = c->box[2];
+    const int nI = c->box[1] - i0 + 1, nJ = c->box[3] - j0 + 1;
+    const int64_t total = (int64_t)nI * nJ;
+    const double dt = c->dt;
+    const bool outs = c->write_outputs;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = i0 + (int)(t / nJ), j = j0 + (int)(t % nJ);
+        const int64_t k = (int64_t)i * P.Ny + j;
+        const double mi = n.m[k];
+        double2 nv = make_double2(0.0, 0.0), fl = make_double2(0.0, 0.0);
+        double hn = 0.0, vzn = 0.0;
+        if (mi > 1e-6) {
+            const double vox = n.px[k] / mi, voy = n.py[k] / mi;
+            vzn = n.pvz[k] / mi;
+            hn = n.hm[k] / mi;
+            const double ax = n.Fx[k] / mi, ay = n.Fy[k] / mi;
+            const double vtx = vox + dt * ax, vty = voy + dt * ay;
+            const double vsq = vtx * vtx + vty * vty;
+            if (vsq > 1e-16) {
+                const double2 gr = grad[k];
+                const double ct = cos_t[k];
+                const double vz = vtx * gr.x + vty * gr.y;
+                const double v3sq = vsq + vz * vz;
+                const double v3 = sqrt(v3sq);
+                double af;
+                if (P.fric == SLAB_COULOMB) {
+                    af = P.mu_c * P.g * ct;
+                } else if (P.fric == SLAB_VOELLMY) {
+                    af = P.mu_v * P.g * ct + P.g * v3sq / (P.xi * hn * ct);
+                } else {
+                    const double I = 5. * P.d * v3 / (2. * hn * ct * ct * sqrt(P.g * hn * P.phi));
+                    const double muI = P.mu1 + (P.mu2 - P.mu1) / (1. + P.I0 / I);
+                    af = muI * P.g * ct;
+                }
+                const double dv = dt * af;
+                if (dv < v3) {
+                    const double f = 1. - dv / v3;
+                    nv = make_double2(vtx * f, vty * f);
+                }
+            }
+            fl = make_double2(nv.x - vox, nv.y - voy);
+            if (n.h_max[k] < hn) n.h_max[k] = hn;
+            const double v2 = nv.x * nv.x + nv.y * nv.y;
+            if (n.v_max2[k] < v2) n.v_max2[k] = v2;
+        }
+        n.v[k] = nv;
+        n.flip[k] = fl;
+        if (outs) {
+            n.out_h[k] = hn;
+            n.out_m[k] = mi;
+            n.out_vz[k] = vzn;
+        }
+        n.m[k] = 0.0;
+        n.px[k] = 0.0;
+        n.py[k] = 0.0;
+        n.pvz[k] = 0.0;
+        n.hm[k] = 0.0;
+        n.Fx[k] = 0.0;
+        n.Fy[k] = 0.0;
+    }
+}
+
+__device__ __forceinline__ uint64_t dbits(double v) { return (uint64_t)__double_as_longlong(v); }
+
+// Block-reduce the particle bounding box and max |v|^2 into the control
+// block; the last block to finish closes the step.
+__device__ void block_epilogue(Ctl* c, bool valid, double px, double py, double v2, bool close_step) {
+    __shared__ double s_red[5][8];
+    double mnx = valid ? px : INFINITY, mxx = valid ? px : 0.0, mny = valid ? py : INFINITY, mxy = valid ? py : 0.0;
+    double vv = valid ? v2 : 0.0;
+    mnx = warp_min(mnx);
+    mxx = warp_max(mxx);
+    mny = warp_min(mny);
+    mxy = warp_max(mxy);
+    vv = warp_max(vv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) {
+        s_red[0][wid] = mnx;
+        s_red[1][wid] = mxx;
+        s_red[2][wid] = mny;
+        s_red[3][wid] = mxy;
+        s_red[4][wid] = vv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < nw; ++w) {
+            mnx = fmin(mnx, s_red[0][w]);
+            mxx = fmax(mxx, s_red[1][w]);
+            mny = fmin(mny, s_red[2][w]);
+            mxy = fmax(mxy, s_red[3][w]);
+            vv = fmax(vv, s_red[4][w]);
+        }
+        atomicMin(reinterpret_cast<unsigned long long*>(&c->pos_acc[0]), (unsigned long long)dbits(mnx));
+        atomicMax(reinterpret_cast<unsigned long long*>(&c->pos_acc[1]), (unsigned long long)dbits(mxx));
+        atomicMin(reinterpret_cast<unsigned long long*>(&c->pos_acc[2]), (unsigned long long)dbits(mny));
+        atomicMax(reinterpret_cast<unsigned long long*>(&c->pos_acc[3]), (unsigned long long)dbits(mxy));
+        atomicMax(reinterpret_cast<unsigned long long*>(&c->vmax2_acc), (unsigned long long)dbits(vv));
+        if (close_step) {
+            __threadfence();
+            const unsigned prev = atomicAdd(&c->done_blocks, 1u);
+            if (prev == gridDim.x - 1) {
+                __threadfence();
+                ctl_end(c);
+            }
+        }
+    }
+}
+
+// G2P (src/simulation.cpp:877-940).
+__global__ void __launch_bounds__(256) k64_g2p(Ctl* c, P64 p, N64 n, const double2* __restrict__ grad, const double* __restrict__ z,
+                                               Phys P, int Np) {
+    if (!c->active) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = q < Np;
+    double2 nx = make_double2(0, 0);
+    double v2 = 0.0;
+    if (valid) {
+        const double2 x = p.x[q];
+        const int cell = (int)floor(x.x * P.one_over_dx) * P.Ny + (int)floor(x.y * P.one_over_dx);
+        const double2 pg = grad[cell];
+        const int ib = (int)floor(x.x * P.one_over_dx - 0.5), jb = (int)floor(x.y * P.one_over_dx - 0.5);
+        double wx[3], wy[3], dwx[3], dwy[3];
+        stencil_weights(P, x.x, ib, wx, dwx);
+        stencil_weights(P, x.y, jb, wy, dwy);
+        double picx = 0.0, picy = 0.0, flx = 0.0, fly = 0.0, zp = 0.0, strain = 0.0;
+#pragma unroll
+        for (int di = 0; di < 3; ++di) {
+#pragma unroll
+            for (int dj = 0; dj < 3; ++dj) {
+                const double w = wx[di] * wy[dj];
+                const int64_t k = (int64_t)(ib + di) * P.Ny + (jb + dj);
+                const double gwx = dwx[di] * wy[dj], gwy = dwy[dj] * wx[di];
+                const double2 gv = n.v[k], gf = n.flip[k];
+                picx += gv.x * w;
+                picy += gv.y * w;
+                flx += gf.x * w;
+                fly += gf.y * w;
+                zp += z[k] * w;
+                strain += gwx * gv.x + gwy * gv.y;
+            }
+        }
+        const double dt = c->dt;
+        strain *= dt;
+        const double2 v = p.v[q];
+        const double fr = P.flip_ratio;
+        const double nvx = fr * (v.x + flx) + (1. - fr) * picx;
+        const double nvy = fr * (v.y + fly) + (1. - fr) * picy;
+        p.z[q] = zp;
+        p.v[q] = make_double2(nvx, nvy);
+        p.vz[q] = nvx * pg.x + nvy * pg.y;
+        nx = make_double2(x.x + dt * picx, x.y + dt * picy);
+        p.x[q] = nx;
+        const double hn = p.h[q] / (1. + strain);
+        p.h[q] = hn;
+        p.A[q] = p.m[q] / (hn * P.rho);
+        v2 = nvx * nvx + nvy * nvy;
+        if (!isfinite(nx.x) || !isfinite(nx.y) || !isfinite(v2) || !isfinite(hn)) atomicOr(&c->err, ERR_NONFINITE);
+        if (nx.x < 0.0 || nx.y < 0.0) atomicOr(&c->err, ERR_DOMAIN);
+    }
+    block_epilogue(c, valid, nx.x, nx.y, v2, true);
+}
+
+// Particle box and max |v|^2 of freshly uploaded particles.
+__global__ void k64_stats(Ctl* c, P64 p, int Np) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = q < Np;
+    double2 x = make_double2(0, 0);
+    double v2 = 0;
+    if (valid) {
+        x = p.x[q];
+        const double2 v = p.v[q];
+        v2 = v.x * v.x + v.y * v.y;
+        if (x.x < 0.0 || x.y < 0.0) atomicOr(&c->err, ERR_DOMAIN);
+    }
+    block_epilogue(c, valid, x.x, x.y, v2, false);
+}
+
+struct Plain64 final : Path {
+    const Terrain& T;
+    slab_params prm;
+    cudaStream_t st;
+    Ctl* dc;
+    Ctl* hc;
+    Phys P{};
+    int Np = 0;
+    dptr<double2> x, v;
+    dptr<double> vz, h, A, m, z;
+    dptr<double> acc;  // 7 accumulators, each Nx*Ny
+    dptr<double2> gv, gflip;
+    dptr<double> out3;  // out_h, out_m, out_vz
+    dptr<double> maxes; // h_max, v_max2
+    int64_t nlaunch = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_chunk = 0;
+
+    Plain64(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d, Ctl* h_) : T(t), prm(p), st(s), dc(d), hc(h_) {
+        P.g = p.gravity;
+        P.rho = p.rho;
+        P.flip_ratio = p.flip_ratio;
+        P.one_over_dx = 1. / t.dx;
+        P.dx = t.dx;
+        P.fric = p.friction.type;
+        P.mu_c = p.friction.coulomb_mu;
+        P.mu_v = p.friction.voellmy_mu;
+        P.xi = p.friction.voellmy_xi;
+        P.mu1 = p.friction.mu_1;
+        P.mu2 = p.friction.mu_2;
+        P.I0 = p.friction.I0;
+        P.d = p.friction.d;
+        P.phi = p.friction.phi;
+        P.Nx = t.Nx;
+        P.Ny = t.Ny;
+        const size_t nn = (size_t)t.Nx * t.Ny;
+        acc = dalloc<double>(7 * nn);
+        gv = dalloc<double2>(nn);
+        gflip = dalloc<double2>(nn);
+        out3 = dalloc<double>(3 * nn);
+        maxes = dalloc<double>(2 * nn);
+        SLAB_CUDA(cudaMemsetAsync(acc.get(), 0, 7 * nn * sizeof(double), st));
+        SLAB_CUDA(cudaMemsetAsync(gv.get(), 0, nn * sizeof(double2), st));
+        SLAB_CUDA(cudaMemsetAsync(gflip.get(), 0, nn * sizeof(double2), st));
+        SLAB_CUDA(cudaMemsetAsync(out3.get(), 0, 3 * nn * sizeof(double), st));
+        SLAB_CUDA(cudaMemsetAsync(maxes.get(), 0, 2 * nn * sizeof(double), st));
+    }
+    ~Plain64() override {
+        if (graph) cudaGraphExecDestroy(graph);
+    }
+
+    P64 parts() { return P64{x.get(), v.get(), vz.get(), h.get(), A.get(), m.get(), z.get()}; }
+    N64 nodes() {
+        const size_t nn = (size_t)T.Nx * T.Ny;
+        double* a = acc.get();
+        double* o = out3.get();
+        return N64{a, a + nn, a + 2 * nn, a + 3 * nn, a + 4 * nn, a + 5 * nn, a + 6 * nn, gv.get(), gflip.get(),
+                   o, o + nn, o + 2 * nn, maxes.get(), maxes.get() + nn};
+    }
+
+    void upload(int np, const double* hx, const double* hv, const double* hvz, const double* hh, const double* hA, const double* hm,
+                const double* hz) override {
+        Np = np;
+        x = dalloc<double2>(np);
+        v = dalloc<double2>(np);
+        vz = dalloc<double>(np);
+        h = dalloc<double>(np);
+        A = dalloc<double>(np);
+        m = dalloc<double>(np);
+        z = dalloc<double>(np);
+        SLAB_CUDA(cudaMemcpyAsync(x.get(), hx, np * sizeof(double2), cudaMemcpyHostToDevice, st));
+        SLAB_CUDA(cudaMemcpyAsync(v.get(), hv, np * sizeof(double2), cudaMemcpyHostToDevice, st));
+        SLAB_CUDA(cudaMemcpyAsync(vz.get(), hvz, np * sizeof(double), cudaMemcpyHostToDevice, st));
+        SLAB_CUDA(cudaMemcpyAsync(h.get(), hh, np * sizeof(double), cudaMemcpyHostToDevice, st));
+        SLAB_CUDA(cudaMemcpyAsync(A.get(), hA, np * sizeof(double), cudaMemcpyHostToDevice, st));
+        SLAB_CUDA(cudaMemcpyAsync(m.get(), hm, np * sizeof(double), cudaMemcpyHostToDevice, st));
+        SLAB_CUDA(cudaMemcpyAsync(z.get(), hz, np * sizeof(double), cudaMemcpyHostToDevice, st));
+        // the control block was reset by the caller; collect the initial box / max speed
+        k64_stats<<<(np + 255) / 256, 256, 0, st>>>(dc, parts(), np);
+        SLAB_CUDA(cudaGetLastError());
+        ++nlaunch;
+        SLAB_CUDA(cudaMemcpyAsync(&dc->vmax2_bits, &dc->vmax2_acc, sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+    }
+
+    int grid_blocks() const { return 148 * 4; }
+
+    void launch_step() {
+        const int pb = (Np + 255) / 256;
+        k64_begin<<<1, 32, 0, st>>>(dc, T.Nx, T.Ny);
+        k64_p2g<<<pb, 256, 0, st>>>(dc, parts(), nodes(), T.grad.get(), T.cos_t.get(), P, Np);
+        k64_grid<<<grid_blocks(), 256, 0, st>>>(dc, nodes(), T.grad.get(), T.cos_t.get(), P);
+        k64_g2p<<<pb, 256, 0, st>>>(dc, parts(), nodes(), T.grad.get(), T.z.get(), P, Np);
+    }
+
+    void initial_pass() override {
+        k64_begin_t0<<<1, 32, 0, st>>>(dc, T.Nx, T.Ny);
+        k64_p2g<<<(Np + 255) / 256, 256, 0, st>>>(dc, parts(), nodes(), T.grad.get(), T.cos_t.get(), P, Np);
+        k64_grid<<<grid_blocks(), 256, 0, st>>>(dc, nodes(), T.grad.get(), T.cos_t.get(), P);
+        SLAB_CUDA(cudaGetLastError());
+        nlaunch += 3;
+    }
+
+    void enqueue_steps(int chunk) override {
+        if (!graph || graph_chunk != chunk) {
+            if (graph) cudaGraphExecDestroy(graph);
+            graph = nullptr;
+            cudaGraph_t g;
+            SLAB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < chunk; ++k) launch_step();
+            SLAB_CUDA(cudaStreamEndCapture(st, &g));
+            cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+            cudaGraphDestroy(g);
+            SLAB_CUDA(e);
+            graph_chunk = chunk;
+        }
+        SLAB_CUDA(cudaGraphLaunch(graph, st));
+        nlaunch += 4 * chunk;
+    }
+
+    void download_particles(double* hx, double* hv, double* hvz, double* hh, double* hA, double* hm, double* hz) override {
+        auto cp = [&](double* dst, const void* src, size_t bytes) {
+            if (dst) SLAB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        };
+        cp(hx, x.get(), Np * sizeof(double2));
+        cp(hv, v.get(), Np * sizeof(double2));
+        cp(hvz, vz.get(), Np * sizeof(double));
+        cp(hh, h.get(), Np * sizeof(double));
+        cp(hA, A.get(), Np * sizeof(double));
+        cp(hm, m.get(), Np * sizeof(double));
+        cp(hz, z.get(), Np * sizeof(double));
+        SLAB_CUDA(cudaStreamSynchronize(st));
+    }
+
+    void download_grid(slab_grid_view* gv_) override {
+        SLAB_CUDA(cudaMemcpyAsync(hc, dc, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        SLAB_CUDA(cudaStreamSynchronize(st));
+        const int i0 = hc->box[0], i1 = hc->box[1], j0 = hc->box[2], j1 = hc->box[3];
+        const int gNx = i1 - i0 + 1, gNy = j1 - j0 + 1;
+        gv_->Nx = gNx;
+        gv_->Ny = gNy;
+        gv_->i_off = i0;
+        gv_->j_off = j0;
+        if ((int64_t)gNx * gNy > gv_->cap_nodes) throw Error{SLAB_E_ARG, "grid view capacity too small"};
+        N64 n = nodes();
+        std::vector<double> row(2 * (size_t)gNy);
+        for (int i = 0; i < gNx; ++i) {
+            const size_t src = (size_t)(i0 + i) * T.Ny + j0, dst = (size_t)i * gNy;
+            if (gv_->h) SLAB_CUDA(cudaMemcpyAsync(gv_->h + dst, n.out_h + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (gv_->mass) SLAB_CUDA(cudaMemcpyAsync(gv_->mass + dst, n.out_m + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (gv_->vz) SLAB_CUDA(cudaMemcpyAsync(gv_->vz + dst, n.out_vz + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (gv_->v) SLAB_CUDA(cudaMemcpyAsync(gv_->v + 2 * dst, n.v + src, gNy * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        }
+        SLAB_CUDA(cudaStreamSynchronize(st));
+    }
+
+    void download_max(double* hmax, double* vmax2) override {
+        const size_t nn = (size_t)T.Nx * T.Ny;
+        if (hmax) SLAB_CUDA(cudaMemcpyAsync(hmax, maxes.get(), nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (vmax2) SLAB_CUDA(cudaMemcpyAsync(vmax2, maxes.get() + nn, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SLAB_CUDA(cudaStreamSynchronize(st));
+    }
+
+    void conservation(double out[4]) override {
+        std::vector<double> hmass(Np), hv(2 * (size_t)Np);
+        download_particles(nullptr, hv.data(), nullptr, nullptr, nullptr, hmass.data(), nullptr);
+        double M = 0, Px = 0, Py = 0;
+        for (int q = 0; q < Np; ++q) {
+            M += hmass[q];
+            Px += hmass[q] * hv[2 * q];
+            Py += hmass[q] * hv[2 * q + 1];
+        }
+        SLAB_CUDA(cudaMemcpyAsync(hc, dc, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        SLAB_CUDA(cudaStreamSynchronize(st));
+        const int i0 = hc->box[0], i1 = hc->box[1], j0 = hc->box[2], j1 = hc->box[3];
+        double G = 0;
+        std::vector<double> row(j1 - j0 + 1);
+        for (int i = i0; i <= i1; ++i) {
+            SLAB_CUDA(cudaMemcpy(row.data(), nodes().out_m + (size_t)i * T.Ny + j0, row.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (double r : row) G += r;
+        }
+        out[0] = M;
+        out[1] = G;
+        out[2] = Px;
+        out[3] = Py;
+    }
+
+    int64_t launches() const override { return nlaunch; }
+};
+
+}  // namespace
+
+std::unique_ptr<Path> make_plain64(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d_ctl, Ctl* h_ctl) {
+    return std::unique_ptr<Path>(new Plain64(t, p, s, d_ctl, h_ctl));
+}
+
+}  // namespace slab

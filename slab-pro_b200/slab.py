@@ -1,0 +1,209 @@
+"""Python binding of libslab_gpu.so (include/slab_gpu.h) over ctypes.
+
+The library is the product; this module only marshals numpy arrays. It loads
+the in-tree build (slab-pro_b200/lib/libslab_gpu.so) and fails loudly when it
+is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libslab_gpu.so")
+
+COULOMB, VOELLMY, MU_I = 0, 1, 2
+FRICTION_NAMES = {"COULOMB": COULOMB, "VOELLMY": VOELLMY, "MU_I": MU_I}
+FP64_PLAIN, FP32_SPLIT = 0, 1
+
+STATUS = {0: "SLAB_OK", 1: "SLAB_E_ARG", 2: "SLAB_E_CUDA", 3: "SLAB_E_OOM", 4: "SLAB_E_DOMAIN",
+          5: "SLAB_E_NONFINITE", 6: "SLAB_E_TIMEOUT", 7: "SLAB_E_STATE", 8: "SLAB_E_NOTFOUND"}
+
+
+class SlabError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Friction(C.Structure):
+    _fields_ = [("type", C.c_int32), ("pad_", C.c_int32), ("coulomb_mu", C.c_double),
+                ("voellmy_mu", C.c_double), ("voellmy_xi", C.c_double),
+                ("mu_1", C.c_double), ("mu_2", C.c_double), ("I0", C.c_double), ("d", C.c_double), ("phi", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [("gravity", C.c_double), ("rho", C.c_double), ("C_cfl", C.c_double), ("dt_max", C.c_double),
+                ("flip_ratio", C.c_double), ("output_dt", C.c_double), ("total_time", C.c_double),
+                ("friction", Friction), ("precision", C.c_int32), ("pad_", C.c_int32)]
+
+
+class TerrainDesc(C.Structure):
+    _fields_ = [("Nx", C.c_int32), ("Ny", C.c_int32), ("dx", C.c_double), ("xllcorner", C.c_double), ("yllcorner", C.c_double)]
+
+
+class GridView(C.Structure):
+    _fields_ = [("Nx", C.c_int32), ("Ny", C.c_int32), ("i_off", C.c_int32), ("j_off", C.c_int32), ("cap_nodes", C.c_int64),
+                ("h", C.POINTER(C.c_double)), ("mass", C.POINTER(C.c_double)), ("v", C.POINTER(C.c_double)),
+                ("vz", C.POINTER(C.c_double))]
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C slab-pro_b200` or __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        vp = C.c_void_p
+        L.slab_create.argtypes = [C.POINTER(TerrainDesc), dp, C.POINTER(vp)]
+        L.slab_set_params.argtypes = [vp, C.POINTER(Params)]
+        L.slab_set_stream.argtypes = [vp, vp]
+        L.slab_upload_particles.argtypes = [vp, C.c_int32] + [dp] * 7
+        L.slab_initial_pass.argtypes = [vp]
+        L.slab_advance_to_frame.argtypes = [vp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+        L.slab_advance_steps.argtypes = [vp, C.c_int64, C.POINTER(C.c_int64)]
+        L.slab_download_particles.argtypes = [vp] + [dp] * 7
+        L.slab_download_grid.argtypes = [vp, C.POINTER(GridView)]
+        L.slab_download_max.argtypes = [vp, dp, dp]
+        L.slab_conservation.argtypes = [vp, dp]
+        L.slab_get_state.argtypes = [vp, dp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+        L.slab_set_profiling.argtypes = [vp, C.c_int32]
+        L.slab_get_phase_times.argtypes = [vp, dp]
+        L.slab_kernel_launches.argtypes = [vp]
+        L.slab_kernel_launches.restype = C.c_int64
+        L.slab_last_error.argtypes = [vp]
+        L.slab_last_error.restype = C.c_char_p
+        L.slab_destroy.argtypes = [vp]
+        L.slab_version.restype = C.c_char_p
+        L.slab_status_name.restype = C.c_char_p
+        L.slab_status_name.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def make_params(cfg: dict, precision: int = FP64_PLAIN) -> Params:
+    """cfg: flat dict with gravity, rho, C_cfl, dt_max, flip_ratio, output_dt,
+    total_time, friction ('COULOMB'|'VOELLMY'|'MU_I') and its coefficients
+    (coulomb_mu | voellmy_mu, voellmy_xi | mui_mu1, mui_mu2, mui_I0, mui_d, mui_phi)."""
+    p = Params()
+    p.gravity, p.rho = cfg["gravity"], cfg["rho"]
+    p.C_cfl, p.dt_max, p.flip_ratio = cfg["C_cfl"], cfg["dt_max"], cfg["flip_ratio"]
+    p.output_dt, p.total_time = cfg["output_dt"], cfg["total_time"]
+    f = p.friction
+    f.type = FRICTION_NAMES[cfg["friction"]]
+    f.coulomb_mu = cfg.get("coulomb_mu", 0.0)
+    f.voellmy_mu, f.voellmy_xi = cfg.get("voellmy_mu", 0.0), cfg.get("voellmy_xi", 1.0)
+    f.mu_1, f.mu_2 = cfg.get("mui_mu1", 0.0), cfg.get("mui_mu2", 0.0)
+    f.I0, f.d, f.phi = cfg.get("mui_I0", 1.0), cfg.get("mui_d", 0.0), cfg.get("mui_phi", 1.0)
+    p.precision = precision
+    return p
+
+
+class Slab:
+    """One simulation context on the current CUDA device."""
+
+    def __init__(self, z: np.ndarray, dx: float, xll: float = 0.0, yll: float = 0.0):
+        self.L = lib()
+        self.Nx, self.Ny = z.shape
+        zz = np.ascontiguousarray(z, dtype=np.float64)
+        td = TerrainDesc(self.Nx, self.Ny, float(dx), float(xll), float(yll))
+        h = C.c_void_p()
+        self._check(self.L.slab_create(C.byref(td), _dp(zz), C.byref(h)), None)
+        self.h = h
+        self.Np = 0
+
+    def _check(self, code, h="self"):
+        if code != 0:
+            msg = self.L.slab_last_error(self.h if h == "self" else None)
+            raise SlabError(code, (msg or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.slab_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_params(self, cfg: dict, precision: int = FP64_PLAIN):
+        self._params = make_params(cfg, precision)
+        self._check(self.L.slab_set_params(self.h, C.byref(self._params)))
+
+    def set_stream(self, stream_handle: int):
+        self._check(self.L.slab_set_stream(self.h, C.c_void_p(stream_handle)))
+
+    def upload(self, P: dict):
+        n = len(P["h"])
+        arrs = [np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "v", "vz", "h", "A", "mass", "z")]
+        self._check(self.L.slab_upload_particles(self.h, n, *[_dp(a) for a in arrs]))
+        self.Np = n
+
+    def initial_pass(self):
+        self._check(self.L.slab_initial_pass(self.h))
+
+    def advance_to_frame(self):
+        t, f, s = C.c_double(), C.c_int32(), C.c_int64()
+        self._check(self.L.slab_advance_to_frame(self.h, C.byref(t), C.byref(f), C.byref(s)))
+        return t.value, f.value, s.value
+
+    def advance_steps(self, n: int) -> int:
+        s = C.c_int64()
+        self._check(self.L.slab_advance_steps(self.h, int(n), C.byref(s)))
+        return s.value
+
+    def particles(self) -> dict:
+        n = self.Np
+        out = {k: np.zeros(2 * n if k in ("x", "v") else n) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
+        self._check(self.L.slab_download_particles(self.h, *[_dp(out[k]) for k in ("x", "v", "vz", "h", "A", "mass", "z")]))
+        out["x"] = out["x"].reshape(n, 2)
+        out["v"] = out["v"].reshape(n, 2)
+        return out
+
+    def grid(self) -> dict:
+        cap = self.Nx * self.Ny
+        bufs = {k: np.zeros(2 * cap if k == "v" else cap) for k in ("h", "mass", "v", "vz")}
+        gv = GridView(0, 0, 0, 0, cap, _dp(bufs["h"]), _dp(bufs["mass"]), _dp(bufs["v"]), _dp(bufs["vz"]))
+        self._check(self.L.slab_download_grid(self.h, C.byref(gv)))
+        n = gv.Nx * gv.Ny
+        g = {k: bufs[k][:n].reshape(gv.Nx, gv.Ny) for k in ("h", "mass", "vz")}
+        g["v"] = bufs["v"][:2 * n].reshape(gv.Nx, gv.Ny, 2)
+        g.update(Nx=gv.Nx, Ny=gv.Ny, i_off=gv.i_off, j_off=gv.j_off)
+        return g
+
+    def max_maps(self):
+        hm = np.zeros(self.Nx * self.Ny)
+        vm = np.zeros(self.Nx * self.Ny)
+        self._check(self.L.slab_download_max(self.h, _dp(hm), _dp(vm)))
+        return hm.reshape(self.Nx, self.Ny), vm.reshape(self.Nx, self.Ny)
+
+    def conservation(self):
+        out = np.zeros(4)
+        self._check(self.L.slab_conservation(self.h, _dp(out)))
+        return out
+
+    def state(self):
+        t, dt, f, s = C.c_double(), C.c_double(), C.c_int32(), C.c_int64()
+        self._check(self.L.slab_get_state(self.h, C.byref(t), C.byref(dt), C.byref(f), C.byref(s)))
+        return t.value, dt.value, f.value, s.value
+
+    def kernel_launches(self) -> int:
+        return self.L.slab_kernel_launches(self.h)
+
+    def set_profiling(self, on: bool):
+        self._check(self.L.slab_set_profiling(self.h, 1 if on else 0))
+
+    def phase_times(self):
+        out = np.zeros(5)
+        self._check(self.L.slab_get_phase_times(self.h, _dp(out)))
+        return out

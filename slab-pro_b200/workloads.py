@@ -1,0 +1,332 @@
+"""Synthetic inputs and host-side setup for the Slab-Pro step loop.
+
+* ESRI ASCII grid (.asc) reading and writing with the reference's conventions
+  (Simulation::readASC, src/complex_terrain.cpp:31-65: rows are stored top
+  to bottom and reversed so that j grows northwards; node (i, j) sits at
+  (i*cellsize, j*cellsize) and z is flattened i*Ny + j).
+* The reference's particle initialisation for RECTANGLE / ELLIPSE / RASTER
+  releases with UNIFORM sampling (Simulation::initializeParticles,
+  src/simulation.cpp:259-476), restated with numpy in the same operation
+  order so the particle sets are bit-identical.
+* Seeded generators for the benchmark workloads: the 35-degree slope with a
+  circular-arc runout (1 600 particles), fractal slopes with spectral
+  roughness on 4096^2 / 8192^2 / 2048^2 DEMs, star-polygon raster releases
+  with lognormal heights, and ensembles of elliptical releases.
+
+No public dataset is involved: every workload is generated here from a seed.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+# ---------------------------------------------------------------- .asc files
+
+
+def read_asc(path: str):
+    """Return (z[Nx, Ny], header dict) exactly as Simulation::readASC."""
+    with open(path) as f:
+        hdr = {}
+        for _ in range(6):
+            k, v = f.readline().split()
+            hdr[k.lower()] = float(v)
+        nc, nr = int(hdr["ncols"]), int(hdr["nrows"])
+        vals = np.array(f.read().split(), dtype=np.float64)
+    if vals.size != nc * nr:
+        raise ValueError(f"{path}: expected {nc * nr} values, found {vals.size}")
+    z = np.empty((nc, nr))
+    z[:, ::-1] = vals.reshape(nr, nc).T
+    return z, hdr
+
+
+def write_asc(path: str, z: np.ndarray, cellsize: float, xll: float = 0.0, yll: float = 0.0, nodata: float = -9999.0):
+    """Write z[Nx, Ny] so that read_asc (and the reference) read back the same doubles."""
+    nc, nr = z.shape
+    with open(path, "w") as f:
+        f.write(f"ncols {nc}\nnrows {nr}\nxllcorner {xll!r}\nyllcorner {yll!r}\ncellsize {cellsize!r}\nNODATA_value {nodata!r}\n")
+        rows = z[:, ::-1].T  # top row first
+        for r in rows:
+            f.write(" ".join(repr(float(v)) for v in r))
+            f.write("\n")
+
+
+# ------------------------------------------------------- reference particle setup
+
+
+def _N(u):
+    """Quadratic B-spline, src/tools.hpp:119-128 (vectorised)."""
+    a = np.abs(u)
+    return np.where(a < 0.5, 0.75 - a * a, np.where(a < 1.5, 0.5 * (1.5 - a) * (1.5 - a), 0.0))
+
+
+def terrain_gradient_norm(z: np.ndarray, dx: float) -> np.ndarray:
+    """|grad z| of terrainGradients (src/complex_terrain.cpp:84-100)."""
+    ood = 1.0 / dx
+    gx = np.zeros_like(z)
+    gy = np.zeros_like(z)
+    gx[:-1, :-1] = (z[1:, :-1] + z[1:, 1:] - z[:-1, :-1] - z[:-1, 1:]) / 2.0 * ood
+    gy[:-1, :-1] = (z[:-1, 1:] + z[1:, 1:] - z[:-1, :-1] - z[1:, :-1]) / 2.0 * ood
+    return np.sqrt(gx * gx + gy * gy)
+
+
+def libm_atan(a: np.ndarray) -> np.ndarray:
+    """atan through the C library (as the reference calls it); numpy's own
+    vectorised arctan can differ in the last bit."""
+    return np.frompyfunc(math.atan, 1, 1)(a).astype(np.float64)
+
+
+def terrain_theta(z: np.ndarray, dx: float) -> np.ndarray:
+    """terrainTheta (src/complex_terrain.cpp:102-111) over the whole terrain."""
+    return libm_atan(terrain_gradient_norm(z, dx))
+
+
+def release_particles(z: np.ndarray, dx: float, release: dict, rho: float, sampling: str = "UNIFORM",
+                      samples: np.ndarray | None = None) -> dict:
+    """Simulation::initializeParticles for RECTANGLE/ELLIPSE/RASTER releases.
+
+    release: {"type": "RECTANGLE", "center": (x, y), "Lx", "Ly", "rotation_deg", "h0"}
+             {"type": "ELLIPSE", "center": (x, y), "rx", "ry", "rotation_deg", "h0"}
+             {"type": "RASTER", "h": h[nc, nr], "x0", "y0", "cellsize", "nodata", "h_min"}
+               (x0, y0: raster origin relative to the terrain origin)
+    sampling: "UNIFORM" (2x2 per cell) or "GIVEN" (samples: positions relative
+    to the bounding box corner, as the Poisson sampler returns them).
+    """
+    ood = 1.0 / dx
+    typ = release["type"]
+    if typ == "RECTANGLE":
+        cx, cy = release["center"]
+        Lx, Ly = release["Lx"], release["Ly"]
+        diag = math.sqrt(Lx * Lx + Ly * Ly) / 2.0
+        x_min, x_max, y_min, y_max = cx - diag, cx + diag, cy - diag, cy + diag
+        area = Lx * Ly
+    elif typ == "ELLIPSE":
+        cx, cy = release["center"]
+        big = max(release["rx"], release["ry"])
+        x_min, x_max, y_min, y_max = cx - big, cx + big, cy - big, cy + big
+        area = math.pi * release["rx"] * release["ry"]
+    elif typ == "RASTER":
+        rh = release["h"]
+        cs = release["cellsize"]
+        x_min, y_min = release["x0"], release["y0"]
+        x_max = x_min + cs * (rh.shape[0] - 1)
+        y_max = y_min + cs * (rh.shape[1] - 1)
+        # loop order j outer, i inner as in the reference (src/simulation.cpp:337-345)
+        mask = (rh >= release["h_min"]) & (rh > 0.0)
+        vol = 0.0
+        cell_area = cs * cs
+        for j in range(rh.shape[1]):
+            for i in np.nonzero(mask[:, j])[0]:
+                vol += rh[i, j] * cell_area
+        area = int(mask.sum()) * cell_area
+    else:
+        raise ValueError(f"release type {typ} not supported here")
+    volume = vol if typ == "RASTER" else area * release["h0"]
+    x_min = math.floor(x_min * ood) * dx
+    x_max = math.ceil(x_max * ood) * dx
+    y_min = math.floor(y_min * ood) * dx
+    y_max = math.ceil(y_max * ood) * dx
+    if sampling == "UNIFORM":
+        nxc = int(round((x_max - x_min) * ood))
+        nyc = int(round((y_max - y_min) * ood))
+        dxp = np.array([0.25, 0.75, 0.25, 0.75])
+        dyp = np.array([0.25, 0.25, 0.75, 0.75])
+        I, J, D = np.meshgrid(np.arange(nxc, dtype=np.float64), np.arange(nyc, dtype=np.float64), np.arange(4), indexing="ij")
+        px = ((I + dxp[D]) * dx).ravel()
+        py = ((J + dyp[D]) * dx).ravel()
+    else:
+        px, py = samples[:, 0].copy(), samples[:, 1].copy()
+    sx = px + x_min
+    sy = py + y_min
+    if typ in ("RECTANGLE", "ELLIPSE"):
+        rot = release["rotation_deg"] * math.pi / 180.0
+        c, s = math.cos(-rot), math.sin(-rot)
+        dx0, dy0 = sx - release["center"][0], sy - release["center"][1]
+        lx = c * dx0 - s * dy0
+        ly = s * dx0 + c * dy0
+        if typ == "RECTANGLE":
+            keep = (np.abs(lx) <= release["Lx"] / 2.0) & (np.abs(ly) <= release["Ly"] / 2.0)
+        else:
+            keep = (lx / release["rx"]) ** 2 + (ly / release["ry"]) ** 2 <= 1.0
+        hk = None
+    else:
+        hk = raster_height(release, sx, sy)
+        keep = (hk >= release["h_min"]) & (hk > 0.0)
+        hk = hk[keep]
+    x = np.stack([sx[keep], sy[keep]], axis=1)
+    n = len(x)
+    h = np.full(n, float(release.get("h0", 0.0))) if hk is None else hk
+    sum_h = float(np.cumsum(h)[-1]) if n else 0.0  # sequential sum, as the reference loop
+    A_init = volume / sum_h
+    A = np.full(n, A_init)
+    mass = rho * h * A
+    gn = terrain_gradient_norm(z, dx)
+    ci = np.floor(x[:, 0] * ood).astype(np.int64)
+    cj = np.floor(x[:, 1] * ood).astype(np.int64)
+    cells, inv = np.unique(ci * z.shape[1] + cj, return_inverse=True)
+    theta = libm_atan(gn.ravel()[cells])[inv]  # particleSlopeAngle (src/complex_terrain.cpp:113-120)
+    # z by the 4x4 stencil of src/simulation.cpp:455-465
+    zp = np.zeros(n)
+    ib = (x[:, 0] * ood).astype(np.int64) - 1
+    jb = (x[:, 1] * ood).astype(np.int64) - 1
+    for a in range(4):
+        for b in range(4):
+            i = ib + a
+            j = jb + b
+            w = _N((x[:, 0] - i * dx) * ood) * _N((x[:, 1] - j * dx) * ood)
+            zp = zp + z[i, j] * w
+    return {"x": x, "z": zp, "v": np.zeros((n, 2)), "vz": np.zeros(n), "h": h, "A": A, "mass": mass, "theta": theta}
+
+
+def raster_height(release: dict, px: np.ndarray, py: np.ndarray) -> np.ndarray:
+    """Simulation::getReleaseHeightFromRaster (src/complex_terrain.cpp:132-183), vectorised."""
+    rh = release["h"]
+    cs = release["cellsize"]
+    nx, ny = rh.shape
+    x0, y0 = release["x0"], release["y0"]
+    xr = px - x0
+    yr = py - y0
+    # the reference compares the relative position with the raster's last
+    # absolute coordinate x.back(); the index test below is the binding one
+    xlast = x0 + (nx - 1) * cs
+    ylast = y0 + (ny - 1) * cs
+    dxl = (x0 + cs) - x0
+    dyl = (y0 + cs) - y0
+    out = np.zeros_like(px)
+    ok = (xr >= 0) & (yr >= 0) & (xr < xlast) & (yr < ylast)
+    i = np.floor(xr / dxl).astype(np.int64)
+    j = np.floor(yr / dyl).astype(np.int64)
+    ok &= (i >= 0) & (j >= 0) & (i < nx - 1) & (j < ny - 1)
+    i = np.where(ok, i, 0)
+    j = np.where(ok, j, 0)
+    fx = (xr - i * dxl) / dxl
+    fy = (yr - j * dyl) / dyl
+    z00, z10, z01, z11 = rh[i, j], rh[i + 1, j], rh[i, j + 1], rh[i + 1, j + 1]
+    nd = release.get("nodata", -9999.0)
+    bad = (np.abs(z00 - nd) < 1e-6) | (np.abs(z10 - nd) < 1e-6) | (np.abs(z01 - nd) < 1e-6) | (np.abs(z11 - nd) < 1e-6)
+    z0 = z00 * (1.0 - fx) + z10 * fx
+    z1 = z01 * (1.0 - fx) + z11 * fx
+    hgt = z0 * (1.0 - fy) + z1 * fy
+    hgt = np.where(hgt > 0.0, hgt, 0.0)
+    return np.where(ok & ~bad, hgt, 0.0)
+
+
+# ------------------------------------------------------------ terrains
+
+
+def slope_arc_dem(Lx=2000.0, Ly=500.0, dx=5.0, angle_deg=35.0, x_break=1200.0, radius=100.0):
+    """35-degree plane z = tan(35)(1200 - x) for x < 1200, blended into a flat
+    runout by a circular arc of the given radius tangent to both (the arc's
+    tangent points lie R tan(a/2) from the break on either side)."""
+    a = math.radians(angle_deg)
+    t = radius * math.tan(a / 2.0)
+    x1 = x_break - t * math.cos(a)
+    x2 = x_break + t
+    nx = int(round(Lx / dx)) + 1
+    ny = int(round(Ly / dx)) + 1
+    x = np.arange(nx) * dx
+    zx = np.where(x <= x1, math.tan(a) * (x_break - x),
+                  np.where(x < x2, radius - np.sqrt(np.maximum(radius * radius - (x - x2) ** 2, 0.0)), 0.0))
+    return np.repeat(zx[:, None], ny, axis=1)
+
+
+def analytical_plane(Lx: float, Ly: float, dx: float):
+    """The reference's hard-coded ANALYTICAL terrain (src/simulation.cpp:181-185):
+    z = -x tan5 - y tan5 on generateGrid nodes (src/complex_terrain.cpp:67-82)."""
+    def gen(L):
+        g = [0.0]
+        x, idx = 0.0, 0
+        while x < L:
+            idx += 1
+            x = float(idx) * dx
+            g.append(x)
+        return np.array(g)
+    xs, ys = gen(Lx), gen(Ly)
+    th = 5.0 * math.pi / 180.0
+    return -xs[:, None] * math.tan(th) - ys[None, :] * math.tan(th)
+
+
+def fractal_slope_dem(n: int, dx: float, seed: int, rms: float = 15.0, hurst: float = 0.8, lowpass_m: float = 20.0,
+                      x_plane_end: float = 2500.0, ease_m: float = 500.0, steep_deg: float = 30.0, flat_deg: float = 5.0):
+    """Planar 30-degree slope for x < 2500 m easing (smoothstep in tan) to a
+    5-degree runout over 500 m, plus seeded fBm roughness: spectrum
+    PSD ~ k^-(2H+2), wavelengths shorter than lowpass_m removed, scaled to rms."""
+    rng = np.random.default_rng(seed)
+    L = n * dx
+    x = np.arange(n) * dx
+    s0, s1 = math.tan(math.radians(steep_deg)), math.tan(math.radians(flat_deg))
+    u = np.clip((x - x_plane_end) / ease_m, 0.0, 1.0)
+    slope = s0 + (s1 - s0) * (u * u * (3 - 2 * u))
+    zx = -np.concatenate([[0.0], np.cumsum(0.5 * (slope[1:] + slope[:-1]) * dx)])
+    zx -= zx.min()
+    kx = np.fft.fftfreq(n, d=dx)
+    ky = np.fft.rfftfreq(n, d=dx)
+    K = np.sqrt(kx[:, None] ** 2 + ky[None, :] ** 2)
+    amp = np.zeros_like(K)
+    nz = K > 0
+    amp[nz] = K[nz] ** (-(2 * hurst + 2) / 2.0)
+    amp[K > 1.0 / lowpass_m] = 0.0
+    amp[K < 1.0 / L] = 0.0
+    ph = rng.standard_normal(K.shape) + 1j * rng.standard_normal(K.shape)
+    rough = np.fft.irfft2(amp * ph, s=(n, n))
+    rough *= rms / max(rough.std(), 1e-30)
+    return zx[:, None] + rough
+
+
+# ----------------------------------------------------------- releases
+
+
+def star_polygon(seed: int, center, ax: float, ay: float, nvert: int = 12):
+    rng = np.random.default_rng(seed)
+    ang = np.sort(rng.uniform(0, 2 * np.pi, nvert))
+    r = rng.uniform(0.6, 1.0, nvert)
+    return np.stack([center[0] + ax * r * np.cos(ang), center[1] + ay * r * np.sin(ang)], axis=1)
+
+
+def point_in_polygon(px, py, poly):
+    """Even-odd rule (the algorithm of src/polygon_tools.cpp), vectorised."""
+    inside = np.zeros(px.shape, dtype=bool)
+    n = len(poly)
+    j = n - 1
+    for i in range(n):
+        xi, yi = poly[i]
+        xj, yj = poly[j]
+        cond = ((yi > py) != (yj > py)) & (px < (xj - xi) * (py - yi) / (yj - yi + 1e-300) + xi)
+        inside ^= cond
+        j = i
+    return inside
+
+
+def lognormal_release_raster(seed: int, poly, cellsize: float, median: float = 1.5, sigma_log: float = 0.4, corr_m: float = 10.0):
+    """RASTER release covering the polygon: lognormal heights (median, sigma_log)
+    from a smooth seeded Gaussian field, zero (below h_min) outside the polygon."""
+    rng = np.random.default_rng(seed)
+    x0, y0 = np.floor(poly.min(axis=0) / cellsize) * cellsize - 2 * cellsize
+    x1, y1 = np.ceil(poly.max(axis=0) / cellsize) * cellsize + 2 * cellsize
+    nx = int(round((x1 - x0) / cellsize)) + 1
+    ny = int(round((y1 - y0) / cellsize)) + 1
+    g = rng.standard_normal((nx, ny))
+    kx = np.fft.fftfreq(nx, d=cellsize)
+    ky = np.fft.fftfreq(ny, d=cellsize)
+    filt = np.exp(-0.5 * (2 * np.pi * corr_m) ** 2 * (kx[:, None] ** 2 + ky[None, :] ** 2))
+    g = np.real(np.fft.ifft2(np.fft.fft2(g) * filt))
+    g /= max(g.std(), 1e-30)
+    h = np.exp(math.log(median) + sigma_log * g)
+    X = x0 + np.arange(nx)[:, None] * cellsize + 0 * np.arange(ny)[None, :]
+    Y = y0 + 0 * np.arange(nx)[:, None] + np.arange(ny)[None, :] * cellsize
+    inside = point_in_polygon(X, Y, poly)
+    h = np.where(inside, h, 0.0)
+    return {"type": "RASTER", "h": h, "x0": float(x0), "y0": float(y0), "cellsize": cellsize, "nodata": -9999.0}
+
+
+# ------------------------------------------------------------ configs
+
+
+def config1():
+    """35-degree slope with circular-arc runout, 1 600 particles, Coulomb."""
+    z = slope_arc_dem()
+    cfg = dict(gravity=9.81, rho=300.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=60.0,
+               friction="COULOMB", coulomb_mu=0.4)
+    rel = {"type": "RECTANGLE", "center": (150.0, 250.0), "Lx": 100.0, "Ly": 100.0, "rotation_deg": 0.0, "h0": 2.0}
+    P = release_particles(z, 5.0, rel, cfg["rho"])
+    return {"name": "slope35_arc_401x101_dx5", "z": z, "dx": 5.0, "cfg": cfg, "release": rel, "particles": P}

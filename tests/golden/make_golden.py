@@ -1,0 +1,125 @@
+"""Generate the golden fixtures tests/golden/<case>.npz by running the
+reference's own step-loop sources (oracle/_ref/slab_ref, built by
+`make -C oracle ref` from the reference tree) on the cases in cases.py.
+
+    python tests/golden/make_golden.py [case ...]
+
+Each fixture holds, from the reference run:
+  frame0_digest   sha256 of the initial particle arrays (setup parity)
+  f<k>_<field>    particle arrays at output frame k (x, z, v, vz, h, A, mass,
+                  theta), plus f<k>_time / f<k>_dt
+  s<k>_<field>    state after step k of the phase driver (steps 1, 2, 50, 51)
+  max_idx, max_h, max_v2   nonzero entries of the final h_max / v_max2
+  nsteps          steps taken to total_time
+The reference binary writes raw FP64 dumps (oracle/ref_hooks.cpp), so the
+fixtures are the reference's exact doubles.
+"""
+from __future__ import annotations
+
+import glob
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import cases  # noqa: E402
+import oracle as O  # noqa: E402
+
+sys.path.insert(0, os.path.join(ROOT, "slab-pro_b200"))
+import workloads as W  # noqa: E402
+
+PHASE_STEPS = (1, 2, 50, 51)
+
+
+def write_inputs(c: dict, d: str) -> str:
+    cfg = c["cfg"]
+    if "analytical" in c:
+        terrain = {"type": "ANALYTICAL", "analytical": c["analytical"]}
+    else:
+        W.write_asc(os.path.join(d, "dem.asc"), c["z"], c["dx"])
+        terrain = {"type": "DEM", "dem": {"filepath": os.path.join(d, "dem.asc")}}
+    rel = dict(c["json_release"])
+    if rel["type"] == "RASTER":
+        r = c["release"]
+        W.write_asc(os.path.join(d, "release.asc"), r["h"], r["cellsize"], xll=r["x0"], yll=r["y0"])
+        rel["raster"] = dict(rel["raster"], filepath=os.path.join(d, "release.asc"))
+    j = {"project_dir": os.path.join(d, "out"), "sim_name": c["name"],
+         "physical_params": {"gravity": cfg["gravity"], "rho": cfg["rho"]},
+         "time_params": {"output_dt": cfg["output_dt"], "total_time": cfg["total_time"]},
+         "numerical_params": {"C_cfl": cfg["C_cfl"], "dt_max": cfg["dt_max"], "flip_ratio": cfg["flip_ratio"],
+                              "sampling_method": "UNIFORM"},
+         "friction": c["json_friction"], "terrain": terrain, "release": rel}
+    path = os.path.join(d, "config.json")
+    with open(path, "w") as f:
+        json.dump(j, f, indent=1)
+    return path
+
+
+def run_ref(cfg_path: str, *args):
+    out = subprocess.run([O.REF_BIN, cfg_path, *args], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError(f"slab_ref failed: {out.stderr}")
+    return out.stdout
+
+
+def make(name: str):
+    c = cases.CASES[name]()
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        cfg_path = write_inputs(c, d)
+        sim_dir = os.path.join(d, "out", c["name"])
+        run_ref(cfg_path, "--init-only")
+        f0 = O.read_particles_bin(sorted(glob.glob(os.path.join(sim_dir, "particles", "particles_frame_*.bin")))[0])
+        out["frame0_digest"] = np.array(cases.particle_digest(f0))
+        if cases.particle_digest(c["particles"]) != str(out["frame0_digest"]):
+            raise RuntimeError(f"{name}: numpy setup differs from the reference's initializeParticles")
+        log = run_ref(cfg_path)
+        nsteps = int([ln for ln in log.splitlines() if ln.startswith("Time step:")][-1].split()[2])
+        out["nsteps"] = np.array(nsteps)
+        for k in c["frames"]:
+            P = O.read_particles_bin(_frame_file(sim_dir, k))
+            for fld in O.PARTICLE_FIELDS:
+                out[f"f{k}_{fld}"] = P[fld]
+            out[f"f{k}_time"] = np.array(P["time"])
+            out[f"f{k}_dt"] = np.array(P["dt"])
+        hm, vm = O.read_max_bin(os.path.join(sim_dir, "max_values.bin"))
+        idx = np.nonzero((hm != 0) | (vm != 0))
+        out["max_idx"] = np.stack(idx, axis=1).astype(np.int32)
+        out["max_h"] = hm[idx]
+        out["max_v2"] = vm[idx]
+        out["max_shape"] = np.array(hm.shape)
+        run_ref(cfg_path, "--steps", str(max(PHASE_STEPS)))
+        recs = O.read_steps_bin(os.path.join(sim_dir, "steps.bin"))
+        for k in PHASE_STEPS:
+            r = recs[k]
+            out[f"s{k}_time"] = np.array(r["time"])
+            out[f"s{k}_dt"] = np.array(r["dt"])
+            for fld in ("x", "v", "h", "z", "vz"):
+                out[f"s{k}_{fld}"] = r["particles"][fld]
+            g = r["grid"]
+            out[f"s{k}_grid_box"] = np.array([g["Nx"], g["Ny"], g["i_off"], g["j_off"]])
+            for fld in ("mass", "h", "v", "flip", "vz"):
+                out[f"s{k}_grid_{fld}"] = g[fld]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: Np={len(c['particles']['h'])} steps={nsteps} -> {name}.npz")
+
+
+def _frame_file(sim_dir: str, k: int) -> str:
+    for p in glob.glob(os.path.join(sim_dir, "particles", "particles_frame_*.bin")):
+        if int(os.path.basename(p)[len("particles_frame_"):-4]) == k:
+            return p
+    raise FileNotFoundError(f"frame {k} in {sim_dir}")
+
+
+if __name__ == "__main__":
+    if not os.path.exists(O.REF_BIN):
+        sys.exit("oracle/_ref/slab_ref is not built (make -C oracle ref)")
+    for n in (sys.argv[1:] or list(cases.CASES)):
+        make(n)

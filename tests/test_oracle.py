@@ -1,0 +1,140 @@
+"""The C oracle against the golden fixtures written by the reference's own
+step-loop sources (oracle/_ref/slab_ref): bit-exact, step by step and frame by
+frame, plus the numpy restatement of the reference's particle setup."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import cases
+import oracle as O
+
+CASES = list(cases.CASES)
+
+
+@pytest.fixture(scope="module", params=CASES)
+def case(request):
+    return request.param, cases.CASES[request.param]()
+
+
+def test_setup_matches_reference(case, golden):
+    name, c = case
+    assert cases.particle_digest(c["particles"]) == str(golden(name)["frame0_digest"])
+
+
+def _oracle(c):
+    o = O.Oracle(c["cfg"], c["z"], c["dx"])
+    o.set_particles(c["particles"])
+    o.t0()
+    return o
+
+
+def test_phase_steps_bit_exact(case, golden):
+    name, c = case
+    g = golden(name)
+    o = _oracle(c)
+    done = 0
+    for k in (1, 2, 50, 51):
+        while done < k:
+            o.step()
+            done += 1
+        t, dt, _, _ = o.state()
+        assert t == g[f"s{k}_time"] and dt == g[f"s{k}_dt"]
+        P = o.particles()
+        for fld in ("x", "v", "h", "z", "vz"):
+            assert np.array_equal(P[fld], g[f"s{k}_{fld}"]), (k, fld)
+        G = o.grid()
+        assert [G["Nx"], G["Ny"], G["i_off"], G["j_off"]] == list(g[f"s{k}_grid_box"])
+        for fld in ("mass", "h", "v", "flip", "vz"):
+            assert np.array_equal(G[fld], g[f"s{k}_grid_{fld}"]), (k, fld)
+
+
+def test_frames_and_max_maps_bit_exact(case, golden):
+    name, c = case
+    g = golden(name)
+    o = _oracle(c)
+    nsteps = 0
+    for f in range(1, max(c["frames"]) + 1):
+        while True:
+            nsteps += 1
+            if o.step() == 1:
+                break
+        if f in c["frames"]:
+            t, dt, frame, _ = o.state()
+            assert frame == f
+            assert t == g[f"f{f}_time"] and dt == g[f"f{f}_dt"]
+            P = o.particles()
+            for fld in O.PARTICLE_FIELDS:
+                assert np.array_equal(P[fld], g[f"f{f}_{fld}"]), (f, fld)
+    nsteps += o.run()
+    assert nsteps == int(g["nsteps"])
+    hm, vm = o.max_maps()
+    idx = tuple(g["max_idx"].T)
+    assert np.array_equal(hm[idx], g["max_h"]) and np.array_equal(vm[idx], g["max_v2"])
+    nz = (hm != 0) | (vm != 0)
+    assert nz.sum() == len(g["max_h"])
+
+
+def test_oracle_terrain_metrics(case):
+    name, c = case
+    o = O.Oracle(c["cfg"], c["z"], c["dx"])
+    import workloads as W
+    _, th = o.terrain_metrics()
+    assert np.array_equal(th, W.terrain_theta(c["z"], c["dx"]))
+
+
+def test_oracle_particle_ids_track_sort():
+    c = cases.case_slope35()
+    o = _oracle(c)
+    for _ in range(50):
+        o.step()
+    ids = o.ids()
+    assert sorted(ids.tolist()) == list(range(len(ids)))
+    assert not np.array_equal(ids, np.arange(len(ids)))  # the step-50 sort permuted them
+    Pb = o.particles_by_id()
+    P = o.particles()
+    assert np.array_equal(Pb["x"][ids], P["x"])
+
+
+REF_EXAMPLES = "/root/reference/examples"
+
+
+@pytest.mark.skipif(not (os.path.exists(O.REF_BIN) and os.path.isdir(REF_EXAMPLES)), reason="reference tree not present")
+def test_oracle_vs_reference_binary_brienz_5m(tmp_path):
+    """Live check on the reference's own example (5 m Brienz DEM, raster
+    release, POISSON sampling with the reference's std::rand, mu(I)): 120
+    steps of the oracle against the reference binary, bit for bit."""
+    import json
+    import workloads as W
+    j = json.load(open(os.path.join(REF_EXAMPLES, "brienz_raster.json")))
+    j["project_dir"] = str(tmp_path)
+    j["sim_name"] = "b5"
+    j["terrain"]["dem"]["filepath"] = os.path.join(REF_EXAMPLES, "brienz_terrain_5m.asc")
+    j["release"]["raster"]["filepath"] = os.path.join(REF_EXAMPLES, "brienz_release_raster_5m.asc")
+    j["time_params"]["total_time"] = 20.0
+    j["time_params"]["output_dt"] = 5.0
+    cfgp = tmp_path / "b5.json"
+    cfgp.write_text(json.dumps(j))
+    subprocess.run([O.REF_BIN, str(cfgp), "--init-only"], check=True, capture_output=True)
+    import glob
+    P0 = O.read_particles_bin(glob.glob(str(tmp_path / "b5" / "particles" / "*.bin"))[0])
+    n = 120
+    subprocess.run([O.REF_BIN, str(cfgp), "--steps", str(n)], check=True, capture_output=True)
+    recs = O.read_steps_bin(str(tmp_path / "b5" / "steps.bin"))
+    z, hdr = W.read_asc(os.path.join(REF_EXAMPLES, "brienz_terrain_5m.asc"))
+    fr = j["friction"]["mu_I"]
+    params = dict(gravity=j["physical_params"]["gravity"], rho=j["physical_params"]["rho"], C_cfl=0.5, dt_max=0.04,
+                  flip_ratio=0.9, output_dt=5.0, total_time=20.0, friction="MU_I", mui_mu1=fr["mu_1"],
+                  mui_mu2=fr["mu_2"], mui_I0=fr["I0"], mui_d=fr["d"], mui_phi=fr["phi"])
+    o = O.Oracle(params, z, hdr["cellsize"])
+    o.set_particles(P0)
+    o.t0()
+    for k in range(1, n + 1):
+        o.step()
+        if k % 20 == 0 or k in (1, 50, 51):
+            P = o.particles()
+            for fld in O.PARTICLE_FIELDS:
+                assert np.array_equal(P[fld], recs[k]["particles"][fld]), (k, fld)
+    hm, vm = o.max_maps()
+    assert np.array_equal(hm, recs[n]["h_max"]) and np.array_equal(vm, recs[n]["v_max2"])
