@@ -1,0 +1,430 @@
+"""Benchmark of the depth-averaged MPM step loop on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1|c3]
+
+Default workload (c2): 4096^2 fractal-slope DEM at 1 m, star-polygon RASTER
+release with lognormal heights, POISSON sampling at 0.5 m (665 653
+particles), Voellmy friction -- all generated from fixed seeds (data:
+synthetic). A "step" is one MPM time step (dt, P2G, grid update with
+friction, G2P) of the whole scenario; the metric is particle-steps/s.
+
+Our arm (--impl ours): the FP32 split-precision path through the C ABI
+(libslab_gpu.so). The scenario is first advanced 2 s of simulated time
+(untimed) so the flow is developed; then W warm-up steps and K timed steps,
+each step bracketed by CUDA events on the library's stream, with a 256 MiB
+write between steps to flush L2 (126 MB). Reported beside it: the plain
+FP64 GPU path on the same state, per-kernel device times and the HBM
+roofline of the dominant kernel, the reference CPU code on the same state
+(cpu_baseline), and the end-to-end rate through the public API with host
+buffers (e2e).
+
+The reference arm (--impl reference) runs the reference's own step-loop
+sources (oracle/_ref/slab_ref) on the box's host cores: one process per core
+(up to 8), each on the same workload, timed by the reference's own per-phase
+timers.
+
+Multi-GPU: the single-scenario path does not shard; N ranks run N replicas
+(scaling "weak"), value = all ranks' particle-steps / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "slab-pro_b200"))
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "particle-steps/s"
+# algorithmic bytes of the FP32 split path (per particle-step, per active node-step)
+BYTES_P, BYTES_N = 76, 124
+KERNEL_BYTES = {  # per kernel: (bytes per particle-step, bytes per active node-step)
+    "p2g": (28, 28),
+    "grid": (0, 76),
+    "g2p": (48, 20),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_workload(name: str):
+    import slab
+    import workloads as W
+    if name == "c1":
+        return W.config1()
+    if name == "c2":
+        return W.config2(sampler=slab.poisson_disk)
+    if name == "c3":
+        return W.config3()
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and s[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def measured_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def write_ref_inputs(c, P, d):
+    """Binary DEM + particle files and a JSON for oracle/_ref/slab_ref."""
+    import struct
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    dem = os.path.join(d, "dem.bin")
+    with open(dem, "wb") as f:
+        f.write(struct.pack("<qqd", c["z"].shape[0], c["z"].shape[1], c["dx"]))
+        f.write(np.ascontiguousarray(c["z"], dtype=np.float64).tobytes())
+    parts = os.path.join(d, "particles.bin")
+    O.write_particles_bin(parts, P)
+    return dem, parts
+
+
+def ref_json(c, d, nsteps_time):
+    cfg = c["cfg"]
+    fr = cfg["friction"]
+    fj = {"type": fr}
+    if fr == "COULOMB":
+        fj["coulomb"] = {"mu": cfg["coulomb_mu"]}
+    elif fr == "VOELLMY":
+        fj["voellmy"] = {"mu": cfg["voellmy_mu"], "xi": cfg["voellmy_xi"]}
+    else:
+        fj["mu_I"] = {"mu_1": cfg["mui_mu1"], "mu_2": cfg["mui_mu2"], "I0": cfg["mui_I0"], "d": cfg["mui_d"], "phi": cfg["mui_phi"]}
+    j = {"project_dir": os.path.join(d, "out"), "sim_name": "bench",
+         "physical_params": {"gravity": cfg["gravity"], "rho": cfg["rho"]},
+         "time_params": {"output_dt": nsteps_time, "total_time": nsteps_time},
+         "numerical_params": {"C_cfl": cfg["C_cfl"], "dt_max": cfg["dt_max"], "flip_ratio": cfg["flip_ratio"], "sampling_method": "UNIFORM"},
+         "friction": fj,
+         "terrain": {"type": "ANALYTICAL", "analytical": {"Lx": 8.0, "Ly": 8.0, "dx": c["dx"]}},
+         "release": {"type": "RECTANGLE", "h0": 1.0, "rectangle": {"center": [4.0, 4.0], "Lx": 1.0, "Ly": 1.0, "rotation_deg": 0.0}}}
+    path = os.path.join(d, f"cfg_{os.getpid()}_{len(os.listdir(d))}.json")
+    with open(path, "w") as f:
+        json.dump(j, f)
+    return path
+
+
+def run_reference(c, P, nsteps, replicas):
+    """Run the reference binary `replicas` times concurrently for about
+    `nsteps` steps from state P; returns (particle-steps/s aggregate, steps,
+    seconds of the slowest replica)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not os.path.exists(O.REF_BIN):
+        raise RuntimeError("oracle/_ref/slab_ref not built")
+    with tempfile.TemporaryDirectory() as d:
+        dem, parts = write_ref_inputs(c, P, d)
+        T = nsteps * c["cfg"]["dt_max"]
+        procs = []
+        for r in range(replicas):
+            cfg = ref_json(c, d, T)
+            env = dict(os.environ, SLAB_REF_NO_DUMP="1")
+            procs.append(subprocess.Popen([O.REF_BIN, cfg, "--dem-bin", dem, "--particles", parts], stdout=subprocess.PIPE,
+                                          stderr=subprocess.PIPE, text=True, env=env))
+        secs, steps = [], []
+        for p in procs:
+            out, err = p.communicate()
+            if p.returncode != 0:
+                raise RuntimeError(f"slab_ref failed: {err.strip()[-300:]}")
+            phase = 0.0
+            last = 0
+            for ln in out.splitlines():
+                if ln.startswith("Time step:"):
+                    last = int(ln.split()[2])
+                for key in ("updateDt took", "sort took", "remesh took", "P2G took", "computeGridVelocity took", "G2P took"):
+                    if ln.startswith(key):
+                        phase += float(ln.split()[-2])
+            secs.append(phase)
+            steps.append(last)
+    Np = len(P["h"])
+    tmax = max(secs)
+    return sum(steps) * Np / tmax, steps[0], tmax
+
+
+def ours(args, rank, world):
+    import torch
+    import slab
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    c = load_workload(args.workload)
+    P0 = c["particles"]
+    Np = len(P0["h"])
+    cfg = dict(c["cfg"], output_dt=c["cfg"]["total_time"])  # no frame stops inside the timed region
+    log(f"[rank {rank}] workload {c['name']}: Np={Np} DEM {c['z'].shape} dx={c['dx']}")
+
+    def make(prec):
+        s = slab.Slab(c["z"], c["dx"])
+        s.set_stream(stream.cuda_stream)
+        s.set_params(cfg, prec)
+        s.upload(P0)
+        s.initial_pass()
+        return s
+
+    spin = int(round(args.spinup / cfg["dt_max"]))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(s, K, profile=False):
+        if profile:
+            s.set_profiling(True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        w0 = s.work_counters()
+        l0 = s.kernel_launches()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for k in range(K):
+                flush.zero_()
+                ev[k][0].record(stream)
+                s.advance_steps_async(1)
+                ev[k][1].record(stream)
+        s.synchronize()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        if world > 1:
+            torch.distributed.barrier()
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        w1 = s.work_counters()
+        phases = None
+        if profile:
+            phases = s.phase_times()
+            s.set_profiling(False)
+        return ms, wall, (w1[0] - w0[0], w1[1] - w0[1]), s.kernel_launches() - l0, phases
+
+    # ---- FP32 split path (the product)
+    s32 = make(slab.FP32_SPLIT)
+    s32.advance_steps(spin)
+    s32.advance_steps(args.warmup)
+    with ClockSampler(dev) as clk:
+        ms, wall, work, launches, _ = timed(s32, args.steps)
+    assert work[0] == Np * args.steps, work
+    ms_prof, _, work_prof, _, phases = timed(s32, args.steps, profile=True)
+    state = s32.particles()
+    t32 = s32.state()[0]
+
+    # ---- plain FP64 path on the same schedule
+    s64 = make(slab.FP64_PLAIN)
+    s64.advance_steps(spin)
+    s64.advance_steps(args.warmup)
+    ms64, _, work64, _, _ = timed(s64, args.steps)
+    state64 = s64.particles()
+    s64.close()
+
+    # ---- max over ranks
+    step_ms = ms / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_all = float(t.item())
+    else:
+        ms_all = ms
+    value = Np * args.steps * world / (ms_all * 1e-3)
+    if rank != 0:
+        return None
+
+    # ---- roofline of the dominant kernel (profiled pass, same schedule)
+    peak, peak_kind = measured_peak()
+    names = {2: "p2g", 3: "grid", 4: "g2p"}
+    nodes_per_step = work_prof[1] / args.steps
+    per_kernel = {}
+    for idx, nm in names.items():
+        t_ms = phases[idx] / args.steps
+        bp, bn = KERNEL_BYTES[nm]
+        bytes_launch = bp * Np + bn * nodes_per_step
+        per_kernel[nm] = {"ms": round(t_ms, 5), "algorithmic_bytes": int(bytes_launch),
+                          "gbs": round(bytes_launch / (t_ms * 1e-3) / 1e9, 1) if t_ms > 0 else None,
+                          "share": round(phases[idx] / max(sum(phases), 1e-12), 3)}
+    dom = max(names.values(), key=lambda k: per_kernel[k]["ms"])
+    ach = per_kernel[dom]["gbs"]
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", f"traffic_{args.workload}.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4) if ach else None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s", "traffic": traffic,
+                "whole_step": {"algorithmic_bytes": int(BYTES_P * Np + BYTES_N * nodes_per_step),
+                               "gbs": round((BYTES_P * Np + BYTES_N * nodes_per_step) / (step_ms * 1e-3) / 1e9, 1)},
+                "per_kernel": per_kernel, "active_nodes_per_step": round(nodes_per_step, 1)}
+
+    # ---- CPU baseline: the reference's own step loop, 1 core, same state
+    cpu = None
+    if not args.no_cpu:
+        try:
+            Pref = dict(state64)
+            Pref["theta"] = np.zeros(Np)
+            k_cpu = max(3, int(args.cpu_seconds * 8e6 / Np))
+            v_cpu, st_cpu, sec_cpu = run_reference(c, Pref, k_cpu, 1)
+            cpu = {"value": round(v_cpu, 1), "unit": METRIC, "cores": 1, "kind": "reference",
+                   "sample": f"{st_cpu} steps of the same {Np}-particle scenario from the same developed state, "
+                             f"reference step-loop sources (oracle/_ref/slab_ref), per-phase timers, {sec_cpu:.1f} s"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    # ---- e2e through the public API with host buffers
+    K_e2e = args.e2e_steps
+    hb = {k: np.ascontiguousarray(state[k]) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
+    e = slab.Slab(c["z"], c["dx"])
+    e.set_stream(stream.cuda_stream)
+    e.set_params(cfg, slab.FP32_SPLIT)
+    hm = np.zeros(c["z"].shape)
+    e2e_times = []
+    for it in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.upload(hb)
+        e.initial_pass()
+        e.advance_steps(K_e2e)
+        out = e.particles()
+        hmx, _ = e.max_maps()
+        e2e_times.append(time.perf_counter() - t0)
+    h2d = sum(hb[k].nbytes for k in hb)
+    d2h = sum(out[k].nbytes for k in out) + 2 * hmx.nbytes
+    e2e = {"value": round(Np * K_e2e / min(e2e_times), 1), "unit": METRIC,
+           "h2d_bytes_per_step": int(h2d / K_e2e), "d2h_bytes_per_step": int(d2h / K_e2e),
+           "window": f"upload + t=0 pass + {K_e2e} steps + particle and max-map download, host FP64 arrays, best of 2"}
+    e.close()
+
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_all / args.steps, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (f64 dt, time, metric terms, sums)", "data": "synthetic",
+        "config": {"workload": c["name"], "particles": Np, "dem": list(c["z"].shape), "dx": c["dx"],
+                   "friction": c["cfg"]["friction"], "spinup_s": args.spinup, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "fp64_plain": {"value": round(Np * args.steps / (ms64 * 1e-3), 1), "ms_per_step": round(ms64 / args.steps, 5),
+                       "fp32_speedup": round(ms64 / ms, 2)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "wall_s_timed": round(wall, 4),
+        "sim_time_s": round(t32, 4),
+    }
+    return line
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    import slab  # noqa: F401 (sampler for the workload)
+    c = load_workload(args.workload)
+    P = dict(c["particles"])
+    Np = len(P["h"])
+    replicas = max(1, min(os.cpu_count() or 1, args.ref_procs))
+    k = max(2, min(args.steps, int(args.cpu_seconds * 8e6 / Np)))
+    t0 = time.perf_counter()
+    v, st, sec = run_reference(c, P, k, replicas)
+    wall = time.perf_counter() - t0
+    return {"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": METRIC, "n_gpus": world, "steps": st,
+            "warmup": 0, "ms_per_step": round(sec / max(st, 1) * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": c["name"], "particles": Np, "dem": list(c["z"].shape), "dx": c["dx"],
+                       "friction": c["cfg"]["friction"], "parallelism": f"{replicas} concurrent single-threaded processes"},
+            "cpu_baseline": {"value": round(v, 1), "unit": METRIC, "cores": replicas, "kind": "reference",
+                             "sample": f"{st} steps from t=0 per process, {replicas} processes, per-phase timers "
+                                       f"(slowest {sec:.1f} s, wall {wall:.1f} s)"},
+            "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--spinup", type=float, default=2.0, help="simulated seconds before timing")
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-procs", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        log("warmup raised to 3")
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    try:
+        line = ours(args, rank, world) if args.impl == "ours" else reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

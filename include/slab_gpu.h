@@ -142,6 +142,14 @@ slab_status slab_advance_to_frame(slab_ctx* ctx, double* time_out, int32_t* fram
  * total_time. For benchmarks and tests. */
 slab_status slab_advance_steps(slab_ctx* ctx, int64_t nsteps, int64_t* steps_out);
 
+/* Enqueue nsteps iterations like slab_advance_steps on the context's stream
+ * and return without waiting. The work and any device error are observed by
+ * the next synchronising call (slab_synchronize or any download). */
+slab_status slab_advance_steps_async(slab_ctx* ctx, int64_t nsteps);
+
+/* Wait for the context's stream and report device-side errors. */
+slab_status slab_synchronize(slab_ctx* ctx);
+
 /* Copy the particle state back in the upload order (the reference reorders
  * particles every 50 steps, src/simulation.cpp:540; the engine keeps stable
  * ids instead). Any pointer may be NULL. A = mass/(h*rho) as in G2P
@@ -170,11 +178,28 @@ slab_status slab_get_state(slab_ctx* ctx, double* time, double* dt, int32_t* fra
 slab_status slab_set_profiling(slab_ctx* ctx, int32_t on);
 slab_status slab_get_phase_times(slab_ctx* ctx, double out[5]);
 
+/* Work done so far: out[0] = particle-steps (Np x completed steps),
+ * out[1] = active node-steps (grid nodes with mass > 1e-6, summed over the
+ * grid updates). These are the units of the roofline accounting. */
+slab_status slab_work_counters(slab_ctx* ctx, int64_t out[2]);
+
 /* Number of kernels this context has launched since creation. */
 int64_t slab_kernel_launches(const slab_ctx* ctx);
 
 const char* slab_last_error(const slab_ctx* ctx);
 void slab_destroy(slab_ctx* ctx);
+
+/* ---- setup utilities (host only; no device work) ---------------------- */
+
+/* Poisson-disk samples in [0,Lx] x [0,Ly] with minimum distance r and k
+ * candidates per active sample: the sampler of POISSON release sampling
+ * (class Poisson_disk, src/poisson_disk_sampling.hpp:23-134). seed 0 draws
+ * from the C library's rand() seeded with 1 -- the sequence the reference
+ * consumes -- so it reproduces the reference's samples; any other seed uses a
+ * seeded generator of this library. Positions are relative to the lower-left
+ * corner, as the reference returns them. With out_xy == NULL only *n_out is
+ * set; otherwise cap must be >= *n_out. */
+slab_status slab_poisson_disk(double Lx, double Ly, double r, int32_t k, uint64_t seed, double* out_xy, int64_t cap, int64_t* n_out);
 
 /* Library version string and status-code names. */
 const char* slab_version(void);

@@ -14,6 +14,16 @@
 //                                                layout as particles_frame_*.bin)
 //   slab_ref <config.json> --steps N            phase driver: t=0 pass + N steps
 //                                                dumped to <sim_dir>/steps.bin
+//   slab_ref <config.json> --dem-bin f.bin      replace the terrain after
+//                                                initializeTerrain by the DEM in
+//                                                f.bin (i64 Nx, i64 Ny, f64 dx,
+//                                                then Nx*Ny z doubles, i*Ny+j)
+//                                                through the public setTerrain /
+//                                                setDx / terrainGradients /
+//                                                terrainTheta (for large DEMs
+//                                                where ASCII parsing dominates)
+// With SLAB_REF_NO_DUMP=1 the output hooks write nothing, so timed runs
+// contain no file output.
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -24,6 +34,22 @@
 #include "simulation.hpp"
 
 using Sim = Simulation<double, Eigen::Matrix<double, 2, 1>>;
+
+static Grid load_dem(const char* path, double& dx) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) throw std::runtime_error(std::string("cannot open ") + path);
+    int64_t n[2];
+    if (std::fread(n, sizeof n, 1, f) != 1 || std::fread(&dx, sizeof dx, 1, f) != 1) throw std::runtime_error("short DEM file");
+    Grid g(static_cast<int>(n[0]), static_cast<int>(n[1]));
+    for (int i = 0; i < g.Nx; ++i) g.x[i] = i * dx;
+    for (int j = 0; j < g.Ny; ++j) g.y[j] = j * dx;
+    const size_t cnt = static_cast<size_t>(n[0]) * static_cast<size_t>(n[1]);
+    if (std::fread(g.z.data(), sizeof(double), cnt, f) != cnt) throw std::runtime_error("short DEM file");
+    std::fclose(f);
+    g.xllcorner = 0.;
+    g.yllcorner = 0.;
+    return g;
+}
 
 static Particles load_particles(const char* path, int& Np_out) {
     FILE* f = std::fopen(path, "rb");
@@ -63,6 +89,7 @@ int main(int argc, char** argv) {
         return 1;
     }
     const char* particles_file = nullptr;
+    const char* dem_file = nullptr;
     bool init_only = false;
     int steps = -1;
     for (int a = 2; a < argc; ++a) {
@@ -70,6 +97,8 @@ int main(int argc, char** argv) {
             init_only = true;
         else if (!std::strcmp(argv[a], "--particles") && a + 1 < argc)
             particles_file = argv[++a];
+        else if (!std::strcmp(argv[a], "--dem-bin") && a + 1 < argc)
+            dem_file = argv[++a];
         else if (!std::strcmp(argv[a], "--steps") && a + 1 < argc)
             steps = std::atoi(argv[++a]);
         else {
@@ -82,6 +111,14 @@ int main(int argc, char** argv) {
         sim.loadFromJSON(argv[1]);
         sim.initialize();
         sim.initializeTerrain();
+        if (dem_file) {
+            double dx = 0;
+            Grid g = load_dem(dem_file, dx);
+            sim.setDx(dx);
+            sim.setTerrain(g);
+            sim.terrainGradients();
+            sim.terrainTheta();
+        }
         if (particles_file) {
             int Np = 0;
             Particles p = load_particles(particles_file, Np);

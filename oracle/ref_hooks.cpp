@@ -70,7 +70,13 @@ std::string frame_name(const char* stem, int padding, int frame, const char* ext
 
 }  // namespace
 
+static bool no_dump() {
+    const char* e = std::getenv("SLAB_REF_NO_DUMP");
+    return e && e[0] == '1';
+}
+
 template <typename T_, typename TV2_> void Simulation<T_, TV2_>::saveParticleData() const {
+    if (no_dump()) return;
     Out o(particle_path / frame_name("particles_frame_", padding, frame, ".bin"));
     o.i64(Np);
     o.i64(frame);
@@ -87,6 +93,7 @@ template <typename T_, typename TV2_> void Simulation<T_, TV2_>::saveParticleDat
 }
 
 template <typename T_, typename TV2_> void Simulation<T_, TV2_>::saveGridData() const {
+    if (no_dump()) return;
     Out o(raster_path / frame_name("rasters_frame_", padding, frame, ".bin"));
     const size_t n = static_cast<size_t>(grid.Nx) * grid.Ny;
     o.i64(grid.Nx);
@@ -104,6 +111,7 @@ template <typename T_, typename TV2_> void Simulation<T_, TV2_>::saveGridData() 
 }
 
 template <typename T_, typename TV2_> void Simulation<T_, TV2_>::saveMaxData() const {
+    if (no_dump()) return;
     Out o(sim_dir_path / "max_values.bin");
     const size_t n = static_cast<size_t>(terrain.Nx) * terrain.Ny;
     o.i64(terrain.Nx);

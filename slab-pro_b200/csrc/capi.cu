@@ -101,18 +101,27 @@ void raise_device_errors(slab_ctx* c) {
     if (e & ERR_TIMEOUT) throw Error{SLAB_E_TIMEOUT, "bounded device wait gave up"};
 }
 
+void enqueue_nsteps(slab_ctx* c, int64_t nsteps) {
+    k_arm<<<1, 32, 0, c->stream>>>(c->d_ctl, nsteps, 0);
+    SLAB_CUDA(cudaGetLastError());
+    ++c->extra_launches;
+    int64_t k = 0;
+    for (; k + c->chunk <= nsteps; k += c->chunk) c->path->enqueue_steps(c->chunk);
+    if (k < nsteps) c->path->enqueue_steps((int)(nsteps - k));
+}
+
 void advance(slab_ctx* c, int64_t nsteps, bool stop_at_frame, int64_t* steps_out) {
     need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
     pull_ctl(c);
     const int64_t s0 = c->h_ctl->steps;
-    k_arm<<<1, 32, 0, c->stream>>>(c->d_ctl, nsteps, stop_at_frame ? 1 : 0);
-    SLAB_CUDA(cudaGetLastError());
-    ++c->extra_launches;
     if (!stop_at_frame) {
         // the step budget is on the device: enqueue enough chunks, sync once
-        for (int64_t k = 0; k < nsteps; k += c->chunk) c->path->enqueue_steps(c->chunk);
+        enqueue_nsteps(c, nsteps);
         pull_ctl(c);
     } else {
+        k_arm<<<1, 32, 0, c->stream>>>(c->d_ctl, nsteps, 1);
+        SLAB_CUDA(cudaGetLastError());
+        ++c->extra_launches;
         double last_time = c->h_ctl->time;
         int stalled = 0;
         for (;;) {
@@ -260,6 +269,23 @@ slab_status slab_advance_steps(slab_ctx* c, int64_t nsteps, int64_t* steps_out) 
     });
 }
 
+slab_status slab_advance_steps_async(slab_ctx* c, int64_t nsteps) {
+    if (!c) return SLAB_E_ARG;
+    return guard(c, [&] {
+        need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
+        need(nsteps >= 0, SLAB_E_ARG, "nsteps must be >= 0");
+        enqueue_nsteps(c, nsteps);
+    });
+}
+
+slab_status slab_synchronize(slab_ctx* c) {
+    if (!c) return SLAB_E_ARG;
+    return guard(c, [&] {
+        pull_ctl(c);
+        raise_device_errors(c);
+    });
+}
+
 slab_status slab_download_particles(slab_ctx* c, double* x, double* v, double* vz, double* h, double* A, double* m, double* z) {
     if (!c) return SLAB_E_ARG;
     return guard(c, [&] {
@@ -317,6 +343,16 @@ slab_status slab_get_phase_times(slab_ctx* c, double out[5]) {
     return guard(c, [&] {
         need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
         c->path->phase_times(out);
+    });
+}
+
+slab_status slab_work_counters(slab_ctx* c, int64_t out[2]) {
+    if (!c || !out) return SLAB_E_ARG;
+    return guard(c, [&] {
+        need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
+        pull_ctl(c);
+        out[0] = c->h_ctl->steps * (int64_t)c->Np;
+        out[1] = (int64_t)c->h_ctl->node_steps;
     });
 }
 

@@ -45,6 +45,7 @@ struct Ctl {
     int32_t box[4];
     uint32_t done_blocks;  // last-block-done counter
     int32_t keep_outputs;  // write grid output fields every step (tests); else frame steps only
+    unsigned long long node_steps;  // grid nodes with mass > 1e-6, summed over all steps so far
 };
 
 // The reference's remesh box from the particle bounding box

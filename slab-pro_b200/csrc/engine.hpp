@@ -4,6 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
+#include <functional>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -54,6 +57,86 @@ struct Terrain {
     dptr<double2> grad;    // cell gradient stored at the bottom-left node
     dptr<double> cos_t;    // cos(atan|grad|)
     dptr<float4> dem32;    // FP32 copy for the split path: gx, gy, cos(theta), z
+};
+
+// CUDA graphs of `chunk` consecutive steps, one per chunk size used.
+struct StepGraphs {
+    std::map<int, cudaGraphExec_t> g;
+    ~StepGraphs() { clear(); }
+    void clear() {
+        for (auto& kv : g) cudaGraphExecDestroy(kv.second);
+        g.clear();
+    }
+    void launch(int chunk, cudaStream_t st, const std::function<void()>& one_step) {
+        auto it = g.find(chunk);
+        if (it == g.end()) {
+            cudaGraph_t gr;
+            SLAB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < chunk; ++k) one_step();
+            SLAB_CUDA(cudaStreamEndCapture(st, &gr));
+            cudaGraphExec_t ex;
+            cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+            cudaGraphDestroy(gr);
+            SLAB_CUDA(e);
+            it = g.emplace(chunk, ex).first;
+        }
+        SLAB_CUDA(cudaGraphLaunch(it->second, st));
+    }
+};
+
+// Per-kernel device times of profiled steps: events between the 4 kernels of
+// each step, read back lazily. Phases: 0 begin/dt, 1 (unused: binning is
+// fused into G2P), 2 P2G, 3 grid update, 4 G2P.
+struct PhaseTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::array<int, 5>> pending;
+    size_t used = 0;
+    double acc[5] = {0, 0, 0, 0, 0};
+    int64_t steps = 0;
+    ~PhaseTimer() {
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+    void reset() {
+        pending.clear();
+        used = 0;
+        for (double& a : acc) a = 0;
+        steps = 0;
+    }
+    int mark(cudaStream_t st) {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            SLAB_CUDA(cudaEventCreate(&e));
+            pool.push_back(e);
+        }
+        SLAB_CUDA(cudaEventRecord(pool[used], st));
+        return (int)used++;
+    }
+    // launches: 4 callables, one per kernel of the step
+    void profiled_step(cudaStream_t st, const std::function<void(int)>& launch_kernel) {
+        std::array<int, 5> ev;
+        ev[0] = mark(st);
+        for (int k = 0; k < 4; ++k) {
+            launch_kernel(k);
+            ev[k + 1] = mark(st);
+        }
+        pending.push_back(ev);
+    }
+    void collect() {
+        if (pending.empty()) return;
+        SLAB_CUDA(cudaEventSynchronize(pool[pending.back()[4]]));
+        static const int phase_of[4] = {0, 2, 3, 4};
+        for (auto& ev : pending) {
+            for (int k = 0; k < 4; ++k) {
+                float ms = 0;
+                SLAB_CUDA(cudaEventElapsedTime(&ms, pool[ev[k]], pool[ev[k + 1]]));
+                acc[phase_of[k]] += ms;
+            }
+            ++steps;
+        }
+        pending.clear();
+        used = 0;
+    }
 };
 
 struct Path {

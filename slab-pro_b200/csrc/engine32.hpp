@@ -1,0 +1,69 @@
+// Host object that owns the device state of one or many FP32 split-precision
+// scenarios on a shared terrain and launches their steps together.
+#pragma once
+
+#include <deque>
+#include <vector>
+
+#include "engine.hpp"
+#include "split32.cuh"
+
+namespace slab {
+
+class Engine32 {
+  public:
+    struct Store {
+        int Np = 0;
+        int act_cap = 0;
+        Ctl* ctl = nullptr;
+        Ctl* h_ctl = nullptr;
+        double mass_fp64 = 0;
+        dptr<int32_t> cell[2], id[2], grp[2], grp_stamp[2], act_list[2];
+        dptr<float2> f[2], v[2];
+        dptr<float> h[2], m[2], vz[2], z[2];
+        dptr<int32_t> act_stamp, slot_of, nxt_off, gt_stamp, gt_list, blk_of;
+        dptr<float> part;
+        dptr<SCnt> cnt;
+    };
+
+    Engine32(const Terrain& t, cudaStream_t s, int max_scenarios, int64_t blk_cap);
+    ~Engine32();
+
+    int add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, const double* x, const double* v, const double* vz,
+                     const double* h, const double* m, const double* z);
+    void launch_begin(int t0);
+    void launch_t0();
+    void launch_step();
+    void launch_kernel(int k, const Shared& sh);
+    void enqueue_steps(int chunk);
+    PhaseTimer timer;
+    SCnt counters(int sid);
+    void download_particles(int sid, double* x, double* v, double* vz, double* h, double* A, double* m, double* z, double rho);
+    void download_grid(int sid, slab_grid_view* gv);
+    void download_max(int sid, double* hmax, double* vmax2);
+    void conservation(int sid, double out[4], double rho);
+    Shared shared() const;
+
+    const Terrain& T;
+    cudaStream_t st;
+    int max_scn;
+    int nscn = 0;
+    int TX = 0, TY = 0, ntiles = 0;
+    int blk_cap = 0;
+    int grid_p2g = 0, grid_g2p = 0, grid_grid = 0;
+    int64_t nlaunch = 0;
+    std::deque<Store> stores;
+    std::vector<Scn> host_scn;
+
+  private:
+    std::vector<float> gather_nodes(int sid, int stepid, int i0, int j0, int nI, int nJ, const std::vector<const float*>& fields,
+                                    bool with_v);
+    dptr<float4> d_nv;
+    dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz;
+    dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_grid_pref;
+    dptr<Scn> d_scn;
+    StepGraphs graphs;
+    int graph_nscn = 0;
+};
+
+}  // namespace slab

@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(256) k64_p2g(const Ctl* __restrict__ c, P64 p,
 
 // computeGridVelocity (src/simulation.cpp:800-875) over the remesh box, then
 // the accumulators are zeroed for the next step.
-__global__ void __launch_bounds__(256) k64_grid(const Ctl* __restrict__ c, N64 n, const double2* __restrict__ grad,
+__global__ void __launch_bounds__(256) k64_grid(Ctl* c, N64 n, const double2* __restrict__ grad,
                                                 const double* __restrict__ cos_t, Phys P) {
     if (!c->active) return;
     const int i0 = c->box[0], j0 = c->box[2];
@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(256) k64_grid(const Ctl* __restrict__ c, N64 n
     const int64_t total = (int64_t)nI * nJ;
     const double dt = c->dt;
     const bool outs = c->write_outputs;
+    unsigned nact = 0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int i = i0 + (int)(t / nJ), j = j0 + (int)(t % nJ);
         const int64_t k = (int64_t)i * P.Ny + j;
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(256) k64_grid(const Ctl* __restrict__ c, N64 n
                 }
             }
             fl = make_double2(nv.x - vox, nv.y - voy);
+            ++nact;
             if (n.h_max[k] < hn) n.h_max[k] = hn;
             const double v2 = nv.x * nv.x + nv.y * nv.y;
             if (n.v_max2[k] < v2) n.v_max2[k] = v2;
@@ -169,6 +171,8 @@ __global__ void __launch_bounds__(256) k64_grid(const Ctl* __restrict__ c, N64 n
         n.Fx[k] = 0.0;
         n.Fy[k] = 0.0;
     }
+    for (int o = 16; o > 0; o >>= 1) nact += __shfl_xor_sync(0xffffffffu, nact, o);
+    if ((threadIdx.x & 31) == 0 && nact) atomicAdd(&c->node_steps, (unsigned long long)nact);
 }
 
 __device__ __forceinline__ uint64_t dbits(double v) { return (uint64_t)__double_as_longlong(v); }
@@ -301,8 +305,8 @@ struct Plain64 final : Path {
     dptr<double> out3;  // out_h, out_m, out_vz
     dptr<double> maxes; // h_max, v_max2
     int64_t nlaunch = 0;
-    cudaGraphExec_t graph = nullptr;
-    int graph_chunk = 0;
+    StepGraphs graphs;
+    PhaseTimer timer;
 
     Plain64(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d, Ctl* h_) : T(t), prm(p), st(s), dc(d), hc(h_) {
         P.g = p.gravity;
@@ -332,9 +336,6 @@ struct Plain64 final : Path {
         SLAB_CUDA(cudaMemsetAsync(gflip.get(), 0, nn * sizeof(double2), st));
         SLAB_CUDA(cudaMemsetAsync(out3.get(), 0, 3 * nn * sizeof(double), st));
         SLAB_CUDA(cudaMemsetAsync(maxes.get(), 0, 2 * nn * sizeof(double), st));
-    }
-    ~Plain64() override {
-        if (graph) cudaGraphExecDestroy(graph);
     }
 
     P64 parts() { return P64{x.get(), v.get(), vz.get(), h.get(), A.get(), m.get(), z.get()}; }
@@ -368,20 +369,22 @@ struct Plain64 final : Path {
         SLAB_CUDA(cudaGetLastError());
         ++nlaunch;
         SLAB_CUDA(cudaMemcpyAsync(&dc->vmax2_bits, &dc->vmax2_acc, sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
-        if (graph) {
-            cudaGraphExecDestroy(graph);
-            graph = nullptr;
-        }
+        graphs.clear();
     }
 
     int grid_blocks() const { return 148 * 4; }
 
-    void launch_step() {
+    void launch_kernel(int k) {
         const int pb = (Np + 255) / 256;
-        k64_begin<<<1, 32, 0, st>>>(dc, T.Nx, T.Ny);
-        k64_p2g<<<pb, 256, 0, st>>>(dc, parts(), nodes(), T.grad.get(), T.cos_t.get(), P, Np);
-        k64_grid<<<grid_blocks(), 256, 0, st>>>(dc, nodes(), T.grad.get(), T.cos_t.get(), P);
-        k64_g2p<<<pb, 256, 0, st>>>(dc, parts(), nodes(), T.grad.get(), T.z.get(), P, Np);
+        switch (k) {
+            case 0: k64_begin<<<1, 32, 0, st>>>(dc, T.Nx, T.Ny); break;
+            case 1: k64_p2g<<<pb, 256, 0, st>>>(dc, parts(), nodes(), T.grad.get(), T.cos_t.get(), P, Np); break;
+            case 2: k64_grid<<<grid_blocks(), 256, 0, st>>>(dc, nodes(), T.grad.get(), T.cos_t.get(), P); break;
+            case 3: k64_g2p<<<pb, 256, 0, st>>>(dc, parts(), nodes(), T.grad.get(), T.z.get(), P, Np); break;
+        }
+    }
+    void launch_step() {
+        for (int k = 0; k < 4; ++k) launch_kernel(k);
     }
 
     void initial_pass() override {
@@ -393,20 +396,22 @@ struct Plain64 final : Path {
     }
 
     void enqueue_steps(int chunk) override {
-        if (!graph || graph_chunk != chunk) {
-            if (graph) cudaGraphExecDestroy(graph);
-            graph = nullptr;
-            cudaGraph_t g;
-            SLAB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            for (int k = 0; k < chunk; ++k) launch_step();
-            SLAB_CUDA(cudaStreamEndCapture(st, &g));
-            cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
-            cudaGraphDestroy(g);
-            SLAB_CUDA(e);
-            graph_chunk = chunk;
+        if (timer.on) {
+            for (int k = 0; k < chunk; ++k) timer.profiled_step(st, [&](int kk) { launch_kernel(kk); });
+            SLAB_CUDA(cudaGetLastError());
+        } else {
+            graphs.launch(chunk, st, [&] { launch_step(); });
         }
-        SLAB_CUDA(cudaGraphLaunch(graph, st));
         nlaunch += 4 * chunk;
+    }
+    void set_profiling(bool on) override {
+        timer.collect();
+        timer.reset();
+        timer.on = on;
+    }
+    void phase_times(double out[5]) override {
+        timer.collect();
+        for (int k = 0; k < 5; ++k) out[k] = timer.acc[k];
     }
 
     void download_particles(double* hx, double* hv, double* hvz, double* hh, double* hA, double* hm, double* hz) override {

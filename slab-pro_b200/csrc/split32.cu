@@ -1,6 +1,459 @@
+// Host side of the FP32 split-precision step loop: per-scenario device
+// storage, particle upload (binning into tiles), step launch / CUDA-graph
+// capture, and downloads that restore the reference layouts.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "engine.hpp"
+#include "engine32.hpp"
+#include "split32_kernels.cuh"
+
 namespace slab {
-std::unique_ptr<Path> make_split32(const Terrain&, const slab_params&, cudaStream_t, Ctl*, Ctl*) {
-    throw Error{SLAB_E_ARG, "FP32_SPLIT path not built yet"};
+
+namespace {
+template <typename T> void h2d(T* d, const T* h, size_t n, cudaStream_t s) {
+    if (n) SLAB_CUDA(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
 }
+template <typename T> void d2h(T* h, const T* d, size_t n, cudaStream_t s) {
+    if (n) SLAB_CUDA(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+}
+}  // namespace
+
+namespace k32 {
+
+// Dense copies of per-block node fields for downloads: node (i, j) of the box
+// [i0, i0+nI) x [j0, j0+nJ) reads the block of its owner tile if that block
+// was updated at `stepid` (any stamp if stepid < 0), else 0.
+__global__ void k_gather_nodes(const int32_t* __restrict__ blk_of, const int32_t* __restrict__ blk_stamp, int stepid, int TY, int i0,
+                               int j0, int nI, int nJ, int nf, const float* const* __restrict__ fields, const float4* __restrict__ nv,
+                               float* __restrict__ out) {
+    const int64_t total = (int64_t)nI * nJ;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        const int i = i0 + (int)(k / nJ), j = j0 + (int)(k % nJ);
+        const int blk = blk_of[(i / TILE) * TY + (j / TILE)];
+        const bool ok = blk >= 0 && (stepid < 0 || blk_stamp[blk] == stepid);
+        const size_t n = (size_t)blk * NCELL + (i % TILE) * TILE + (j % TILE);
+        for (int q = 0; q < nf; ++q) out[q * total + k] = ok ? fields[q][n] : 0.f;
+        if (nv) {
+            const float4 v = ok ? nv[n] : make_float4(0.f, 0.f, 0.f, 0.f);
+            out[nf * total + k] = v.x;
+            out[(nf + 1) * total + k] = v.y;
+        }
+    }
+}
+
+}  // namespace k32
+
+Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_cap) : T(t), st(s), max_scn(max_scn) {
+    TX = (t.Nx + TILE - 1) / TILE;
+    TY = (t.Ny + TILE - 1) / TILE;
+    ntiles = TX * TY;
+    this->blk_cap = (int)std::min<int64_t>(blk_cap, INT32_MAX);
+    d_nv = dalloc<float4>((size_t)this->blk_cap * NCELL);
+    d_hmax = dalloc<float>((size_t)this->blk_cap * NCELL);
+    d_vmax2 = dalloc<float>((size_t)this->blk_cap * NCELL);
+    d_oh = dalloc<float>((size_t)this->blk_cap * NCELL);
+    d_om = dalloc<float>((size_t)this->blk_cap * NCELL);
+    d_ovz = dalloc<float>((size_t)this->blk_cap * NCELL);
+    d_blk_stamp = dalloc<int32_t>(this->blk_cap);
+    d_blk_owner = dalloc<int32_t>(this->blk_cap);
+    d_misc = dalloc<int32_t>(8);
+    d_work_pref = dalloc<int32_t>(max_scn + 1);
+    d_grid_pref = dalloc<int32_t>(max_scn + 1);
+    d_scn = dalloc<Scn>(max_scn);
+    SLAB_CUDA(cudaMemsetAsync(d_hmax.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
+    SLAB_CUDA(cudaMemsetAsync(d_vmax2.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
+    SLAB_CUDA(cudaMemsetAsync(d_blk_stamp.get(), 0xff, (size_t)this->blk_cap * sizeof(int32_t), st));
+    SLAB_CUDA(cudaMemsetAsync(d_misc.get(), 0, 8 * sizeof(int32_t), st));
+    SLAB_CUDA(cudaMemsetAsync(d_work_pref.get(), 0, (max_scn + 1) * sizeof(int32_t), st));
+    SLAB_CUDA(cudaMemsetAsync(d_grid_pref.get(), 0, (max_scn + 1) * sizeof(int32_t), st));
+    host_scn.resize(max_scn);
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
+    int dev = 0, sms = 0, occ_p = 0, occ_g = 0, occ_u = 0;
+    SLAB_CUDA(cudaGetDevice(&dev));
+    SLAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g, NCELL, sizeof(k32::P2GSmem)));
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, k32::k_g2p, NCELL, 0));
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k32::k_grid, NCELL, 0));
+    grid_p2g = sms * std::max(occ_p, 1);
+    grid_g2p = sms * std::max(occ_g, 1);
+    grid_grid = sms * std::max(occ_u, 1);
+}
+
+Engine32::~Engine32() {}
+
+Shared Engine32::shared() const {
+    Shared sh{};
+    sh.Nx = T.Nx;
+    sh.Ny = T.Ny;
+    sh.TX = TX;
+    sh.TY = TY;
+    sh.dem = T.dem32.get();
+    sh.nv = d_nv.get();
+    sh.hmax = d_hmax.get();
+    sh.vmax2 = d_vmax2.get();
+    sh.oh = d_oh.get();
+    sh.om = d_om.get();
+    sh.ovz = d_ovz.get();
+    sh.blk_stamp = d_blk_stamp.get();
+    sh.blk_owner = d_blk_owner.get();
+    sh.blk_count = d_misc.get();
+    sh.blk_cap = blk_cap;
+    sh.nscn = nscn;
+    sh.scn = d_scn.get();
+    sh.work_pref = d_work_pref.get();
+    sh.grid_pref = d_grid_pref.get();
+    sh.done = reinterpret_cast<uint32_t*>(d_misc.get() + 2);
+    return sh;
+}
+
+int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, const double* x, const double* v, const double* vz,
+                           const double* h, const double* m, const double* z) {
+    if (nscn >= max_scn) throw Error{SLAB_E_OOM, "scenario capacity exceeded"};
+    const int sid = nscn;
+    Store& S = stores.emplace_back();
+    S.Np = Np;
+    S.ctl = ctl;
+    S.h_ctl = h_ctl;
+    S.act_cap = std::max(1, std::min(ntiles, Np));
+    for (int b = 0; b < 2; ++b) {
+        S.cell[b] = dalloc<int32_t>(Np);
+        S.f[b] = dalloc<float2>(Np);
+        S.v[b] = dalloc<float2>(Np);
+        S.h[b] = dalloc<float>(Np);
+        S.m[b] = dalloc<float>(Np);
+        S.id[b] = dalloc<int32_t>(Np);
+        S.vz[b] = dalloc<float>(Np);
+        S.z[b] = dalloc<float>(Np);
+        S.grp[b] = dalloc<int32_t>((size_t)ntiles * 10);
+        S.grp_stamp[b] = dalloc<int32_t>(ntiles);
+        S.act_list[b] = dalloc<int32_t>(S.act_cap);
+    }
+    S.act_stamp = dalloc<int32_t>(ntiles);
+    S.slot_of = dalloc<int32_t>(ntiles);
+    S.nxt_off = dalloc<int32_t>(ntiles);
+    S.gt_stamp = dalloc<int32_t>(ntiles);
+    S.gt_list = dalloc<int32_t>(ntiles);
+    S.blk_of = dalloc<int32_t>(ntiles);
+    S.part = dalloc<float>((size_t)S.act_cap * PART_STRIDE);
+    S.cnt = dalloc<SCnt>(1);
+
+    // ---- bin particles into tiles (stable in upload order)
+    const double dx = T.dx, ood = 1.0 / T.dx;
+    std::vector<int32_t> cell(Np), tile(Np);
+    std::vector<float2> f(Np);
+    double mnx = INFINITY, mxx = 0, mny = INFINITY, mxy = 0, vv = 0;
+    for (int q = 0; q < Np; ++q) {
+        const double ux = x[2 * q] * ood, uy = x[2 * q + 1] * ood;
+        int ib = (int)std::floor(ux - 0.5), jb = (int)std::floor(uy - 0.5);
+        float fx = (float)(ux - ib), fy = (float)(uy - jb);
+        if (fx >= 1.5f) { ++ib; fx -= 1.f; }
+        if (fy >= 1.5f) { ++jb; fy -= 1.f; }
+        if (ib < 0 || jb < 0 || ib + 2 > T.Nx - 1 || jb + 2 > T.Ny - 1) throw Error{SLAB_E_DOMAIN, "particle stencil outside the terrain"};
+        cell[q] = pack_cell(ib, jb);
+        f[q] = make_float2(fx, fy);
+        tile[q] = (ib / TILE) * TY + (jb / TILE);
+        const double px = ((double)ib + (double)fx) * dx, py = ((double)jb + (double)fy) * dx;
+        mnx = std::min(mnx, px);
+        mxx = std::max(mxx, px);
+        mny = std::min(mny, py);
+        mxy = std::max(mxy, py);
+        const float vx = (float)v[2 * q], vy = (float)v[2 * q + 1];
+        vv = std::max(vv, (double)(vx * vx + vy * vy));
+    }
+    std::vector<int32_t> cnt(ntiles, 0), start(ntiles + 1, 0);
+    for (int q = 0; q < Np; ++q) cnt[tile[q]]++;
+    for (int t = 0; t < ntiles; ++t) start[t + 1] = start[t] + cnt[t];
+    std::vector<int32_t> pos(start.begin(), start.end() - 1);
+    std::vector<int32_t> o_cell(Np), o_id(Np);
+    std::vector<float2> o_f(Np), o_v(Np);
+    std::vector<float> o_h(Np), o_m(Np), o_vz(Np), o_z(Np);
+    for (int q = 0; q < Np; ++q) {
+        const int k = pos[tile[q]]++;
+        o_cell[k] = cell[q];
+        o_f[k] = f[q];
+        o_v[k] = make_float2((float)v[2 * q], (float)v[2 * q + 1]);
+        o_h[k] = (float)h[q];
+        o_m[k] = (float)m[q];
+        o_vz[k] = (float)vz[q];
+        o_z[k] = (float)z[q];
+        o_id[k] = q;
+    }
+    std::vector<int32_t> grp((size_t)ntiles * 10, 0), gstamp(ntiles, -1), astamp(ntiles, -1), alist;
+    for (int t = 0; t < ntiles; ++t) {
+        if (!cnt[t]) continue;
+        for (int d = 0; d < 10; ++d) grp[(size_t)t * 10 + d] = d <= 4 ? start[t] : start[t + 1];
+        gstamp[t] = 0;
+        astamp[t] = 0;
+        alist.push_back(t);
+    }
+    if ((int)alist.size() > S.act_cap) throw Error{SLAB_E_OOM, "active tile capacity"};
+    h2d(S.cell[0].get(), o_cell.data(), Np, st);
+    h2d(S.f[0].get(), o_f.data(), Np, st);
+    h2d(S.v[0].get(), o_v.data(), Np, st);
+    h2d(S.h[0].get(), o_h.data(), Np, st);
+    h2d(S.m[0].get(), o_m.data(), Np, st);
+    h2d(S.id[0].get(), o_id.data(), Np, st);
+    h2d(S.vz[0].get(), o_vz.data(), Np, st);
+    h2d(S.z[0].get(), o_z.data(), Np, st);
+    h2d(S.grp[0].get(), grp.data(), grp.size(), st);
+    h2d(S.grp_stamp[0].get(), gstamp.data(), ntiles, st);
+    SLAB_CUDA(cudaMemsetAsync(S.grp_stamp[1].get(), 0xff, ntiles * sizeof(int32_t), st));
+    h2d(S.act_stamp.get(), astamp.data(), ntiles, st);
+    h2d(S.act_list[0].get(), alist.data(), alist.size(), st);
+    SLAB_CUDA(cudaMemsetAsync(S.gt_stamp.get(), 0xff, ntiles * sizeof(int32_t), st));
+    SLAB_CUDA(cudaMemsetAsync(S.blk_of.get(), 0xff, ntiles * sizeof(int32_t), st));
+    SCnt c0{};
+    c0.act_count[0] = (int)alist.size();
+    c0.t0_pending = 1;
+    h2d(S.cnt.get(), &c0, 1, st);
+    // particle box and max speed for the first step (Simulation::updateDt / remesh)
+    h_ctl->pos_acc[0] = (uint64_t)__builtin_bit_cast(uint64_t, mnx);
+    h_ctl->pos_acc[1] = (uint64_t)__builtin_bit_cast(uint64_t, mxx);
+    h_ctl->pos_acc[2] = (uint64_t)__builtin_bit_cast(uint64_t, mny);
+    h_ctl->pos_acc[3] = (uint64_t)__builtin_bit_cast(uint64_t, mxy);
+    h_ctl->vmax2_bits = (uint64_t)__builtin_bit_cast(uint64_t, vv);
+    h2d(ctl, h_ctl, 1, st);
+    double msum = 0;
+    for (int q = 0; q < Np; ++q) msum += m[q];
+    S.mass_fp64 = msum;
+
+    Scn& D = host_scn[sid];
+    D = Scn{};
+    D.ctl = ctl;
+    D.cnt = S.cnt.get();
+    D.g = (float)p.gravity;
+    D.rho = (float)p.rho;
+    D.fr = (float)p.flip_ratio;
+    D.ood = (float)ood;
+    D.fric = p.friction.type;
+    D.mu_c = (float)p.friction.coulomb_mu;
+    D.mu_v = (float)p.friction.voellmy_mu;
+    D.xi = (float)p.friction.voellmy_xi;
+    D.mu1 = (float)p.friction.mu_1;
+    D.mu2 = (float)p.friction.mu_2;
+    D.I0 = (float)p.friction.I0;
+    D.d = (float)p.friction.d;
+    D.phi = (float)p.friction.phi;
+    D.Np = Np;
+    for (int b = 0; b < 2; ++b) {
+        D.buf[b] = PBuf{S.cell[b].get(), S.f[b].get(), S.v[b].get(), S.h[b].get(), S.m[b].get(), S.id[b].get(), S.vz[b].get(), S.z[b].get()};
+        D.grp[b] = S.grp[b].get();
+        D.grp_stamp[b] = S.grp_stamp[b].get();
+        D.act_list[b] = S.act_list[b].get();
+    }
+    D.act_stamp = S.act_stamp.get();
+    D.slot_of = S.slot_of.get();
+    D.nxt_off = S.nxt_off.get();
+    D.gt_stamp = S.gt_stamp.get();
+    D.gt_list = S.gt_list.get();
+    D.blk_of = S.blk_of.get();
+    D.part = S.part.get();
+    D.act_cap = S.act_cap;
+    h2d(d_scn.get() + sid, &D, 1, st);
+    nscn += 1;
+    graphs.clear();
+    return sid;
+}
+
+void Engine32::launch_begin(int t0) {
+    k32::k_begin<<<1, 1024, 0, st>>>(shared(), t0);
+    SLAB_CUDA(cudaGetLastError());
+}
+
+void Engine32::launch_t0() {
+    const Shared sh = shared();
+    k32::k_begin<<<1, 1024, 0, st>>>(sh, 1);
+    k32::k_p2g<<<grid_p2g, NCELL, sizeof(k32::P2GSmem), st>>>(sh);
+    k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
+    SLAB_CUDA(cudaGetLastError());
+    nlaunch += 3;
+}
+
+void Engine32::launch_kernel(int k, const Shared& sh) {
+    switch (k) {
+        case 0: k32::k_begin<<<1, 1024, 0, st>>>(sh, 0); break;
+        case 1: k32::k_p2g<<<grid_p2g, NCELL, sizeof(k32::P2GSmem), st>>>(sh); break;
+        case 2: k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh); break;
+        case 3: k32::k_g2p<<<grid_g2p, NCELL, 0, st>>>(sh, T.z.get()); break;
+    }
+}
+
+void Engine32::launch_step() {
+    const Shared sh = shared();
+    for (int k = 0; k < 4; ++k) launch_kernel(k, sh);
+}
+
+void Engine32::enqueue_steps(int chunk) {
+    if (graph_nscn != nscn) {
+        graphs.clear();
+        graph_nscn = nscn;
+    }
+    if (timer.on) {
+        const Shared sh = shared();
+        for (int k = 0; k < chunk; ++k) timer.profiled_step(st, [&](int kk) { launch_kernel(kk, sh); });
+        SLAB_CUDA(cudaGetLastError());
+    } else {
+        graphs.launch(chunk, st, [&] { launch_step(); });
+    }
+    nlaunch += 4 * chunk;
+}
+
+SCnt Engine32::counters(int sid) {
+    SCnt c;
+    d2h(&c, stores[sid].cnt.get(), 1, st);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    return c;
+}
+
+void Engine32::download_particles(int sid, double* x, double* v, double* vz, double* h, double* A, double* m, double* z, double rho) {
+    Store& S = stores[sid];
+    const SCnt c = counters(sid);
+    const int b = c.seq & 1;
+    const int Np = S.Np;
+    std::vector<int32_t> cell(Np), id(Np);
+    std::vector<float2> f(Np), vv(Np);
+    std::vector<float> hh(Np), mm(Np), vzz(Np), zz(Np);
+    d2h(cell.data(), S.cell[b].get(), Np, st);
+    d2h(id.data(), S.id[b].get(), Np, st);
+    d2h(f.data(), S.f[b].get(), Np, st);
+    d2h(vv.data(), S.v[b].get(), Np, st);
+    d2h(hh.data(), S.h[b].get(), Np, st);
+    d2h(mm.data(), S.m[b].get(), Np, st);
+    d2h(vzz.data(), S.vz[b].get(), Np, st);
+    d2h(zz.data(), S.z[b].get(), Np, st);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    const double dx = T.dx;
+    for (int k = 0; k < Np; ++k) {
+        const int q = id[k];
+        if (q < 0 || q >= Np) throw Error{SLAB_E_CUDA, "corrupt particle id"};
+        if (x) {
+            x[2 * q] = ((double)cell_i(cell[k]) + (double)f[k].x) * dx;
+            x[2 * q + 1] = ((double)cell_j(cell[k]) + (double)f[k].y) * dx;
+        }
+        if (v) {
+            v[2 * q] = vv[k].x;
+            v[2 * q + 1] = vv[k].y;
+        }
+        if (vz) vz[q] = vzz[k];
+        if (h) h[q] = hh[k];
+        if (m) m[q] = mm[k];
+        if (A) A[q] = (double)mm[k] / ((double)hh[k] * rho);
+        if (z) z[q] = zz[k];
+    }
+}
+
+std::vector<float> Engine32::gather_nodes(int sid, int stepid, int i0, int j0, int nI, int nJ, const std::vector<const float*>& fields,
+                                          bool with_v) {
+    Store& S = stores[sid];
+    const int64_t total = (int64_t)nI * nJ;
+    const int nout = (int)fields.size() + (with_v ? 2 : 0);
+    std::vector<float> host((size_t)nout * total);
+    if (total == 0) return host;
+    dptr<float> buf = dalloc<float>((size_t)nout * total);
+    dptr<const float*> fp = dalloc<const float*>(std::max<size_t>(1, fields.size()));
+    h2d(fp.get(), fields.data(), fields.size(), st);
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
+    k32::k_gather_nodes<<<blocks, 256, 0, st>>>(S.blk_of.get(), d_blk_stamp.get(), stepid, TY, i0, j0, nI, nJ, (int)fields.size(), fp.get(),
+                                                with_v ? d_nv.get() : nullptr, buf.get());
+    SLAB_CUDA(cudaGetLastError());
+    d2h(host.data(), buf.get(), host.size(), st);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    return host;
+}
+
+void Engine32::download_grid(int sid, slab_grid_view* gv) {
+    Store& S = stores[sid];
+    d2h(S.h_ctl, S.ctl, 1, st);
+    const SCnt c = counters(sid);
+    const int i0 = S.h_ctl->box[0], i1 = S.h_ctl->box[1], j0 = S.h_ctl->box[2], j1 = S.h_ctl->box[3];
+    const int gNx = i1 - i0 + 1, gNy = j1 - j0 + 1;
+    gv->Nx = gNx;
+    gv->Ny = gNy;
+    gv->i_off = i0;
+    gv->j_off = j0;
+    if ((int64_t)gNx * gNy > gv->cap_nodes) throw Error{SLAB_E_ARG, "grid view capacity too small"};
+    const std::vector<float> f = gather_nodes(sid, c.stepid, i0, j0, gNx, gNy, {d_oh.get(), d_om.get(), d_ovz.get()}, true);
+    const size_t n = (size_t)gNx * gNy;
+    for (size_t k = 0; k < n; ++k) {
+        if (gv->h) gv->h[k] = f[k];
+        if (gv->mass) gv->mass[k] = f[n + k];
+        if (gv->vz) gv->vz[k] = f[2 * n + k];
+        if (gv->v) {
+            gv->v[2 * k] = f[3 * n + k];
+            gv->v[2 * k + 1] = f[4 * n + k];
+        }
+    }
+}
+
+void Engine32::download_max(int sid, double* hmax, double* vmax2) {
+    const std::vector<float> f = gather_nodes(sid, -1, 0, 0, T.Nx, T.Ny, {d_hmax.get(), d_vmax2.get()}, false);
+    const size_t nn = (size_t)T.Nx * T.Ny;
+    for (size_t k = 0; k < nn; ++k) {
+        if (hmax) hmax[k] = f[k];
+        if (vmax2) vmax2[k] = f[nn + k];
+    }
+}
+
+void Engine32::conservation(int sid, double out[4], double rho) {
+    Store& S = stores[sid];
+    std::vector<double> v(2 * (size_t)S.Np), m(S.Np);
+    download_particles(sid, nullptr, v.data(), nullptr, nullptr, nullptr, m.data(), nullptr, rho);
+    double M = 0, Px = 0, Py = 0;
+    for (int q = 0; q < S.Np; ++q) {
+        M += m[q];
+        Px += m[q] * v[2 * q];
+        Py += m[q] * v[2 * q + 1];
+    }
+    const SCnt c = counters(sid);
+    out[0] = M;
+    out[1] = c.grid_mass;
+    out[2] = Px;
+    out[3] = Py;
+}
+
+namespace {
+
+// The single-scenario FP32 path behind slab_ctx.
+struct Split32 final : Path {
+    Engine32 E;
+    slab_params prm;
+    Ctl* dc;
+    Ctl* hc;
+    int sid = -1;
+    Split32(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d, Ctl* h)
+        : E(t, s, 1, (int64_t)((t.Nx + TILE - 1) / TILE) * ((t.Ny + TILE - 1) / TILE)), prm(p), dc(d), hc(h) {}
+    void upload(int Np, const double* x, const double* v, const double* vz, const double* h, const double* A, const double* m,
+                const double* z) override {
+        (void)A;
+        sid = E.add_scenario(prm, dc, hc, Np, x, v, vz, h, m, z);
+    }
+    void initial_pass() override { E.launch_t0(); }
+    void enqueue_steps(int chunk) override { E.enqueue_steps(chunk); }
+    void download_particles(double* x, double* v, double* vz, double* h, double* A, double* m, double* z) override {
+        E.download_particles(sid, x, v, vz, h, A, m, z, prm.rho);
+    }
+    void download_grid(slab_grid_view* gv) override { E.download_grid(sid, gv); }
+    void download_max(double* hm, double* vm) override { E.download_max(sid, hm, vm); }
+    void conservation(double out[4]) override { E.conservation(sid, out, prm.rho); }
+    int64_t launches() const override { return E.nlaunch; }
+    void set_profiling(bool on) override {
+        E.timer.collect();
+        E.timer.reset();
+        E.timer.on = on;
+    }
+    void phase_times(double out[5]) override {
+        E.timer.collect();
+        for (int k = 0; k < 5; ++k) out[k] = E.timer.acc[k];
+    }
+};
+
+}  // namespace
+
+std::unique_ptr<Path> make_split32(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d_ctl, Ctl* h_ctl) {
+    return std::unique_ptr<Path>(new Split32(t, p, s, d_ctl, h_ctl));
+}
+
 }  // namespace slab

@@ -1,0 +1,113 @@
+// FP32 split-precision step loop: data layout shared by the single-scenario
+// path, the batched path and the server.
+//
+// Particles. A position is an int32 base cell (ib << 16 | jb) plus an FP32
+// offset f = x/dx - ib in [0.5, 1.5): the quadratic B-spline stencil of the
+// particle is nodes ib..ib+2 (the reference's i_base = int(x/dx - 0.5),
+// src/simulation.cpp:741-742). Offsets stay O(1), so km-scale domains keep
+// ~1e-7 dx resolution where an absolute FP32 coordinate would keep ~1e-3 m.
+// Per particle (SoA): cell 4 B, f 8, v 8, h 4, m 4, id 4; vz and z only in
+// steps that feed an output frame.
+//
+// Sparse tiles. Base cells are grouped in TILE x TILE tiles. Particles are
+// stored per tile: the segment of tile t in a particle buffer is split into
+// 9 groups by the direction (-1..1)^2 of the tile the particle moves to. The
+// kernels of the next step collect tile t's particles from group d of the
+// 9 neighbours t - dir(d). Nothing is sorted globally; the G2P kernel writes
+// each tile's particles already grouped for the next step (double buffered).
+//
+// Nodes. Node (i, j) is owned by tile (i / TILE, j / TILE). Per-step grid
+// fields and the persistent h_max / v_max2 live in TILE x TILE node blocks
+// allocated on first touch from a pool. P2G writes, per active tile, partial
+// sums over its (TILE+2)^2 node window; the grid update adds the partials of
+// the up-to-4 tiles covering a node in a fixed order, so every sum has a
+// fixed order and results are bitwise reproducible.
+#pragma once
+
+#include "common.cuh"
+
+namespace slab {
+
+constexpr int TILE = 16;              // base cells per tile edge
+constexpr int TN = TILE + 2;          // node window edge of a tile
+constexpr int NCELL = TILE * TILE;    // cells per tile = threads per CTA
+constexpr int NQ = 7;                 // P2G sums: m, m vx, m vy, m h, Fx, Fy, m vz
+constexpr int PART_STRIDE = NQ * TN * TN;  // floats per tile partial
+constexpr int CHUNK = 1024;           // particles staged per pass of P2G/G2P
+
+__host__ __device__ inline int32_t pack_cell(int ib, int jb) { return (ib << 16) | jb; }
+__host__ __device__ inline int cell_i(int32_t c) { return (int)((uint32_t)c >> 16); }
+__host__ __device__ inline int cell_j(int32_t c) { return (int)(c & 0xffff); }
+
+struct PBuf {
+    int32_t* cell;
+    float2* f;
+    float2* v;
+    float* h;
+    float* m;
+    int32_t* id;
+    float* vz;
+    float* z;
+};
+
+// Per-scenario counters (device).
+struct SCnt {
+    int32_t act_count[2];  // active tiles of the list of each parity
+    int32_t gt_count;      // grid tiles of the running step
+    int32_t cursor;        // particles placed in the next buffer
+    int32_t seq;           // completed G2P passes (buffer parity = seq & 1)
+    int32_t stepid;        // P2G passes so far (stamps grid tiles / blocks)
+    int32_t vz_next;       // the running G2P must store vz (a frame may follow)
+    int32_t outs;          // the running step writes output fields
+    double grid_mass;      // FP64 sum of node masses of the last grid update
+    int32_t t0_pending;    // the scenario still needs simulate()'s t=0 pass
+    int32_t pad_;
+};
+
+// Device descriptor of one scenario.
+struct Scn {
+    Ctl* ctl;
+    SCnt* cnt;
+    // physics (FP32 copies of slab_params)
+    float g, rho, fr, ood;
+    int32_t fric;
+    float mu_c, mu_v, xi, mu1, mu2, I0, d, phi;
+    int32_t Np;
+    PBuf buf[2];
+    int32_t* grp[2];        // [ntiles][10] group offsets of each tile segment
+    int32_t* grp_stamp[2];  // [ntiles] seq at which grp was written
+    int32_t* act_stamp;     // [ntiles] last seq the tile was put on an active list
+    int32_t* act_list[2];   // active tiles of each parity
+    int32_t* slot_of;       // [ntiles] index in the active list of the running step
+    int32_t* nxt_off;       // [ntiles] start of the tile's segment in the next buffer
+    int32_t* gt_stamp;      // [ntiles] stepid at which the tile joined the grid list
+    int32_t* gt_list;       // grid tiles of the running step
+    int32_t* blk_of;        // [ntiles] node block of the tile, -1 if none yet
+    float* part;            // [act_cap][PART_STRIDE]
+    int32_t act_cap;
+    int32_t pad_;
+};
+
+// Shared by all scenarios of a context: terrain and node-block pool.
+struct Shared {
+    int32_t Nx, Ny, TX, TY;
+    const float4* dem;  // gx, gy, cos(theta), z per node
+    // node blocks, NCELL nodes each
+    float4* nv;        // vx, vy, flip x, flip y
+    float* hmax;       // persistent maxima
+    float* vmax2;
+    float* oh;         // output fields (frame steps)
+    float* om;
+    float* ovz;
+    int32_t* blk_stamp;   // stepid of the last grid update of the block
+    int32_t* blk_owner;   // scenario of the block
+    int32_t* blk_count;
+    int32_t blk_cap;
+    int32_t nscn;
+    const Scn* scn;
+    int32_t* work_pref;   // [nscn+1] prefix of active tiles (P2G / G2P work)
+    int32_t* grid_pref;   // [nscn+1] prefix of grid tiles
+    uint32_t* done;       // last-block-done counters [2]
+};
+
+}  // namespace slab

@@ -69,6 +69,8 @@ def lib():
         L.slab_initial_pass.argtypes = [vp]
         L.slab_advance_to_frame.argtypes = [vp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
         L.slab_advance_steps.argtypes = [vp, C.c_int64, C.POINTER(C.c_int64)]
+        L.slab_advance_steps_async.argtypes = [vp, C.c_int64]
+        L.slab_synchronize.argtypes = [vp]
         L.slab_download_particles.argtypes = [vp] + [dp] * 7
         L.slab_download_grid.argtypes = [vp, C.POINTER(GridView)]
         L.slab_download_max.argtypes = [vp, dp, dp]
@@ -76,6 +78,9 @@ def lib():
         L.slab_get_state.argtypes = [vp, dp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
         L.slab_set_profiling.argtypes = [vp, C.c_int32]
         L.slab_get_phase_times.argtypes = [vp, dp]
+        L.slab_work_counters.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.slab_poisson_disk.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int32, C.c_uint64, dp, C.c_int64,
+                                        C.POINTER(C.c_int64)]
         L.slab_kernel_launches.argtypes = [vp]
         L.slab_kernel_launches.restype = C.c_int64
         L.slab_last_error.argtypes = [vp]
@@ -90,6 +95,21 @@ def lib():
 
 def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def poisson_disk(Lx: float, Ly: float, r: float, seed: int, k: int = 30) -> np.ndarray:
+    """Poisson-disk samples (n, 2) in [0,Lx]x[0,Ly] relative to the corner
+    (seed 0 reproduces the reference's rand()-driven sampler)."""
+    L = lib()
+    n = C.c_int64()
+    code = L.slab_poisson_disk(Lx, Ly, r, k, seed, None, 0, C.byref(n))
+    if code:
+        raise SlabError(code, "slab_poisson_disk")
+    out = np.zeros(2 * n.value)
+    code = L.slab_poisson_disk(Lx, Ly, r, k, seed, _dp(out), n.value, C.byref(n))
+    if code:
+        raise SlabError(code, "slab_poisson_disk")
+    return out.reshape(-1, 2)
 
 
 def make_params(cfg: dict, precision: int = FP64_PLAIN) -> Params:
@@ -162,6 +182,13 @@ class Slab:
         self._check(self.L.slab_advance_steps(self.h, int(n), C.byref(s)))
         return s.value
 
+    def advance_steps_async(self, n: int):
+        """Enqueue n steps on the context's stream without waiting."""
+        self._check(self.L.slab_advance_steps_async(self.h, int(n)))
+
+    def synchronize(self):
+        self._check(self.L.slab_synchronize(self.h))
+
     def particles(self) -> dict:
         n = self.Np
         out = {k: np.zeros(2 * n if k in ("x", "v") else n) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
@@ -196,6 +223,12 @@ class Slab:
         t, dt, f, s = C.c_double(), C.c_double(), C.c_int32(), C.c_int64()
         self._check(self.L.slab_get_state(self.h, C.byref(t), C.byref(dt), C.byref(f), C.byref(s)))
         return t.value, dt.value, f.value, s.value
+
+    def work_counters(self):
+        """(particle-steps, active node-steps) done so far."""
+        out = (C.c_int64 * 2)()
+        self._check(self.L.slab_work_counters(self.h, out))
+        return int(out[0]), int(out[1])
 
     def kernel_launches(self) -> int:
         return self.L.slab_kernel_launches(self.h)

@@ -82,7 +82,7 @@ def terrain_theta(z: np.ndarray, dx: float) -> np.ndarray:
 
 
 def release_particles(z: np.ndarray, dx: float, release: dict, rho: float, sampling: str = "UNIFORM",
-                      samples: np.ndarray | None = None) -> dict:
+                      samples: np.ndarray | None = None, fast_theta: bool = False) -> dict:
     """Simulation::initializeParticles for RECTANGLE/ELLIPSE/RASTER releases.
 
     release: {"type": "RECTANGLE", "center": (x, y), "Lx", "Ly", "rotation_deg", "h0"}
@@ -163,8 +163,11 @@ def release_particles(z: np.ndarray, dx: float, release: dict, rho: float, sampl
     gn = terrain_gradient_norm(z, dx)
     ci = np.floor(x[:, 0] * ood).astype(np.int64)
     cj = np.floor(x[:, 1] * ood).astype(np.int64)
-    cells, inv = np.unique(ci * z.shape[1] + cj, return_inverse=True)
-    theta = libm_atan(gn.ravel()[cells])[inv]  # particleSlopeAngle (src/complex_terrain.cpp:113-120)
+    if fast_theta:  # numpy's arctan (may differ from libm in the last bit); theta is recomputed by the step anyway
+        theta = np.arctan(gn[ci, cj])
+    else:
+        cells, inv = np.unique(ci * z.shape[1] + cj, return_inverse=True)
+        theta = libm_atan(gn.ravel()[cells])[inv]  # particleSlopeAngle (src/complex_terrain.cpp:113-120)
     # z by the 4x4 stencil of src/simulation.cpp:455-465
     zp = np.zeros(n)
     ib = (x[:, 0] * ood).astype(np.int64) - 1
@@ -330,3 +333,40 @@ def config1():
     rel = {"type": "RECTANGLE", "center": (150.0, 250.0), "Lx": 100.0, "Ly": 100.0, "rotation_deg": 0.0, "h0": 2.0}
     P = release_particles(z, 5.0, rel, cfg["rho"])
     return {"name": "slope35_arc_401x101_dx5", "z": z, "dx": 5.0, "cfg": cfg, "release": rel, "particles": P}
+
+
+def config2(seed: int = 2026, sampler=None):
+    """4096^2 DEM at 1 m (30-degree slope easing to 5 degrees + fBm roughness,
+    Hurst 0.8, 15 m RMS, wavelengths < 20 m removed), seeded 12-vertex
+    star-convex release polygon with ~500 x 300 m semi-axes rasterised with
+    lognormal heights (median 1.5 m, sigma_log 0.4, h_min 0.2 m), POISSON
+    sampling at r = 0.5 m (~0.55-0.6 M particles), Voellmy mu=0.2 xi=1500,
+    total_time 120 s. `sampler(Lx, Ly, r, seed)` must return Poisson-disk
+    samples (slab.poisson_disk)."""
+    dx = 1.0
+    z = fractal_slope_dem(4096, dx, seed=seed)
+    poly = star_polygon(seed + 1, center=(700.0, 2048.0), ax=500.0, ay=300.0)
+    rel = lognormal_release_raster(seed + 2, poly, cellsize=dx)
+    rel["h_min"] = 0.2
+    cfg = dict(gravity=9.81, rho=300.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=120.0,
+               friction="VOELLMY", voellmy_mu=0.2, voellmy_xi=1500.0)
+    h = rel["h"]
+    Lx = (h.shape[0] - 1) * dx
+    Ly = (h.shape[1] - 1) * dx
+    samples = sampler(Lx, Ly, 0.5, seed + 3)
+    P = release_particles(z, dx, rel, cfg["rho"], sampling="GIVEN", samples=samples)
+    return {"name": "fractal4096_dx1_star_poisson_voellmy", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}
+
+
+def config3(seed: int = 2027):
+    """8192^2 DEM at 0.5 m (same construction, roughness amplitude scaled to
+    7.5 m RMS), 1200 x 800 m ellipse h0 = 3 m, UNIFORM 2x2 sampling
+    (~12 M particles), mu(I) (0.38, 0.64, 0.279, d 0.5 mm, phi 0.6), rho 1500,
+    total_time 90 s."""
+    dx = 0.5
+    z = fractal_slope_dem(8192, dx, seed=seed, rms=7.5)
+    cfg = dict(gravity=9.81, rho=1500.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=90.0,
+               friction="MU_I", mui_mu1=0.38, mui_mu2=0.64, mui_I0=0.279, mui_d=5e-4, mui_phi=0.6)
+    rel = {"type": "ELLIPSE", "center": (800.0, 2048.0), "rx": 600.0, "ry": 400.0, "rotation_deg": 0.0, "h0": 3.0}
+    P = release_particles(z, dx, rel, cfg["rho"], fast_theta=True)
+    return {"name": "fractal8192_dx05_ellipse_uniform_mui", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}

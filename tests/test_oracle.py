@@ -138,3 +138,28 @@ def test_oracle_vs_reference_binary_brienz_5m(tmp_path):
                 assert np.array_equal(P[fld], recs[k]["particles"][fld]), (k, fld)
     hm, vm = o.max_maps()
     assert np.array_equal(hm, recs[n]["h_max"]) and np.array_equal(vm, recs[n]["v_max2"])
+
+
+def test_fp64_sensitivity_envelope():
+    """The reference model is chaotic over long runs: the FP64 oracle with its
+    input positions perturbed by 1e-7 (relative) moves the 60 s h_max map of
+    the slope case by centimetres on a few nodes, while 1e-13 moves it by
+    nanometres. This bounds what any FP32 state can match node by node."""
+    c = cases.case_slope35()
+
+    def run(P):
+        o = O.Oracle(c["cfg"], c["z"], c["dx"])
+        o.set_particles(P)
+        o.t0()
+        o.run()
+        return o.max_maps()[0]
+
+    h0 = run(c["particles"])
+    out = {}
+    for eps in (1e-13, 1e-7):
+        P = {k: v.copy() for k, v in c["particles"].items()}
+        P["x"] = P["x"] * (1 + eps * np.random.default_rng(1).standard_normal(P["x"].shape))
+        d = np.abs(run(P) - h0)
+        out[eps] = d.max()
+    assert out[1e-13] < 1e-6
+    assert out[1e-7] > 0.005
