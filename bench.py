@@ -261,6 +261,13 @@ def ours(args, rank, world):
     ms_prof, _, work_prof, _, phases = timed(s32, args.steps, profile=True)
     state = s32.particles()
     t32 = s32.state()[0]
+    if args.only == "fp32":
+        if rank == 0:
+            return {"metric": METRIC, "value": round(Np * args.steps / (ms * 1e-3), 1), "unit": METRIC, "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
+                    "config": {"workload": c["name"], "particles": Np, "only": "fp32"},
+                    "phases_ms": [round(p / args.steps, 5) for p in phases], "gpu_launches": int(launches)}
+        return None
 
     # ---- plain FP64 path on the same schedule
     s64 = make(slab.FP64_PLAIN)
@@ -402,6 +409,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-procs", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only", default="", choices=["", "fp32"], help="fp32: only the FP32 path (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         log("warmup raised to 3")

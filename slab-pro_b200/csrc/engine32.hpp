@@ -22,7 +22,6 @@ class Engine32 {
         dptr<float2> f[2], v[2];
         dptr<float> h[2], m[2], vz[2], z[2];
         dptr<int32_t> act_stamp, slot_of, nxt_off, gt_stamp, gt_list, blk_of;
-        dptr<float> part;
         dptr<SCnt> cnt;
     };
 
@@ -50,7 +49,10 @@ class Engine32 {
     int nscn = 0;
     int TX = 0, TY = 0, ntiles = 0;
     int blk_cap = 0;
-    int grid_p2g = 0, grid_g2p = 0, grid_grid = 0;
+    int grid_p2g = 0, grid_g2p = 0, grid_grid = 0, grid_prep = 0;
+    int work_cap = 0;
+    int64_t work_cap_total = 0;
+    void ensure_work_cap(int64_t need);
     int64_t nlaunch = 0;
     std::deque<Store> stores;
     std::vector<Scn> host_scn;
@@ -62,6 +64,8 @@ class Engine32 {
     dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz;
     dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_grid_pref;
     dptr<Scn> d_scn;
+    dptr<TileDesc> d_desc;
+    dptr<float> d_part;
     StepGraphs graphs;
     int graph_nscn = 0;
 };

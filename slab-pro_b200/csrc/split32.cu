@@ -80,6 +80,7 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     grid_p2g = sms * std::max(occ_p, 1);
     grid_g2p = sms * std::max(occ_g, 1);
     grid_grid = sms * std::max(occ_u, 1);
+    grid_prep = sms * 2;
 }
 
 Engine32::~Engine32() {}
@@ -106,7 +107,20 @@ Shared Engine32::shared() const {
     sh.work_pref = d_work_pref.get();
     sh.grid_pref = d_grid_pref.get();
     sh.done = reinterpret_cast<uint32_t*>(d_misc.get() + 2);
+    sh.desc = d_desc.get();
+    sh.part = d_part.get();
+    sh.work_cap = work_cap;
     return sh;
+}
+
+void Engine32::ensure_work_cap(int64_t need) {
+    if (need <= work_cap) return;
+    const int64_t cap = std::min<int64_t>(std::max<int64_t>(need, (int64_t)work_cap * 3 / 2), INT32_MAX / PART_STRIDE);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    d_desc = dalloc<TileDesc>(cap);
+    d_part = dalloc<float>((size_t)cap * PART_STRIDE);
+    work_cap = (int)cap;
+    graphs.clear();
 }
 
 int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, const double* x, const double* v, const double* vz,
@@ -137,8 +151,9 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     S.gt_stamp = dalloc<int32_t>(ntiles);
     S.gt_list = dalloc<int32_t>(ntiles);
     S.blk_of = dalloc<int32_t>(ntiles);
-    S.part = dalloc<float>((size_t)S.act_cap * PART_STRIDE);
     S.cnt = dalloc<SCnt>(1);
+    ensure_work_cap(work_cap_total + S.act_cap);
+    work_cap_total += S.act_cap;
 
     // ---- bin particles into tiles (stable in upload order)
     const double dx = T.dx, ood = 1.0 / T.dx;
@@ -208,6 +223,7 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     SCnt c0{};
     c0.act_count[0] = (int)alist.size();
     c0.t0_pending = 1;
+    c0.vz_valid = 1;
     h2d(S.cnt.get(), &c0, 1, st);
     // particle box and max speed for the first step (Simulation::updateDt / remesh)
     h_ctl->pos_acc[0] = (uint64_t)__builtin_bit_cast(uint64_t, mnx);
@@ -250,7 +266,6 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     D.gt_stamp = S.gt_stamp.get();
     D.gt_list = S.gt_list.get();
     D.blk_of = S.blk_of.get();
-    D.part = S.part.get();
     D.act_cap = S.act_cap;
     h2d(d_scn.get() + sid, &D, 1, st);
     nscn += 1;
@@ -266,15 +281,19 @@ void Engine32::launch_begin(int t0) {
 void Engine32::launch_t0() {
     const Shared sh = shared();
     k32::k_begin<<<1, 1024, 0, st>>>(sh, 1);
+    k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
     k32::k_p2g<<<grid_p2g, NCELL, sizeof(k32::P2GSmem), st>>>(sh);
     k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
     SLAB_CUDA(cudaGetLastError());
-    nlaunch += 3;
+    nlaunch += 4;
 }
 
 void Engine32::launch_kernel(int k, const Shared& sh) {
     switch (k) {
-        case 0: k32::k_begin<<<1, 1024, 0, st>>>(sh, 0); break;
+        case 0:
+            k32::k_begin<<<1, 1024, 0, st>>>(sh, 0);
+            k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
+            break;
         case 1: k32::k_p2g<<<grid_p2g, NCELL, sizeof(k32::P2GSmem), st>>>(sh); break;
         case 2: k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh); break;
         case 3: k32::k_g2p<<<grid_g2p, NCELL, 0, st>>>(sh, T.z.get()); break;
@@ -298,7 +317,7 @@ void Engine32::enqueue_steps(int chunk) {
     } else {
         graphs.launch(chunk, st, [&] { launch_step(); });
     }
-    nlaunch += 4 * chunk;
+    nlaunch += 5 * chunk;
 }
 
 SCnt Engine32::counters(int sid) {
@@ -313,6 +332,11 @@ void Engine32::download_particles(int sid, double* x, double* v, double* vz, dou
     const SCnt c = counters(sid);
     const int b = c.seq & 1;
     const int Np = S.Np;
+    if (!c.vz_valid && (vz || z)) {
+        // between output frames the step loop does not keep z / vz
+        k32::k_refresh_vz_z<<<std::min(148 * 8, (Np + 255) / 256), 256, 0, st>>>(shared(), host_scn[sid].buf[b], Np, T.z.get());
+        SLAB_CUDA(cudaGetLastError());
+    }
     std::vector<int32_t> cell(Np), id(Np);
     std::vector<float2> f(Np), vv(Np);
     std::vector<float> hh(Np), mm(Np), vzz(Np), zz(Np);

@@ -61,6 +61,16 @@ struct SCnt {
     int32_t outs;          // the running step writes output fields
     double grid_mass;      // FP64 sum of node masses of the last grid update
     int32_t t0_pending;    // the scenario still needs simulate()'s t=0 pass
+    int32_t vz_valid;      // buffer vz / z were written by the last G2P (an output step)
+};
+
+// Work descriptor of one active tile for the running step (written by
+// k_prep): its particles are groups d = 0..8 at gstart[d], gpref[d] being
+// the running count before group d.
+struct TileDesc {
+    int32_t t, total, nxt_off, sid;
+    int32_t gstart[9];
+    int32_t gpref[10];
     int32_t pad_;
 };
 
@@ -78,12 +88,11 @@ struct Scn {
     int32_t* grp_stamp[2];  // [ntiles] seq at which grp was written
     int32_t* act_stamp;     // [ntiles] last seq the tile was put on an active list
     int32_t* act_list[2];   // active tiles of each parity
-    int32_t* slot_of;       // [ntiles] index in the active list of the running step
+    int32_t* slot_of;       // [ntiles] work index (partial slot) of the tile in the running step
     int32_t* nxt_off;       // [ntiles] start of the tile's segment in the next buffer
     int32_t* gt_stamp;      // [ntiles] stepid at which the tile joined the grid list
     int32_t* gt_list;       // grid tiles of the running step
     int32_t* blk_of;        // [ntiles] node block of the tile, -1 if none yet
-    float* part;            // [act_cap][PART_STRIDE]
     int32_t act_cap;
     int32_t pad_;
 };
@@ -108,6 +117,10 @@ struct Shared {
     int32_t* work_pref;   // [nscn+1] prefix of active tiles (P2G / G2P work)
     int32_t* grid_pref;   // [nscn+1] prefix of grid tiles
     uint32_t* done;       // last-block-done counters [2]
+    TileDesc* desc;       // [work_cap] descriptors of the running step
+    float* part;          // [work_cap][PART_STRIDE] P2G partial sums
+    int32_t work_cap;
+    int32_t pad_;
 };
 
 }  // namespace slab

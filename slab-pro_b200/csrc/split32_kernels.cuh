@@ -1,8 +1,14 @@
 // Kernels of the FP32 split-precision step loop (K1-K6), shared by the
-// single-scenario path and the batched / served paths. One CTA works on one
-// tile at a time; the CTAs stride over a flat list of (scenario, tile) work
-// items, so one launch advances every running scenario by one step, each
-// with its own dt and friction law.
+// single-scenario path and the batched / served paths. One step is
+//   k_begin  (1 CTA)   per-scenario dt / stop rules, work-list prefix
+//   k_prep   (grid)    one thread per active tile: its 9 particle groups,
+//                      its segment in the next buffer, grid-tile list
+//   k_p2g    (grid)    one CTA per active tile: P2G partial sums
+//   k_grid   (grid)    one CTA per grid tile: grid update + friction
+//   k_g2p    (grid)    one CTA per active tile: G2P, advection, regrouping
+// The CTAs stride over a flat list of work items of all scenarios, so one
+// launch advances every running scenario by one step, each with its own dt
+// and friction law.
 #pragma once
 
 #include "split32.cuh"
@@ -26,56 +32,53 @@ __device__ __forceinline__ bool find_work(const int32_t* pref, int nscn, int w, 
     return true;
 }
 
-// exclusive prefix over n <= blockDim.x values held one per thread
-__device__ int block_exclusive_scan(int v, int* s_tmp) {
-    const int tid = threadIdx.x;
-    s_tmp[tid] = v;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        int add = tid >= o ? s_tmp[tid - o] : 0;
-        __syncthreads();
-        s_tmp[tid] += add;
-        __syncthreads();
+// exclusive prefix over one value per thread (any blockDim <= 1024 that is a
+// multiple of 32); s_warp needs blockDim/32 + 1 ints
+__device__ int block_exclusive_scan(int v, int* s_warp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
-    const int incl = s_tmp[tid];
+    if (lane == 31) s_warp[warp] = x;
     __syncthreads();
-    return incl - v;
-}
-
-// Tile t's particles are group d of the 9 neighbour segments t - dir(d) of
-// the current buffer; s_gstart / s_gpref give the concatenated sequence.
-__device__ __forceinline__ void gather_groups(const Scn& S, const Shared& sh, int cur, int seq, int ti, int tj, int* s_gstart,
-                                              int* s_gpref) {
-    int acc = 0;
-    for (int d = 0; d < 9; ++d) {
-        const int si = ti - dir_i(d), sj = tj - dir_j(d);
-        int start = 0, end = 0;
-        if (si >= 0 && sj >= 0 && si < sh.TX && sj < sh.TY) {
-            const int s = si * sh.TY + sj;
-            if (S.grp_stamp[cur][s] == seq) {
-                start = S.grp[cur][s * 10 + d];
-                end = S.grp[cur][s * 10 + d + 1];
-            }
+    if (warp == 0) {
+        int t = lane < nw ? s_warp[lane] : 0;
+        const int t0 = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
         }
-        s_gstart[d] = start;
-        s_gpref[d] = acc;
-        acc += end - start;
+        if (lane < nw) s_warp[lane] = t - t0;
+        if (lane == nw - 1) s_warp[nw] = t;
     }
-    s_gpref[9] = acc;
+    __syncthreads();
+    const int r = s_warp[warp] + x - v;
+    __syncthreads();
+    return r;
 }
 
-__device__ __forceinline__ int seq_to_index(int q, const int* s_gstart, const int* s_gpref) {
+__device__ __forceinline__ int seq_to_index(int q, const TileDesc& D) {
     int d = 0;
-    while (d < 8 && s_gpref[d + 1] <= q) ++d;
-    return s_gstart[d] + (q - s_gpref[d]);
+    while (d < 8 && D.gpref[d + 1] <= q) ++d;
+    return D.gstart[d] + (q - D.gpref[d]);
+}
+
+// copy a descriptor to shared memory (threads 0..23)
+__device__ __forceinline__ void load_desc(const TileDesc* g, TileDesc* s) {
+    if (threadIdx.x < (int)(sizeof(TileDesc) / 4)) reinterpret_cast<int*>(s)[threadIdx.x] = reinterpret_cast<const int*>(g)[threadIdx.x];
 }
 
 // ---------------------------------------------------------------- control
 
 // K5 (first half): per scenario, Simulation::updateDt and the stop rules;
-// then the prefix of active tiles over scenarios (the P2G / G2P work list).
+// then the prefix of active tiles over scenarios (the work list).
 __global__ void k_begin(Shared sh, int t0_pass) {
-    __shared__ int s_tmp[1024];
+    __shared__ int s_warp[33];
+    __shared__ int s_tot;
     const int tid = threadIdx.x;
     int total = 0;
     for (int base = 0; base < sh.nscn; base += blockDim.x) {
@@ -108,18 +111,99 @@ __global__ void k_begin(Shared sh, int t0_pass) {
                 cnt = n->act_count[n->seq & 1];
             }
         }
-        const int ex = block_exclusive_scan(cnt, s_tmp);
+        const int ex = block_exclusive_scan(cnt, s_warp);
         if (s < sh.nscn) sh.work_pref[s] = total + ex;
-        // block total: last thread's exclusive + its value
-        if (tid == blockDim.x - 1) s_tmp[0] = ex + cnt;
+        if (tid == blockDim.x - 1) s_tot = ex + cnt;
         __syncthreads();
-        total += s_tmp[0];
+        total += s_tot;
         __syncthreads();
     }
     if (tid == 0) {
-        sh.work_pref[sh.nscn] = total;
+        sh.work_pref[sh.nscn] = min(total, sh.work_cap);
+        if (total > sh.work_cap) atomicOr(&sh.scn[0].ctl->err, ERR_CAPACITY);
         sh.done[0] = 0;
         sh.done[1] = 0;
+    }
+}
+
+// K1 (bookkeeping half): one thread per active tile. Tile t's particles are
+// group d of the 9 neighbour segments t - dir(d) of the current buffer; the
+// descriptor records them, reserves the tile's segment in the next buffer
+// and puts the 4 tiles owning its node window on the grid-tile list.
+__global__ void __launch_bounds__(256) k_prep(Shared sh) {
+    const int nwork = sh.work_pref[sh.nscn];
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
+        int sid, loc;
+        find_work(sh.work_pref, sh.nscn, w, sid, loc);
+        const Scn& S = sh.scn[sid];
+        SCnt* n = S.cnt;
+        const int seq = n->seq, cur = seq & 1;
+        const int t = S.act_list[cur][loc];
+        const int ti = t / sh.TY, tj = t % sh.TY;
+        TileDesc D;
+        D.t = t;
+        D.sid = sid;
+        int st[9], en[9];
+#pragma unroll
+        for (int d = 0; d < 9; ++d) {
+            const int si = ti - dir_i(d), sj = tj - dir_j(d);
+            st[d] = en[d] = 0;
+            if (si >= 0 && sj >= 0 && si < sh.TX && sj < sh.TY) {
+                const int s = si * sh.TY + sj;
+                if (S.grp_stamp[cur][s] == seq) {
+                    st[d] = S.grp[cur][s * 10 + d];
+                    en[d] = S.grp[cur][s * 10 + d + 1];
+                }
+            }
+        }
+        int acc = 0;
+#pragma unroll
+        for (int d = 0; d < 9; ++d) {
+            D.gstart[d] = st[d];
+            D.gpref[d] = acc;
+            acc += en[d] - st[d];
+        }
+        D.gpref[9] = acc;
+        D.total = acc;
+        D.nxt_off = atomicAdd(&n->cursor, acc);
+        D.pad_ = 0;
+        S.slot_of[t] = w;
+        const int stamp = n->stepid;
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int gi = ti + a, gj = tj + b;
+                if (gi < sh.TX && gj < sh.TY) {
+                    const int g = gi * sh.TY + gj;
+                    if (atomicMax(&S.gt_stamp[g], stamp) < stamp) S.gt_list[atomicAdd(&n->gt_count, 1)] = g;
+                }
+            }
+        sh.desc[w] = D;
+    }
+    // the last CTA builds the grid-tile work list prefix for k_grid
+    __shared__ int s_last, s_tot;
+    __shared__ int s_warp[33];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&sh.done[0], 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        int total = 0;
+        for (int base = 0; base < sh.nscn; base += blockDim.x) {
+            const int s = base + threadIdx.x;
+            const int cnt = (s < sh.nscn && sh.scn[s].ctl->active) ? *(volatile int*)&sh.scn[s].cnt->gt_count : 0;
+            const int ex = block_exclusive_scan(cnt, s_warp);
+            if (s < sh.nscn) sh.grid_pref[s] = total + ex;
+            if (threadIdx.x == blockDim.x - 1) s_tot = ex + cnt;
+            __syncthreads();
+            total += s_tot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) sh.grid_pref[sh.nscn] = total;
     }
 }
 
@@ -136,21 +220,18 @@ struct P2GSmem {
     float vz[CHUNK];
     short idx[CHUNK];
     int ccnt[NCELL];
-    int cstart[NCELL];
     int ccur[NCELL];
-    int scan_tmp[NCELL];
-    int gstart[9];
-    int gpref[10];
-    int sid, loc;
+    int warp[NCELL / 32 + 1];
+    TileDesc d;
 };
 
-// K2: P2G of one tile (src/simulation.cpp:726-798) without atomics. Each
-// thread owns one base cell of the tile and sums the contributions of that
-// cell's particles to its 3x3 nodes in registers, visiting the particles in
-// a fixed order (the tile's particle sequence, sorted by cell in shared
-// memory). The 9 register blocks are then added into the shared (TILE+2)^2
-// node window in 9 conflict-free phases, and the window is written as the
-// tile's partial sums.
+// K2: P2G of one tile (src/simulation.cpp:726-798) without atomics on the
+// sums. Each thread owns one base cell of the tile and sums the
+// contributions of that cell's particles to its 3x3 nodes in registers,
+// visiting the particles in a fixed order (the tile's particle sequence,
+// bucketed by cell in shared memory). The register blocks are combined into
+// the shared (TILE+2)^2 node window along j with warp shuffles and along i in
+// 3 conflict-free phases; the window is written as the tile's partial sums.
 __global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
@@ -158,36 +239,20 @@ __global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
     const int ci = tid / TILE, cj = tid % TILE;
     const int nwork = sh.work_pref[sh.nscn];
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        if (tid == 0) find_work(sh.work_pref, sh.nscn, w, sm.sid, sm.loc);
+        load_desc(sh.desc + w, &sm.d);
         __syncthreads();
-        const Scn& S = sh.scn[sm.sid];
-        SCnt* n = S.cnt;
-        const int seq = n->seq, cur = seq & 1;
-        const int loc = sm.loc;
-        const int t = S.act_list[cur][loc];
+        const Scn& S = sh.scn[sm.d.sid];
+        const int t = sm.d.t;
         const int ti = t / sh.TY, tj = t % sh.TY;
-        if (tid == 0) {
-            gather_groups(S, sh, cur, seq, ti, tj, sm.gstart, sm.gpref);
-            S.nxt_off[t] = atomicAdd(&n->cursor, sm.gpref[9]);
-            S.slot_of[t] = loc;
-            const int sid_stamp = n->stepid;
-            for (int a = 0; a < 2; ++a)
-                for (int b = 0; b < 2; ++b) {
-                    const int gi = ti + a, gj = tj + b;
-                    if (gi < sh.TX && gj < sh.TY) {
-                        const int g = gi * sh.TY + gj;
-                        if (atomicMax(&S.gt_stamp[g], sid_stamp) < sid_stamp) S.gt_list[atomicAdd(&n->gt_count, 1)] = g;
-                    }
-                }
-        }
+        SCnt* n = S.cnt;
+        const int cur = n->seq & 1;
+        const bool outs = n->outs != 0;
         for (int k = tid; k < (TILE + 1) * (TILE + 1); k += NCELL) {
             const int i = ti * TILE + k / (TILE + 1), j = tj * TILE + k % (TILE + 1);
             sm.dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
         }
         for (int k = tid; k < NQ * TN * TN; k += NCELL) sm.node[k] = 0.f;
-        __syncthreads();
-        const int total = sm.gpref[9];
-        const bool outs = n->outs != 0;
+        const int total = sm.d.total;
         const PBuf B = S.buf[cur];
         const float g = S.g, ood = S.ood;
         float acc[9][NQ];
@@ -200,7 +265,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
             sm.ccnt[tid] = 0;
             __syncthreads();
             for (int k = tid; k < nc; k += NCELL) {
-                const int src = seq_to_index(c0 + k, sm.gstart, sm.gpref);
+                const int src = seq_to_index(c0 + k, sm.d);
                 const int32_t cell = B.cell[src];
                 int li = cell_i(cell) - ti * TILE, lj = cell_j(cell) - tj * TILE;
                 if ((unsigned)li >= TILE || (unsigned)lj >= TILE) {
@@ -219,8 +284,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
             }
             __syncthreads();
             const int my_cnt = sm.ccnt[tid];
-            const int my_start = block_exclusive_scan(my_cnt, sm.scan_tmp);
-            sm.cstart[tid] = my_start;
+            const int my_start = block_exclusive_scan(my_cnt, sm.warp);
             sm.ccur[tid] = my_start;
             __syncthreads();
             for (int k = tid; k < nc; k += NCELL) sm.idx[atomicAdd(&sm.ccur[sm.lc[k]], 1)] = (short)k;
@@ -271,43 +335,32 @@ __global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
             }
             __syncthreads();
         }
-        // 9 conflict-free phases: in phase (a,b) thread (ci,cj) adds into node (ci+a, cj+b)
+        // Combine: node (ci+a, nj) gets acc[a][0] of cell nj, acc[a][1] of
+        // cell nj-1 and acc[a][2] of cell nj-2 (same row of the tile, i.e.
+        // adjacent lanes), then rows are added in 3 phases a = 0, 1, 2.
 #pragma unroll
         for (int ia = 0; ia < 3; ++ia) {
+            float* row = sm.node + (ci + ia) * TN;
 #pragma unroll
-            for (int jb = 0; jb < 3; ++jb) {
-                const int nd = (ci + ia) * TN + (cj + jb);
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) sm.node[q * TN * TN + nd] += acc[ia * 3 + jb][q];
-                __syncthreads();
+            for (int q = 0; q < NQ; ++q) {
+                const float a0 = acc[ia * 3 + 0][q], a1 = acc[ia * 3 + 1][q], a2 = acc[ia * 3 + 2][q];
+                const float s1 = __shfl_up_sync(0xffffffffu, a1, 1);
+                const float s2 = __shfl_up_sync(0xffffffffu, a2, 2);
+                const float s21 = __shfl_up_sync(0xffffffffu, a2, 1);
+                float val = a0;
+                if (cj >= 1) val += s1;
+                if (cj >= 2) val += s2;
+                row[q * TN * TN + cj] += val;
+                if (cj == TILE - 1) {
+                    row[q * TN * TN + TILE] += a1 + s21;  // cells 15 (b=1) and 14 (b=2)
+                    row[q * TN * TN + TILE + 1] += a2;    // cell 15 (b=2)
+                }
             }
+            __syncthreads();
         }
-        float* P = S.part + (size_t)loc * PART_STRIDE;
+        float* P = sh.part + (size_t)w * PART_STRIDE;
         for (int k = tid; k < PART_STRIDE; k += NCELL) P[k] = sm.node[k];
         __syncthreads();
-    }
-    // the last CTA builds the grid-tile work list prefix for k_grid
-    __shared__ int s_last;
-    __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        s_last = (atomicAdd(&sh.done[0], 1u) == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (s_last) {
-        __threadfence();
-        int total = 0;
-        for (int base = 0; base < sh.nscn; base += blockDim.x) {
-            const int s = base + tid;
-            const int cnt = (s < sh.nscn && sh.scn[s].ctl->active) ? *(volatile int*)&sh.scn[s].cnt->gt_count : 0;
-            const int ex = block_exclusive_scan(cnt, sm.scan_tmp);
-            if (s < sh.nscn) sh.grid_pref[s] = total + ex;
-            if (tid == blockDim.x - 1) sm.scan_tmp[0] = ex + cnt;
-            __syncthreads();
-            total += sm.scan_tmp[0];
-            __syncthreads();
-        }
-        if (tid == 0) sh.grid_pref[sh.nscn] = total;
     }
 }
 
@@ -320,6 +373,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
 // the conservation diagnostic.
 __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
     __shared__ int s_sid, s_loc, s_blk;
+    __shared__ int s_slot[4];
     __shared__ double s_red[NCELL / 32];
     __shared__ unsigned s_act[NCELL / 32];
     const int tid = threadIdx.x;
@@ -333,7 +387,16 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
         Ctl* c = S.ctl;
         const int gt = S.gt_list[s_loc];
         const int gi = gt / sh.TY, gj = gt % sh.TY;
-        if (tid == 0) {
+        if (tid < 4) {
+            // contributor k: tile (gi - (k>>1), gj - (k&1)); slot if active this step
+            const int ti_ = gi - (tid >> 1), tj_ = gj - (tid & 1);
+            int slot = -1;
+            if (ti_ >= 0 && tj_ >= 0) {
+                const int tt = ti_ * sh.TY + tj_;
+                if (S.act_stamp[tt] == n->seq) slot = S.slot_of[tt];
+            }
+            s_slot[tid] = slot;
+        } else if (tid == 32) {
             int blk = S.blk_of[gt];
             if (blk < 0) {
                 blk = atomicAdd(sh.blk_count, 1);
@@ -352,22 +415,19 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
         const int blk = s_blk;
         double mloc = 0.0;
         if (blk >= 0) {
-            const int seq = n->seq;
             float q[NQ];
 #pragma unroll
             for (int k = 0; k < NQ; ++k) q[k] = 0.f;
-            auto add = [&](int ti_, int tj_, int a, int b) {
-                if (ti_ < 0 || tj_ < 0) return;
-                const int tt = ti_ * sh.TY + tj_;
-                if (S.act_stamp[tt] != seq) return;
-                const float* P = S.part + (size_t)S.slot_of[tt] * PART_STRIDE + a * TN + b;
+            auto add = [&](int slot, int a, int b) {
+                if (slot < 0) return;
+                const float* P = sh.part + (size_t)slot * PART_STRIDE + a * TN + b;
 #pragma unroll
                 for (int k = 0; k < NQ; ++k) q[k] += P[k * TN * TN];
             };
-            add(gi, gj, li, lj);
-            if (li < 2) add(gi - 1, gj, li + TILE, lj);
-            if (lj < 2) add(gi, gj - 1, li, lj + TILE);
-            if (li < 2 && lj < 2) add(gi - 1, gj - 1, li + TILE, lj + TILE);
+            add(s_slot[0], li, lj);
+            if (li < 2) add(s_slot[2], li + TILE, lj);
+            if (lj < 2) add(s_slot[1], li, lj + TILE);
+            if (li < 2 && lj < 2) add(s_slot[3], li + TILE, lj + TILE);
             const int i = gi * TILE + li, j = gj * TILE + lj;
             const size_t bn = (size_t)blk * NCELL + tid;
             float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -466,17 +526,21 @@ __device__ __noinline__ void advect(const float4* s_nv, int ci, int cj, int32_t 
     *pic = make_float2(picx, picy);
 }
 
+__device__ __forceinline__ int dir_of(int ib, int jb, int ti, int tj) {
+    int di = (ib >= 0 ? ib / TILE : -1) - ti, dj = (jb >= 0 ? jb / TILE : -1) - tj;
+    if (di < -1 || di > 1 || dj < -1 || dj > 1) return -1;
+    return (di + 1) * 3 + (dj + 1);
+}
+
 struct G2PSmem {
     float4 nv[TN * TN];
     float4 dem[(TILE + 1) * (TILE + 1)];
-    int gstart[9];
-    int gpref[10];
     int dcnt[9];
     int dpref[10];
     int wtot[NCELL / 32][9];
     int run[9];
     int blk4[4];
-    int sid, loc, base;
+    TileDesc d;
     double red[5][NCELL / 32];
 };
 
@@ -490,27 +554,22 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwork = sh.work_pref[sh.nscn];
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        if (tid == 0) find_work(sh.work_pref, sh.nscn, w, sm.sid, sm.loc);
+        load_desc(sh.desc + w, &sm.d);
         __syncthreads();
-        const int sid = sm.sid;
+        const int sid = sm.d.sid;
         const Scn& S = sh.scn[sid];
         SCnt* n = S.cnt;
         Ctl* c = S.ctl;
         const int seq = n->seq, cur = seq & 1, nxt = cur ^ 1;
-        const int t = S.act_list[cur][sm.loc];
+        const int t = sm.d.t;
         const int ti = t / sh.TY, tj = t % sh.TY;
         const bool outs = n->outs != 0;
         const bool need_vz = outs || n->vz_next;
-        if (tid == 0) {
-            gather_groups(S, sh, cur, seq, ti, tj, sm.gstart, sm.gpref);
-            sm.base = S.nxt_off[t];
-            for (int a = 0; a < 2; ++a)
-                for (int b = 0; b < 2; ++b) {
-                    const int gi = ti + a, gj = tj + b;
-                    sm.blk4[a * 2 + b] = (gi < sh.TX && gj < sh.TY) ? S.blk_of[gi * sh.TY + gj] : -1;
-                }
+        if (tid < 4) {
+            const int gi = ti + (tid >> 1), gj = tj + (tid & 1);
+            sm.blk4[tid] = (gi < sh.TX && gj < sh.TY) ? S.blk_of[gi * sh.TY + gj] : -1;
         }
-        if (tid < 9) sm.dcnt[tid] = 0;
+        if (tid >= 32 && tid < 41) sm.dcnt[tid - 32] = 0;
         __syncthreads();
         for (int k = tid; k < TN * TN; k += NCELL) {
             const int a = k / TN, b = k % TN;
@@ -529,7 +588,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             }
         }
         __syncthreads();
-        const int total = sm.gpref[9];
+        const int total = sm.d.total;
         const PBuf B = S.buf[cur];
         const PBuf O = S.buf[nxt];
         const float dt = (float)c->dt;
@@ -537,7 +596,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
         const double dx = c->dx;
         // pass 1: count the particles per destination group
         for (int q = tid; q < total; q += NCELL) {
-            const int src = seq_to_index(q, sm.gstart, sm.gpref);
+            const int src = seq_to_index(q, sm.d);
             const int32_t cell = B.cell[src];
             const float2 f = B.f[src];
             const int ci = min(max(cell_i(cell) - ti * TILE, 0), TILE - 1);
@@ -545,30 +604,27 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             int ib, jb;
             float2 fn, pic;
             advect(sm.nv, ci, cj, cell, f, dt_ood, &ib, &jb, &fn, &pic);
-            int di = (ib >= 0 ? ib / TILE : -1) - ti, dj = (jb >= 0 ? jb / TILE : -1) - tj;
-            if (di < -1 || di > 1 || dj < -1 || dj > 1) di = dj = 0;  // flagged in pass 2
-            atomicAdd(&sm.dcnt[(di + 1) * 3 + (dj + 1)], 1);
+            const int d = dir_of(ib, jb, ti, tj);
+            atomicAdd(&sm.dcnt[d < 0 ? 4 : d], 1);
         }
         __syncthreads();
-        if (tid == 0) {
+        if (tid < 10) {
             int acc = 0;
-            for (int d = 0; d < 9; ++d) {
-                sm.dpref[d] = acc;
-                S.grp[nxt][t * 10 + d] = sm.base + acc;
-                acc += sm.dcnt[d];
-                sm.run[d] = 0;
-            }
-            sm.dpref[9] = acc;
-            S.grp[nxt][t * 10 + 9] = sm.base + acc;
-            S.grp_stamp[nxt][t] = seq + 1;
-            for (int d = 0; d < 9; ++d) {
-                if (!sm.dcnt[d]) continue;
-                const int tt = (ti + dir_i(d)) * sh.TY + (tj + dir_j(d));
-                if (atomicMax(&S.act_stamp[tt], seq + 1) < seq + 1) {
-                    const int k = atomicAdd(&n->act_count[nxt], 1);
-                    if (k < S.act_cap) S.act_list[nxt][k] = tt;
-                    else atomicOr(&c->err, ERR_CAPACITY);
+            for (int d = 0; d < tid; ++d) acc += sm.dcnt[d];
+            sm.dpref[tid] = acc;
+            S.grp[nxt][t * 10 + tid] = sm.d.nxt_off + acc;
+            if (tid < 9) {
+                sm.run[tid] = 0;
+                if (sm.dcnt[tid]) {
+                    const int tt = (ti + dir_i(tid)) * sh.TY + (tj + dir_j(tid));
+                    if (atomicMax(&S.act_stamp[tt], seq + 1) < seq + 1) {
+                        const int k = atomicAdd(&n->act_count[nxt], 1);
+                        if (k < S.act_cap) S.act_list[nxt][k] = tt;
+                        else atomicOr(&c->err, ERR_CAPACITY);
+                    }
                 }
+            } else {
+                S.grp_stamp[nxt][t] = seq + 1;
             }
         }
         __syncthreads();
@@ -583,7 +639,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             double zp = 0.0;
             int32_t pid = 0;
             if (valid) {
-                const int src = seq_to_index(q, sm.gstart, sm.gpref);
+                const int src = seq_to_index(q, sm.d);
                 const int32_t cell = B.cell[src];
                 const float2 f = B.f[src];
                 const float2 v = B.v[src];
@@ -594,7 +650,6 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
                 const int cj = min(max(cell_j(cell) - tj * TILE, 0), TILE - 1);
                 float2 pic;
                 advect(sm.nv, ci, cj, cell, f, dt_ood, &ib, &jb, &fn, &pic);
-                const float picx = pic.x, picy = pic.y;
                 float wx[3], wy[3], dwx[3], dwy[3];
                 bspline3(f.x, wx, dwx);
                 bspline3(f.y, wy, dwy);
@@ -611,7 +666,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
                     }
                 div *= S.ood;
                 const float fr = S.fr;
-                vn = make_float2(fr * (v.x + flx) + (1.f - fr) * picx, fr * (v.y + fly) + (1.f - fr) * picy);
+                vn = make_float2(fr * (v.x + flx) + (1.f - fr) * pic.x, fr * (v.y + fly) + (1.f - fr) * pic.y);
                 hn = h / (1.f + dt * div);
                 if (need_vz) {
                     const float4 dm = sm.dem[(ci + (f.x >= 1.f ? 1 : 0)) * (TILE + 1) + (cj + (f.y >= 1.f ? 1 : 0))];
@@ -624,17 +679,16 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
 #pragma unroll
                         for (int b = 0; b < 3; ++b) zp += (double)(wx[a] * wy[b]) * z64[(int64_t)(i0 + a) * sh.Ny + (j0 + b)];
                 }
-                int di = (ib >= 0 ? ib / TILE : -1) - ti, dj = (jb >= 0 ? jb / TILE : -1) - tj;
-                if (di < -1 || di > 1 || dj < -1 || dj > 1) {
+                d = dir_of(ib, jb, ti, tj);
+                if (d < 0) {
                     atomicOr(&c->err, ERR_MOVE);
-                    di = dj = 0;
+                    d = 4;
                 }
                 if (ib < 0 || jb < 0 || ib + 2 > sh.Nx - 1 || jb + 2 > sh.Ny - 1) {
                     atomicOr(&c->err, ERR_DOMAIN);
                     ib = min(max(ib, 0), sh.Nx - 3);
                     jb = min(max(jb, 0), sh.Ny - 3);
                 }
-                d = (di + 1) * 3 + (dj + 1);
                 const double px = ((double)ib + (double)fn.x) * dx, py = ((double)jb + (double)fn.y) * dx;
                 mnx = fmin(mnx, px);
                 mxx = fmax(mxx, px);
@@ -663,7 +717,7 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             }
             __syncthreads();
             if (valid) {
-                const int pos = sm.base + sm.dpref[d] + sm.wtot[warp][d] + rank;
+                const int pos = sm.d.nxt_off + sm.dpref[d] + sm.wtot[warp][d] + rank;
                 O.cell[pos] = pack_cell(ib, jb);
                 O.f[pos] = fn;
                 O.v[pos] = vn;
@@ -722,7 +776,28 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             if (*(volatile int*)&n->cursor != S.Np) atomicOr(&c->err, ERR_CAPACITY);
             ctl_end(c);
             n->seq += 1;
+            n->vz_valid = n->outs;
         }
+    }
+}
+
+// Particle z and vz at the current positions (for downloads between output
+// frames, where the step loop does not keep them): vz = v . grad z of the
+// containing cell, z from the quadratic stencil of FP64 terrain heights.
+__global__ void k_refresh_vz_z(Shared sh, PBuf B, int Np, const double* __restrict__ z64) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < Np; q += gridDim.x * blockDim.x) {
+        const int32_t cell = B.cell[q];
+        const float2 f = B.f[q], v = B.v[q];
+        const int i0 = cell_i(cell), j0 = cell_j(cell);
+        float wx[3], wy[3], dwx[3], dwy[3];
+        bspline3(f.x, wx, dwx);
+        bspline3(f.y, wy, dwy);
+        const float4 dm = sh.dem[(int64_t)(i0 + (f.x >= 1.f ? 1 : 0)) * sh.Ny + (j0 + (f.y >= 1.f ? 1 : 0))];
+        double zp = 0.0;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) zp += (double)(wx[a] * wy[b]) * z64[(int64_t)(i0 + a) * sh.Ny + (j0 + b)];
+        B.vz[q] = v.x * dm.x + v.y * dm.y;
+        B.z[q] = (float)zp;
     }
 }
 
