@@ -14,6 +14,7 @@ struct slab_ctx {
     slab_params params{};
     bool have_params = false;
     bool uploaded = false;
+    bool initial_done = false;
     int Np = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -101,10 +102,15 @@ void raise_device_errors(slab_ctx* c) {
     if (e & ERR_TIMEOUT) throw Error{SLAB_E_TIMEOUT, "bounded device wait gave up"};
 }
 
-void enqueue_nsteps(slab_ctx* c, int64_t nsteps) {
-    k_arm<<<1, 32, 0, c->stream>>>(c->d_ctl, nsteps, 0);
+void arm(slab_ctx* c, int64_t steps_left, int stop_at_frame) {
+    if (c->path->arm(steps_left, stop_at_frame)) return;
+    k_arm<<<1, 32, 0, c->stream>>>(c->d_ctl, steps_left, stop_at_frame);
     SLAB_CUDA(cudaGetLastError());
     ++c->extra_launches;
+}
+
+void enqueue_nsteps(slab_ctx* c, int64_t nsteps) {
+    arm(c, nsteps, 0);
     int64_t k = 0;
     for (; k + c->chunk <= nsteps; k += c->chunk) c->path->enqueue_steps(c->chunk);
     if (k < nsteps) c->path->enqueue_steps((int)(nsteps - k));
@@ -112,6 +118,7 @@ void enqueue_nsteps(slab_ctx* c, int64_t nsteps) {
 
 void advance(slab_ctx* c, int64_t nsteps, bool stop_at_frame, int64_t* steps_out) {
     need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
+    need(c->initial_done, SLAB_E_STATE, "call slab_initial_pass before advancing");
     pull_ctl(c);
     const int64_t s0 = c->h_ctl->steps;
     if (!stop_at_frame) {
@@ -119,9 +126,7 @@ void advance(slab_ctx* c, int64_t nsteps, bool stop_at_frame, int64_t* steps_out
         enqueue_nsteps(c, nsteps);
         pull_ctl(c);
     } else {
-        k_arm<<<1, 32, 0, c->stream>>>(c->d_ctl, nsteps, 1);
-        SLAB_CUDA(cudaGetLastError());
-        ++c->extra_launches;
+        arm(c, nsteps, 1);
         double last_time = c->h_ctl->time;
         int stalled = 0;
         for (;;) {
@@ -239,6 +244,7 @@ slab_status slab_upload_particles(slab_ctx* c, int32_t Np, const double* x, cons
         raise_device_errors(c);
         c->Np = Np;
         c->uploaded = true;
+        c->initial_done = false;
     });
 }
 
@@ -249,6 +255,7 @@ slab_status slab_initial_pass(slab_ctx* c) {
         c->path->initial_pass();
         pull_ctl(c);
         raise_device_errors(c);
+        c->initial_done = true;
     });
 }
 
@@ -273,6 +280,7 @@ slab_status slab_advance_steps_async(slab_ctx* c, int64_t nsteps) {
     if (!c) return SLAB_E_ARG;
     return guard(c, [&] {
         need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
+        need(c->initial_done, SLAB_E_STATE, "call slab_initial_pass before advancing");
         need(nsteps >= 0, SLAB_E_ARG, "nsteps must be >= 0");
         enqueue_nsteps(c, nsteps);
     });

@@ -146,6 +146,9 @@ struct Path {
     virtual void initial_pass() = 0;
     // enqueue up to `chunk` steps; the device control block decides which run
     virtual void enqueue_steps(int chunk) = 0;
+    // start an advance call on the device (budget, frame stop); false: the
+    // caller arms the control block itself
+    virtual bool arm(int64_t, int) { return false; }
     virtual void download_particles(double* x, double* v, double* vz, double* h, double* A, double* m, double* z) = 0;
     virtual void download_grid(slab_grid_view* view) = 0;
     virtual void download_max(double* h_max, double* v_max2) = 0;

@@ -34,6 +34,9 @@ class Engine32 {
     void launch_t0();
     void launch_step();
     void launch_kernel(int k, const Shared& sh);
+    void launch_p2g(const Shared& sh);
+    void arm(int64_t steps_left, int stop_at_frame);
+    int acc_mode = 1;  // fixed-point scheme of P2G (k32::ACC_*)
     void enqueue_steps(int chunk);
     PhaseTimer timer;
     SCnt counters(int sid);

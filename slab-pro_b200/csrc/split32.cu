@@ -3,6 +3,7 @@
 // capture, and downloads that restore the reference layouts.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -70,11 +71,14 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaMemsetAsync(d_work_pref.get(), 0, (max_scn + 1) * sizeof(int32_t), st));
     SLAB_CUDA(cudaMemsetAsync(d_grid_pref.get(), 0, (max_scn + 1) * sizeof(int32_t), st));
     host_scn.resize(max_scn);
-    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
+    if (const char* e = std::getenv("SLAB_P2G_ACC")) acc_mode = std::atoi(e);
     int dev = 0, sms = 0, occ_p = 0, occ_g = 0, occ_u = 0;
     SLAB_CUDA(cudaGetDevice(&dev));
     SLAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g, NCELL, sizeof(k32::P2GSmem)));
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g<k32::ACC_HILO>, k32::P2G_THREADS, sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, k32::k_g2p, NCELL, 0));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k32::k_grid, NCELL, 0));
     grid_p2g = sms * std::max(occ_p, 1);
@@ -141,7 +145,7 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
         S.id[b] = dalloc<int32_t>(Np);
         S.vz[b] = dalloc<float>(Np);
         S.z[b] = dalloc<float>(Np);
-        S.grp[b] = dalloc<int32_t>((size_t)ntiles * 10);
+        S.grp[b] = dalloc<int32_t>((size_t)ntiles * GRP_STRIDE);
         S.grp_stamp[b] = dalloc<int32_t>(ntiles);
         S.act_list[b] = dalloc<int32_t>(S.act_cap);
     }
@@ -196,10 +200,14 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
         o_z[k] = (float)z[q];
         o_id[k] = q;
     }
-    std::vector<int32_t> grp((size_t)ntiles * 10, 0), gstamp(ntiles, -1), astamp(ntiles, -1), alist;
+    std::vector<int32_t> grp((size_t)ntiles * GRP_STRIDE, 0), gstamp(ntiles, -1), astamp(ntiles, -1), alist;
     for (int t = 0; t < ntiles; ++t) {
         if (!cnt[t]) continue;
-        for (int d = 0; d < 10; ++d) grp[(size_t)t * 10 + d] = d <= 4 ? start[t] : start[t + 1];
+        int32_t* G = grp.data() + (size_t)t * GRP_STRIDE;
+        G[0] = start[t];
+        G[1] = start[t + 1];
+        G[2] = start[t + 1];
+        G[3 + 4] = cnt[t];
         gstamp[t] = 0;
         astamp[t] = 0;
         alist.push_back(t);
@@ -282,22 +290,34 @@ void Engine32::launch_t0() {
     const Shared sh = shared();
     k32::k_begin<<<1, 1024, 0, st>>>(sh, 1);
     k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
-    k32::k_p2g<<<grid_p2g, NCELL, sizeof(k32::P2GSmem), st>>>(sh);
+    launch_p2g(sh);
     k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
     SLAB_CUDA(cudaGetLastError());
     nlaunch += 4;
 }
 
+void Engine32::launch_p2g(const Shared& sh) {
+    if (acc_mode == k32::ACC_I32)
+        k32::k_p2g<k32::ACC_I32><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
+    else if (acc_mode == k32::ACC_I64)
+        k32::k_p2g<k32::ACC_I64><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
+    else
+        k32::k_p2g<k32::ACC_HILO><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
+}
+
 void Engine32::launch_kernel(int k, const Shared& sh) {
     switch (k) {
-        case 0:
-            k32::k_begin<<<1, 1024, 0, st>>>(sh, 0);
-            k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
-            break;
-        case 1: k32::k_p2g<<<grid_p2g, NCELL, sizeof(k32::P2GSmem), st>>>(sh); break;
+        case 0: k32::k_prep<<<grid_prep, 256, 0, st>>>(sh); break;
+        case 1: launch_p2g(sh); break;
         case 2: k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh); break;
         case 3: k32::k_g2p<<<grid_g2p, NCELL, 0, st>>>(sh, T.z.get()); break;
     }
+}
+
+void Engine32::arm(int64_t steps_left, int stop_at_frame) {
+    k32::k_arm_begin<<<1, 1024, 0, st>>>(shared(), steps_left, stop_at_frame);
+    SLAB_CUDA(cudaGetLastError());
+    nlaunch += 1;
 }
 
 void Engine32::launch_step() {
@@ -317,7 +337,7 @@ void Engine32::enqueue_steps(int chunk) {
     } else {
         graphs.launch(chunk, st, [&] { launch_step(); });
     }
-    nlaunch += 5 * chunk;
+    nlaunch += 4 * chunk;
 }
 
 SCnt Engine32::counters(int sid) {
@@ -456,6 +476,10 @@ struct Split32 final : Path {
     }
     void initial_pass() override { E.launch_t0(); }
     void enqueue_steps(int chunk) override { E.enqueue_steps(chunk); }
+    bool arm(int64_t steps_left, int stop_at_frame) override {
+        E.arm(steps_left, stop_at_frame);
+        return true;
+    }
     void download_particles(double* x, double* v, double* vz, double* h, double* A, double* m, double* z) override {
         E.download_particles(sid, x, v, vz, h, A, m, z, prm.rho);
     }

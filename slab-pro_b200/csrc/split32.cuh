@@ -10,11 +10,11 @@
 // steps that feed an output frame.
 //
 // Sparse tiles. Base cells are grouped in TILE x TILE tiles. Particles are
-// stored per tile: the segment of tile t in a particle buffer is split into
-// 9 groups by the direction (-1..1)^2 of the tile the particle moves to. The
-// kernels of the next step collect tile t's particles from group d of the
-// 9 neighbours t - dir(d). Nothing is sorted globally; the G2P kernel writes
-// each tile's particles already grouped for the next step (double buffered).
+// stored per tile: G2P writes tile t's particles into t's segment of the
+// next buffer, those still in t from the front, those that moved to one of
+// the 8 neighbour tiles from the back (double buffered). The next step
+// collects a tile's particles from its own stayers and its neighbours'
+// movers. Nothing is sorted globally.
 //
 // Nodes. Node (i, j) is owned by tile (i / TILE, j / TILE). Per-step grid
 // fields and the persistent h_max / v_max2 live in TILE x TILE node blocks
@@ -64,15 +64,23 @@ struct SCnt {
     int32_t vz_valid;      // buffer vz / z were written by the last G2P (an output step)
 };
 
-// Work descriptor of one active tile for the running step (written by
-// k_prep): its particles are groups d = 0..8 at gstart[d], gpref[d] being
-// the running count before group d.
+// Work descriptor of one active tile t for the running step (written by
+// k_prep). Its particles are found in 9 candidate ranges of the current
+// buffer: range 4 holds the stayers of t's own segment, range d != 4 the
+// movers of neighbour t - dir(d) (of which only those now in t are used);
+// rpref[d] is the number of candidates before range d; total is the exact
+// particle count of t.
 struct TileDesc {
     int32_t t, total, nxt_off, sid;
-    int32_t gstart[9];
-    int32_t gpref[10];
+    int32_t rstart[9];
+    int32_t rpref[10];
     int32_t pad_;
 };
+
+// Segment record of a tile in a particle buffer (GRP_STRIDE ints): [0] first
+// stayer, [1] first mover (= end of stayers), [2] end, [3 + d] number of
+// particles that moved in direction d (d = 4: the stayers).
+constexpr int GRP_STRIDE = 12;
 
 // Device descriptor of one scenario.
 struct Scn {
@@ -84,7 +92,7 @@ struct Scn {
     float mu_c, mu_v, xi, mu1, mu2, I0, d, phi;
     int32_t Np;
     PBuf buf[2];
-    int32_t* grp[2];        // [ntiles][10] group offsets of each tile segment
+    int32_t* grp[2];        // [ntiles][GRP_STRIDE] segment records (see GRP_STRIDE)
     int32_t* grp_stamp[2];  // [ntiles] seq at which grp was written
     int32_t* act_stamp;     // [ntiles] last seq the tile was put on an active list
     int32_t* act_list[2];   // active tiles of each parity

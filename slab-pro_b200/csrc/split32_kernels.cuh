@@ -1,7 +1,9 @@
 // Kernels of the FP32 split-precision step loop (K1-K6), shared by the
 // single-scenario path and the batched / served paths. One step is
-//   k_begin  (1 CTA)   per-scenario dt / stop rules, work-list prefix
-//   k_prep   (grid)    one thread per active tile: its 9 particle groups,
+//   (begin)            per-scenario dt / stop rules, work-list prefix: run by
+//                      the last CTA of the previous step's k_g2p, or by
+//                      k_arm_begin at the start of an advance call
+//   k_prep   (grid)    one thread per active tile: where its particles are,
 //                      its segment in the next buffer, grid-tile list
 //   k_p2g    (grid)    one CTA per active tile: P2G partial sums
 //   k_grid   (grid)    one CTA per grid tile: grid update + friction
@@ -9,6 +11,12 @@
 // The CTAs stride over a flat list of work items of all scenarios, so one
 // launch advances every running scenario by one step, each with its own dt
 // and friction law.
+//
+// Every result is independent of the order of the particles inside a tile:
+// P2G adds fixed-point integers (exact, associative), the grid update adds
+// the partials of a node's tiles in a fixed order, and everything else is
+// per particle or a max/min. So placement can use atomics freely and the
+// step is still bitwise reproducible, alone or inside a batch.
 #pragma once
 
 #include "split32.cuh"
@@ -61,10 +69,30 @@ __device__ int block_exclusive_scan(int v, int* s_warp) {
     return r;
 }
 
-__device__ __forceinline__ int seq_to_index(int q, const TileDesc& D) {
-    int d = 0;
-    while (d < 8 && D.gpref[d + 1] <= q) ++d;
-    return D.gstart[d] + (q - D.gpref[d]);
+// atomicAdd of `val` to *addr by the lanes in `mask`; lanes with the same
+// address are combined into one atomic. Returns the lane's old value.
+__device__ int warp_atomic_add(int* addr, int val, unsigned mask) {
+    const unsigned peers = __match_any_sync(mask, (unsigned long long)addr);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int prefix = 0, total = 0;
+    for (unsigned m = peers; m; m &= m - 1) {
+        const int l = __ffs(m) - 1;
+        const int v = __shfl_sync(peers, val, l);
+        if (l < lane) prefix += v;
+        total += v;
+    }
+    int base = 0;
+    if (lane == leader) base = atomicAdd(addr, total);
+    base = __shfl_sync(peers, base, leader);
+    return base + prefix;
+}
+
+// candidate index -> particle index in the current buffer (range d)
+__device__ __forceinline__ int cand_to_index(int q, const TileDesc& D, int& d) {
+    d = 0;
+    while (d < 8 && D.rpref[d + 1] <= q) ++d;
+    return D.rstart[d] + (q - D.rpref[d]);
 }
 
 // copy a descriptor to shared memory (threads 0..23)
@@ -72,11 +100,15 @@ __device__ __forceinline__ void load_desc(const TileDesc* g, TileDesc* s) {
     if (threadIdx.x < (int)(sizeof(TileDesc) / 4)) reinterpret_cast<int*>(s)[threadIdx.x] = reinterpret_cast<const int*>(g)[threadIdx.x];
 }
 
+__device__ __forceinline__ int tile_of_cell(int32_t cell, int TY) { return (cell_i(cell) / TILE) * TY + cell_j(cell) / TILE; }
+
 // ---------------------------------------------------------------- control
 
-// K5 (first half): per scenario, Simulation::updateDt and the stop rules;
-// then the prefix of active tiles over scenarios (the work list).
-__global__ void k_begin(Shared sh, int t0_pass) {
+// K5 (first half), run by one CTA: per scenario, the stop rules of the
+// running advance call and Simulation::updateDt (ctl_begin), then the
+// prefix of active tiles over scenarios (the work list of the step).
+// t0_pass: simulate()'s t=0 pass for scenarios that still need it.
+__device__ void begin_scenarios(const Shared& sh, int t0_pass) {
     __shared__ int s_warp[33];
     __shared__ int s_tot;
     const int tid = threadIdx.x;
@@ -95,6 +127,8 @@ __global__ void k_begin(Shared sh, int t0_pass) {
                 } else {
                     c->active = 0;
                 }
+            } else if (n->t0_pending) {
+                c->active = 0;  // added after the last t=0 pass: waits for the next one
             } else {
                 ctl_begin(c, sh.Nx, sh.Ny);
             }
@@ -126,13 +160,36 @@ __global__ void k_begin(Shared sh, int t0_pass) {
     }
 }
 
-// K1 (bookkeeping half): one thread per active tile. Tile t's particles are
-// group d of the 9 neighbour segments t - dir(d) of the current buffer; the
-// descriptor records them, reserves the tile's segment in the next buffer
-// and puts the 4 tiles owning its node window on the grid-tile list.
+__global__ void k_begin(Shared sh, int t0_pass) { begin_scenarios(sh, t0_pass); }
+
+// Start of an advance call: every scenario gets the step budget and the
+// frame-stop rule, then the first step begins.
+__global__ void k_arm_begin(Shared sh, int64_t steps_left, int stop_at_frame) {
+    for (int s = threadIdx.x; s < sh.nscn; s += blockDim.x) {
+        Ctl* c = sh.scn[s].ctl;
+        c->stop = 0;
+        c->frame_hit = 0;
+        c->steps_left = steps_left;
+        c->stop_at_frame = stop_at_frame;
+    }
+    __syncthreads();
+    begin_scenarios(sh, 0);
+}
+
+// K1 (bookkeeping half): one thread per active tile t. Its particles are
+// the stayers of its own segment in the current buffer plus the movers of
+// the 8 neighbour segments that moved to t (those are filtered by cell when
+// read). The descriptor records these 9 candidate ranges and the exact count,
+// reserves t's segment in the next buffer, and puts the 4 tiles owning t's
+// node window on the grid-tile list.
 __global__ void __launch_bounds__(256) k_prep(Shared sh) {
     const int nwork = sh.work_pref[sh.nscn];
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int w0 = blockIdx.x * blockDim.x; w0 < nwork; w0 += stride) {
+        const int w = w0 + threadIdx.x;
+        const bool valid = w < nwork;
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        if (!valid) continue;
         int sid, loc;
         find_work(sh.work_pref, sh.nscn, w, sid, loc);
         const Scn& S = sh.scn[sid];
@@ -143,42 +200,51 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
         TileDesc D;
         D.t = t;
         D.sid = sid;
-        int st[9], en[9];
+        int rs[9], rl[9], cnt = 0;
 #pragma unroll
         for (int d = 0; d < 9; ++d) {
             const int si = ti - dir_i(d), sj = tj - dir_j(d);
-            st[d] = en[d] = 0;
+            rs[d] = rl[d] = 0;
             if (si >= 0 && sj >= 0 && si < sh.TX && sj < sh.TY) {
                 const int s = si * sh.TY + sj;
                 if (S.grp_stamp[cur][s] == seq) {
-                    st[d] = S.grp[cur][s * 10 + d];
-                    en[d] = S.grp[cur][s * 10 + d + 1];
+                    const int32_t* G = S.grp[cur] + s * GRP_STRIDE;
+                    if (d == 4) {
+                        rs[d] = G[0];
+                        rl[d] = G[1] - G[0];
+                    } else {
+                        rs[d] = G[1];
+                        rl[d] = G[2] - G[1];
+                    }
+                    cnt += G[3 + d];
                 }
             }
         }
         int acc = 0;
 #pragma unroll
         for (int d = 0; d < 9; ++d) {
-            D.gstart[d] = st[d];
-            D.gpref[d] = acc;
-            acc += en[d] - st[d];
+            D.rstart[d] = rs[d];
+            D.rpref[d] = acc;
+            acc += rl[d];
         }
-        D.gpref[9] = acc;
-        D.total = acc;
-        D.nxt_off = atomicAdd(&n->cursor, acc);
+        D.rpref[9] = acc;
+        D.total = cnt;
+        D.nxt_off = warp_atomic_add(&n->cursor, cnt, vmask);
         D.pad_ = 0;
         S.slot_of[t] = w;
         const int stamp = n->stepid;
+        int gl[4], ng = 0;
+        int old[4];
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+        for (int k = 0; k < 4; ++k) {
+            const int gi = ti + (k >> 1), gj = tj + (k & 1);
+            old[k] = (gi < sh.TX && gj < sh.TY) ? atomicMax(&S.gt_stamp[gi * sh.TY + gj], stamp) : stamp;
+        }
 #pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const int gi = ti + a, gj = tj + b;
-                if (gi < sh.TX && gj < sh.TY) {
-                    const int g = gi * sh.TY + gj;
-                    if (atomicMax(&S.gt_stamp[g], stamp) < stamp) S.gt_list[atomicAdd(&n->gt_count, 1)] = g;
-                }
-            }
+        for (int k = 0; k < 4; ++k)
+            if (old[k] < stamp) gl[ng++] = (ti + (k >> 1)) * sh.TY + (tj + (k & 1));
+        const int at = warp_atomic_add(&n->gt_count, ng, vmask);
+        for (int k = 0; k < ng; ++k) S.gt_list[at + k] = gl[k];
         sh.desc[w] = D;
     }
     // the last CTA builds the grid-tile work list prefix for k_grid
@@ -209,37 +275,79 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
 
 // ------------------------------------------------------------------- P2G
 
+constexpr int P2G_THREADS = 256;
+
+// Fixed-point accumulation schemes of k_p2g:
+//  ACC_I32   one int32 per sum, 2^-30 of the tile's bound
+//  ACC_HILO  int32 pair: the rounded contribution and, 2^-20 finer, the
+//            part below one quantum -- each contribution keeps about FP32
+//            precision relative to itself; two plain (non-returning) atomics
+//  ACC_I64   one int64 per sum at 2^-52 of the bound
+enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2 };
+
 struct P2GSmem {
-    float node[NQ * TN * TN];
+    long long node[NQ * TN * TN];  // fixed-point sums of the (TILE+2)^2 window (int32 pairs / int64)
     float4 dem[(TILE + 1) * (TILE + 1)];
-    int lc[CHUNK];
-    float2 f[CHUNK];
-    float2 v[CHUNK];
-    float h[CHUNK];
-    float m[CHUNK];
-    float vz[CHUNK];
-    short idx[CHUNK];
     int ccnt[NCELL];
-    int ccur[NCELL];
-    int warp[NCELL / 32 + 1];
+    unsigned bmax[NQ];             // per-quantity bound of one contribution (float bits)
+    int mcc;                       // most particles in one cell of the tile
+    float scale[NQ], iscale[NQ];
     TileDesc d;
 };
 
-// K2: P2G of one tile (src/simulation.cpp:726-798) without atomics on the
-// sums. Each thread owns one base cell of the tile and sums the
-// contributions of that cell's particles to its 3x3 nodes in registers,
-// visiting the particles in a fixed order (the tile's particle sequence,
-// bucketed by cell in shared memory). The register blocks are combined into
-// the shared (TILE+2)^2 node window along j with warp shuffles and along i in
-// 3 conflict-free phases; the window is written as the tile's partial sums.
-__global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
+// Per-particle P2G quantities (src/simulation.cpp:729-756): mass, momentum,
+// m vz, m h, and for the force K = m g cos^2(theta) with the slope of the
+// containing cell (src/complex_terrain.cpp:113-130) and the depth-averaged
+// pressure sigma = -rho g cos^2 h / 2 with h A = m / rho.
+struct PQ {
+    float fx, fy, m, mvx, mvy, mh, mvz, Kgx, Kgy, Khh;
+    int li, lj;
+};
+
+__device__ __forceinline__ PQ load_pq(const PBuf& B, int src, int li, int lj, const float4* dem, float g, float hod, bool outs) {
+    PQ p;
+    const float2 f = B.f[src], v = B.v[src];
+    const float h = B.h[src], m = B.m[src];
+    const float4 dm = dem[(li + (f.x >= 1.f ? 1 : 0)) * (TILE + 1) + (lj + (f.y >= 1.f ? 1 : 0))];
+    const float K = m * g * dm.z * dm.z;
+    p.fx = f.x;
+    p.fy = f.y;
+    p.m = m;
+    p.mvx = m * v.x;
+    p.mvy = m * v.y;
+    p.mh = m * h;
+    p.mvz = outs ? m * B.vz[src] : 0.f;
+    p.Kgx = K * dm.x;
+    p.Kgy = K * dm.y;
+    p.Khh = K * h * hod;
+    p.li = li;
+    p.lj = lj;
+    return p;
+}
+
+// K2: P2G of one tile (src/simulation.cpp:726-798), one thread per particle,
+// sums in 32-bit fixed point with shared-memory integer atomics. Integer
+// addition is exact and associative, so the sums do not depend on the order
+// in which particles arrive: the result is bitwise reproducible without
+// sorting. Pass A finds, per quantity, a bound b on one contribution and the
+// largest particle count of a cell; a node's sum then stays below
+// 9 * cells_max * 0.75 * b, and the scale 2^e is the largest power of two
+// that keeps that below 2^30. The resolution is 2^-30 of that bound, finer
+// than FP32 relative to the largest contribution. Pass B adds the
+// contributions; the window is converted back and written as the partials.
+template <int ACC>
+__global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(Shared sh) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
-    const int tid = threadIdx.x;
-    const int ci = tid / TILE, cj = tid % TILE;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int nwork = sh.work_pref[sh.nscn];
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         load_desc(sh.desc + w, &sm.d);
+        for (int k = tid; k < NQ * TN * TN; k += P2G_THREADS) sm.node[k] = 0;
+        int* node32 = reinterpret_cast<int*>(sm.node);  // ACC_I32: [q][node]; ACC_HILO: hi at [q][node], lo at NQ*TN*TN + [q][node]
+        for (int k = tid; k < NCELL; k += P2G_THREADS) sm.ccnt[k] = 0;
+        if (tid < NQ) sm.bmax[tid] = 0u;
+        if (tid == 0) sm.mcc = 0;
         __syncthreads();
         const Scn& S = sh.scn[sm.d.sid];
         const int t = sm.d.t;
@@ -247,119 +355,116 @@ __global__ void __launch_bounds__(NCELL, 2) k_p2g(Shared sh) {
         SCnt* n = S.cnt;
         const int cur = n->seq & 1;
         const bool outs = n->outs != 0;
-        for (int k = tid; k < (TILE + 1) * (TILE + 1); k += NCELL) {
+        for (int k = tid; k < (TILE + 1) * (TILE + 1); k += P2G_THREADS) {
             const int i = ti * TILE + k / (TILE + 1), j = tj * TILE + k % (TILE + 1);
             sm.dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
         }
-        for (int k = tid; k < NQ * TN * TN; k += NCELL) sm.node[k] = 0.f;
-        const int total = sm.d.total;
+        __syncthreads();
+        const int ncand = sm.d.rpref[9];
         const PBuf B = S.buf[cur];
-        const float g = S.g, ood = S.ood;
-        float acc[9][NQ];
-#pragma unroll
-        for (int a = 0; a < 9; ++a)
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) acc[a][q] = 0.f;
-        for (int c0 = 0; c0 < total; c0 += CHUNK) {
-            const int nc = min(CHUNK, total - c0);
-            sm.ccnt[tid] = 0;
-            __syncthreads();
-            for (int k = tid; k < nc; k += NCELL) {
-                const int src = seq_to_index(c0 + k, sm.d);
-                const int32_t cell = B.cell[src];
-                int li = cell_i(cell) - ti * TILE, lj = cell_j(cell) - tj * TILE;
-                if ((unsigned)li >= TILE || (unsigned)lj >= TILE) {
-                    atomicOr(&S.ctl->err, ERR_MOVE);
-                    li = min(max(li, 0), TILE - 1);
-                    lj = min(max(lj, 0), TILE - 1);
-                }
-                const int lc = li * TILE + lj;
-                sm.lc[k] = lc;
-                sm.f[k] = B.f[src];
-                sm.v[k] = B.v[src];
-                sm.h[k] = B.h[src];
-                sm.m[k] = B.m[src];
-                sm.vz[k] = outs ? B.vz[src] : 0.f;
-                atomicAdd(&sm.ccnt[lc], 1);
+        const float g = S.g, hod = 0.5f * S.ood;
+        // pass A: bounds and cell counts
+        float bm = 0.f, bvx = 0.f, bvy = 0.f, bh = 0.f, bvz = 0.f, bF = 0.f;
+        for (int k = tid; k < ncand; k += P2G_THREADS) {
+            int d;
+            const int src = cand_to_index(k, sm.d, d);
+            const int32_t cell = B.cell[src];
+            const int li = cell_i(cell) - ti * TILE, lj = cell_j(cell) - tj * TILE;
+            if ((unsigned)li >= TILE || (unsigned)lj >= TILE) {
+                if (d == 4) atomicOr(&S.ctl->err, ERR_MOVE);  // a stayer outside its tile
+                continue;
             }
-            __syncthreads();
-            const int my_cnt = sm.ccnt[tid];
-            const int my_start = block_exclusive_scan(my_cnt, sm.warp);
-            sm.ccur[tid] = my_start;
-            __syncthreads();
-            for (int k = tid; k < nc; k += NCELL) sm.idx[atomicAdd(&sm.ccur[sm.lc[k]], 1)] = (short)k;
-            __syncthreads();
-            // this cell's particles in sequence order (insertion sort of the
-            // few indices the scatter above placed in arbitrary order)
-            for (int a = 1; a < my_cnt; ++a) {
-                const short key = sm.idx[my_start + a];
-                int b = a - 1;
-                while (b >= 0 && sm.idx[my_start + b] > key) {
-                    sm.idx[my_start + b + 1] = sm.idx[my_start + b];
-                    --b;
-                }
-                sm.idx[my_start + b + 1] = key;
+            const PQ p = load_pq(B, src, li, lj, sm.dem, g, hod, outs);
+            const int c = atomicAdd(&sm.ccnt[li * TILE + lj], 1) + 1;
+            atomicMax(&sm.mcc, c);
+            bm = fmaxf(bm, p.m);
+            bvx = fmaxf(bvx, fabsf(p.mvx));
+            bvy = fmaxf(bvy, fabsf(p.mvy));
+            bh = fmaxf(bh, p.mh);
+            bvz = fmaxf(bvz, fabsf(p.mvz));
+            bF = fmaxf(bF, p.Khh + fmaxf(fabsf(p.Kgx), fabsf(p.Kgy)));
+        }
+        bm = warp_max(bm);
+        bvx = warp_max(bvx);
+        bvy = warp_max(bvy);
+        bh = warp_max(bh);
+        bvz = warp_max(bvz);
+        bF = warp_max(bF);
+        if (lane == 0) {
+            atomicMax(&sm.bmax[0], __float_as_uint(bm));
+            atomicMax(&sm.bmax[1], __float_as_uint(bvx));
+            atomicMax(&sm.bmax[2], __float_as_uint(bvy));
+            atomicMax(&sm.bmax[3], __float_as_uint(bh));
+            atomicMax(&sm.bmax[4], __float_as_uint(bF));
+            atomicMax(&sm.bmax[5], __float_as_uint(bF));
+            atomicMax(&sm.bmax[6], __float_as_uint(bvz));
+        }
+        __syncthreads();
+        if (tid < NQ) {
+            const float bound = 9.f * (float)sm.mcc * 0.75f * __uint_as_float(sm.bmax[tid]);
+            int e = 0;
+            if (bound > 0.f) {
+                int E;
+                frexpf(bound, &E);  // bound < 2^E
+                e = min(max((ACC == ACC_I64 ? 52 : 30) - E, -120), 120);
             }
-            for (int a = 0; a < my_cnt; ++a) {
-                const int k = sm.idx[my_start + a];
-                const float2 f = sm.f[k], v = sm.v[k];
-                const float h = sm.h[k], m = sm.m[k];
-                float wx[3], wy[3], dwx[3], dwy[3];
-                bspline3(f.x, wx, dwx);
-                bspline3(f.y, wy, dwy);
-                // slope terms of the containing cell (src/complex_terrain.cpp:113-130)
-                const float4 dm = sm.dem[(ci + (f.x >= 1.f ? 1 : 0)) * (TILE + 1) + (cj + (f.y >= 1.f ? 1 : 0))];
-                // gravity along the slope and the depth-averaged pressure
-                // sigma = -rho g cos^2 h / 2 with h A = m / rho
-                // (src/simulation.cpp:744-756, 786-793)
-                const float K = m * g * dm.z * dm.z;
-                const float hh = 0.5f * h * ood;
-                const float mvx = m * v.x, mvy = m * v.y, mh = m * h, mvz = m * sm.vz[k];
+            sm.scale[tid] = ldexpf(1.f, e);
+            sm.iscale[tid] = ldexpf(1.f, -e);
+        }
+        __syncthreads();
+        const float s0 = sm.scale[0], s1 = sm.scale[1], s2 = sm.scale[2], s3 = sm.scale[3], s4 = sm.scale[4], s5 = sm.scale[5],
+                    s6 = sm.scale[6];
+        // pass B: fixed-point contributions
+        for (int k = tid; k < ncand; k += P2G_THREADS) {
+            int d;
+            const int src = cand_to_index(k, sm.d, d);
+            const int32_t cell = B.cell[src];
+            const int li = cell_i(cell) - ti * TILE, lj = cell_j(cell) - tj * TILE;
+            if ((unsigned)li >= TILE || (unsigned)lj >= TILE) continue;
+            const PQ p = load_pq(B, src, li, lj, sm.dem, g, hod, outs);
+            float wx[3], wy[3], dwx[3], dwy[3];
+            bspline3(p.fx, wx, dwx);
+            bspline3(p.fy, wy, dwy);
 #pragma unroll
-                for (int ia = 0; ia < 3; ++ia) {
+            for (int a = 0; a < 3; ++a) {
 #pragma unroll
-                    for (int jb = 0; jb < 3; ++jb) {
-                        const float wgt = wx[ia] * wy[jb];
-                        if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
-                            float* A = acc[ia * 3 + jb];
-                            A[0] += m * wgt;
-                            A[1] += mvx * wgt;
-                            A[2] += mvy * wgt;
-                            A[3] += mh * wgt;
-                            A[4] += K * (hh * dwx[ia] * wy[jb] - dm.x * wgt);
-                            A[5] += K * (hh * dwy[jb] * wx[ia] - dm.y * wgt);
-                            A[6] += mvz * wgt;
+                for (int b = 0; b < 3; ++b) {
+                    const float wgt = wx[a] * wy[b];
+                    if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
+                        const int nd = (li + a) * TN + (lj + b);
+                        const float c[NQ] = {p.m * wgt, p.mvx * wgt, p.mvy * wgt, p.mh * wgt, p.Khh * (dwx[a] * wy[b]) - p.Kgx * wgt,
+                                             p.Khh * (dwy[b] * wx[a]) - p.Kgy * wgt, p.mvz * wgt};
+                        const float sc[NQ] = {s0, s1, s2, s3, s4, s5, s6};
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            if (q == 6 && !outs) continue;
+                            if (ACC == ACC_I64) {
+                                atomicAdd(reinterpret_cast<unsigned long long*>(sm.node + q * TN * TN + nd),
+                                          (unsigned long long)__float2ll_rn(c[q] * sc[q]));
+                            } else {
+                                const float x = c[q] * sc[q];
+                                const int hi = __float2int_rn(x);
+                                atomicAdd(node32 + q * TN * TN + nd, hi);
+                                if (ACC == ACC_HILO) {
+                                    const int lo = __float2int_rn((x - (float)hi) * 1048576.f);
+                                    if (lo) atomicAdd(node32 + (NQ + q) * TN * TN + nd, lo);
+                                }
+                            }
                         }
                     }
                 }
             }
-            __syncthreads();
         }
-        // Combine: node (ci+a, nj) gets acc[a][0] of cell nj, acc[a][1] of
-        // cell nj-1 and acc[a][2] of cell nj-2 (same row of the tile, i.e.
-        // adjacent lanes), then rows are added in 3 phases a = 0, 1, 2.
-#pragma unroll
-        for (int ia = 0; ia < 3; ++ia) {
-            float* row = sm.node + (ci + ia) * TN;
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                const float a0 = acc[ia * 3 + 0][q], a1 = acc[ia * 3 + 1][q], a2 = acc[ia * 3 + 2][q];
-                const float s1 = __shfl_up_sync(0xffffffffu, a1, 1);
-                const float s2 = __shfl_up_sync(0xffffffffu, a2, 2);
-                const float s21 = __shfl_up_sync(0xffffffffu, a2, 1);
-                float val = a0;
-                if (cj >= 1) val += s1;
-                if (cj >= 2) val += s2;
-                row[q * TN * TN + cj] += val;
-                if (cj == TILE - 1) {
-                    row[q * TN * TN + TILE] += a1 + s21;  // cells 15 (b=1) and 14 (b=2)
-                    row[q * TN * TN + TILE + 1] += a2;    // cell 15 (b=2)
-                }
-            }
-            __syncthreads();
-        }
+        __syncthreads();
         float* P = sh.part + (size_t)w * PART_STRIDE;
-        for (int k = tid; k < PART_STRIDE; k += NCELL) P[k] = sm.node[k];
+        for (int k = tid; k < PART_STRIDE; k += P2G_THREADS) {
+            const float is = sm.iscale[k / (TN * TN)];
+            float v;
+            if (ACC == ACC_I64) v = (float)((double)sm.node[k] * (double)is);
+            else if (ACC == ACC_HILO) v = (float)(((double)node32[k] + (double)node32[NQ * TN * TN + k] * (1.0 / 1048576.0)) * (double)is);
+            else v = (float)node32[k] * is;
+            P[k] = v;
+        }
         __syncthreads();
     }
 }
@@ -500,32 +605,6 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
 
 // -------------------------------------------------------------------- G2P
 
-// New base cell and offset of a particle after advection with the PIC
-// velocity of the 3x3 nodes around it. One out-of-line function serves both
-// passes of k_g2p, so both classify every particle identically.
-__device__ __noinline__ void advect(const float4* s_nv, int ci, int cj, int32_t cell, float2 f, float dt_ood, int* ib, int* jb,
-                                   float2* fnew, float2* pic) {
-    float wx[3], wy[3], dwx[3], dwy[3];
-    bspline3(f.x, wx, dwx);
-    bspline3(f.y, wy, dwy);
-    float picx = 0.f, picy = 0.f;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const float w = wx[a] * wy[b];
-            const float4 nv = s_nv[(ci + a) * TN + (cj + b)];
-            picx += nv.x * w;
-            picy += nv.y * w;
-        }
-    const float ux = f.x + dt_ood * picx, uy = f.y + dt_ood * picy;
-    const int ki = (int)floorf(ux - 0.5f), kj = (int)floorf(uy - 0.5f);
-    *ib = cell_i(cell) + ki;
-    *jb = cell_j(cell) + kj;
-    *fnew = make_float2(ux - (float)ki, uy - (float)kj);
-    *pic = make_float2(picx, picy);
-}
-
 __device__ __forceinline__ int dir_of(int ib, int jb, int ti, int tj) {
     int di = (ib >= 0 ? ib / TILE : -1) - ti, dj = (jb >= 0 ? jb / TILE : -1) - tj;
     if (di < -1 || di > 1 || dj < -1 || dj > 1) return -1;
@@ -535,26 +614,30 @@ __device__ __forceinline__ int dir_of(int ib, int jb, int ti, int tj) {
 struct G2PSmem {
     float4 nv[TN * TN];
     float4 dem[(TILE + 1) * (TILE + 1)];
+    int front, back;
     int dcnt[9];
-    int dpref[10];
-    int wtot[NCELL / 32][9];
-    int run[9];
     int blk4[4];
     TileDesc d;
     double red[5][NCELL / 32];
 };
 
 // K4: G2P (src/simulation.cpp:877-940) of one tile: FLIP/PIC blend,
-// advection, depth update, then the particle is written to the next buffer
-// in the group of the tile it moved to. Pass 1 counts the groups, pass 2
-// writes each particle at its stable rank. The block max of |v|^2 and the
-// particle bounding box feed the next step's dt and remesh box (K5).
-__global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __restrict__ z64) {
+// advection, depth update, and the write of the particle into the tile's
+// segment of the next buffer -- stayers from the front, particles that moved
+// to a neighbour tile from the back, with per-direction counts. The block
+// max of |v|^2 and the particle bounding box feed the next step's dt and
+// remesh box (K5).
+__global__ void __launch_bounds__(NCELL, 3) k_g2p(Shared sh, const double* __restrict__ z64) {
     __shared__ G2PSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwork = sh.work_pref[sh.nscn];
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         load_desc(sh.desc + w, &sm.d);
+        if (tid < 9) sm.dcnt[tid] = 0;
+        if (tid == 32) {
+            sm.front = 0;
+            sm.back = 0;
+        }
         __syncthreads();
         const int sid = sm.d.sid;
         const Scn& S = sh.scn[sid];
@@ -569,7 +652,6 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             const int gi = ti + (tid >> 1), gj = tj + (tid & 1);
             sm.blk4[tid] = (gi < sh.TX && gj < sh.TY) ? S.blk_of[gi * sh.TY + gj] : -1;
         }
-        if (tid >= 32 && tid < 41) sm.dcnt[tid - 32] = 0;
         __syncthreads();
         for (int k = tid; k < TN * TN; k += NCELL) {
             const int a = k / TN, b = k % TN;
@@ -588,85 +670,56 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             }
         }
         __syncthreads();
+        const int ncand = sm.d.rpref[9];
         const int total = sm.d.total;
+        const int base = sm.d.nxt_off;
         const PBuf B = S.buf[cur];
         const PBuf O = S.buf[nxt];
         const float dt = (float)c->dt;
         const float dt_ood = dt * S.ood;
         const double dx = c->dx;
-        // pass 1: count the particles per destination group
-        for (int q = tid; q < total; q += NCELL) {
-            const int src = seq_to_index(q, sm.d);
-            const int32_t cell = B.cell[src];
-            const float2 f = B.f[src];
-            const int ci = min(max(cell_i(cell) - ti * TILE, 0), TILE - 1);
-            const int cj = min(max(cell_j(cell) - tj * TILE, 0), TILE - 1);
-            int ib, jb;
-            float2 fn, pic;
-            advect(sm.nv, ci, cj, cell, f, dt_ood, &ib, &jb, &fn, &pic);
-            const int d = dir_of(ib, jb, ti, tj);
-            atomicAdd(&sm.dcnt[d < 0 ? 4 : d], 1);
-        }
-        __syncthreads();
-        if (tid < 10) {
-            int acc = 0;
-            for (int d = 0; d < tid; ++d) acc += sm.dcnt[d];
-            sm.dpref[tid] = acc;
-            S.grp[nxt][t * 10 + tid] = sm.d.nxt_off + acc;
-            if (tid < 9) {
-                sm.run[tid] = 0;
-                if (sm.dcnt[tid]) {
-                    const int tt = (ti + dir_i(tid)) * sh.TY + (tj + dir_j(tid));
-                    if (atomicMax(&S.act_stamp[tt], seq + 1) < seq + 1) {
-                        const int k = atomicAdd(&n->act_count[nxt], 1);
-                        if (k < S.act_cap) S.act_list[nxt][k] = tt;
-                        else atomicOr(&c->err, ERR_CAPACITY);
-                    }
-                }
-            } else {
-                S.grp_stamp[nxt][t] = seq + 1;
-            }
-        }
-        __syncthreads();
-        // pass 2: full update, stable write into the destination groups
         double mnx = INFINITY, mxx = 0.0, mny = INFINITY, mxy = 0.0, vv = 0.0;
-        for (int r0 = 0; r0 < total; r0 += NCELL) {
-            const int q = r0 + tid;
-            const bool valid = q < total;
-            int d = 4, ib = 0, jb = 0;
+        for (int k0 = 0; k0 < ncand; k0 += NCELL) {
+            const int k = k0 + tid;
+            bool valid = k < ncand;
+            int d = 4, ib = 0, jb = 0, src = 0;
+            int32_t cell = 0;
+            if (valid) {
+                int r;
+                src = cand_to_index(k, sm.d, r);
+                cell = B.cell[src];
+                valid = tile_of_cell(cell, sh.TY) == t;
+            }
             float2 fn = make_float2(1.f, 1.f), vn = make_float2(0.f, 0.f);
             float hn = 0.f, m = 0.f, vzp = 0.f;
             double zp = 0.0;
             int32_t pid = 0;
             if (valid) {
-                const int src = seq_to_index(q, sm.d);
-                const int32_t cell = B.cell[src];
                 const float2 f = B.f[src];
                 const float2 v = B.v[src];
                 const float h = B.h[src];
                 m = B.m[src];
                 pid = B.id[src];
-                const int ci = min(max(cell_i(cell) - ti * TILE, 0), TILE - 1);
-                const int cj = min(max(cell_j(cell) - tj * TILE, 0), TILE - 1);
-                float2 pic;
-                advect(sm.nv, ci, cj, cell, f, dt_ood, &ib, &jb, &fn, &pic);
+                const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
                 float wx[3], wy[3], dwx[3], dwy[3];
                 bspline3(f.x, wx, dwx);
                 bspline3(f.y, wy, dwy);
-                float flx = 0.f, fly = 0.f, div = 0.f;
+                float picx = 0.f, picy = 0.f, flx = 0.f, fly = 0.f, div = 0.f;
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
 #pragma unroll
                     for (int b = 0; b < 3; ++b) {
                         const float wgt = wx[a] * wy[b];
                         const float4 nv = sm.nv[(ci + a) * TN + (cj + b)];
+                        picx += nv.x * wgt;
+                        picy += nv.y * wgt;
                         flx += nv.z * wgt;
                         fly += nv.w * wgt;
                         div += (dwx[a] * wy[b]) * nv.x + (dwy[b] * wx[a]) * nv.y;
                     }
                 div *= S.ood;
                 const float fr = S.fr;
-                vn = make_float2(fr * (v.x + flx) + (1.f - fr) * pic.x, fr * (v.y + fly) + (1.f - fr) * pic.y);
+                vn = make_float2(fr * (v.x + flx) + (1.f - fr) * picx, fr * (v.y + fly) + (1.f - fr) * picy);
                 hn = h / (1.f + dt * div);
                 if (need_vz) {
                     const float4 dm = sm.dem[(ci + (f.x >= 1.f ? 1 : 0)) * (TILE + 1) + (cj + (f.y >= 1.f ? 1 : 0))];
@@ -679,6 +732,12 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
 #pragma unroll
                         for (int b = 0; b < 3; ++b) zp += (double)(wx[a] * wy[b]) * z64[(int64_t)(i0 + a) * sh.Ny + (j0 + b)];
                 }
+                // advection with the PIC velocity and re-anchoring of the offset
+                const float ux = f.x + dt_ood * picx, uy = f.y + dt_ood * picy;
+                const int ki = (int)floorf(ux - 0.5f), kj = (int)floorf(uy - 0.5f);
+                ib = cell_i(cell) + ki;
+                jb = cell_j(cell) + kj;
+                fn = make_float2(ux - (float)ki, uy - (float)kj);
                 d = dir_of(ib, jb, ti, tj);
                 if (d < 0) {
                     atomicOr(&c->err, ERR_MOVE);
@@ -688,6 +747,8 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
                     atomicOr(&c->err, ERR_DOMAIN);
                     ib = min(max(ib, 0), sh.Nx - 3);
                     jb = min(max(jb, 0), sh.Ny - 3);
+                    d = dir_of(ib, jb, ti, tj);
+                    if (d < 0) d = 4;
                 }
                 const double px = ((double)ib + (double)fn.x) * dx, py = ((double)jb + (double)fn.y) * dx;
                 mnx = fmin(mnx, px);
@@ -698,26 +759,25 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
                 if (!isfinite(vn.x) || !isfinite(vn.y) || !isfinite(hn) || !isfinite(fn.x) || !isfinite(fn.y))
                     atomicOr(&c->err, ERR_NONFINITE);
             }
-            int rank = 0;
-#pragma unroll
-            for (int dd = 0; dd < 9; ++dd) {
-                const unsigned msk = __ballot_sync(0xffffffffu, valid && d == dd);
-                if (lane == 0) sm.wtot[warp][dd] = __popc(msk);
-                if (valid && d == dd) rank = __popc(msk & ((1u << lane) - 1u));
+            // stayers to the front of the segment, movers to the back
+            const bool stay = valid && d == 4, move = valid && d != 4;
+            const unsigned ms = __ballot_sync(0xffffffffu, stay), mm = __ballot_sync(0xffffffffu, move);
+            int bs = 0, bm = 0;
+            if (lane == 0) {
+                if (ms) bs = atomicAdd(&sm.front, __popc(ms));
+                if (mm) bm = atomicAdd(&sm.back, __popc(mm));
             }
-            __syncthreads();
-            if (tid < 9) {
-                int run = sm.run[tid];
-                for (int wp = 0; wp < NCELL / 32; ++wp) {
-                    const int tmp = sm.wtot[wp][tid];
-                    sm.wtot[wp][tid] = run;
-                    run += tmp;
-                }
-                sm.run[tid] = run;
-            }
-            __syncthreads();
+            bs = __shfl_sync(0xffffffffu, bs, 0);
+            bm = __shfl_sync(0xffffffffu, bm, 0);
+            const unsigned lt = (1u << lane) - 1u;
             if (valid) {
-                const int pos = sm.d.nxt_off + sm.dpref[d] + sm.wtot[warp][d] + rank;
+                int pos;
+                if (stay) {
+                    pos = base + bs + __popc(ms & lt);
+                } else {
+                    pos = base + total - 1 - (bm + __popc(mm & lt));
+                    atomicAdd(&sm.dcnt[d], 1);
+                }
                 O.cell[pos] = pack_cell(ib, jb);
                 O.f[pos] = fn;
                 O.v[pos] = vn;
@@ -727,7 +787,27 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
                 if (need_vz) O.vz[pos] = vzp;
                 if (outs) O.z[pos] = (float)zp;
             }
-            __syncthreads();
+        }
+        __syncthreads();
+        if (tid < 9) {
+            int32_t* G = S.grp[nxt] + t * GRP_STRIDE;
+            const int cnt = tid == 4 ? sm.front : sm.dcnt[tid];
+            G[3 + tid] = cnt;
+            if (tid == 0) {
+                G[0] = base;
+                G[1] = base + sm.front;
+                G[2] = base + sm.front + sm.back;
+                S.grp_stamp[nxt][t] = seq + 1;
+                if (sm.front + sm.back != total) atomicOr(&c->err, ERR_CAPACITY);
+            }
+            if (cnt) {
+                const int tt = (ti + dir_i(tid)) * sh.TY + (tj + dir_j(tid));
+                if (atomicMax(&S.act_stamp[tt], seq + 1) < seq + 1) {
+                    const int kk = atomicAdd(&n->act_count[nxt], 1);
+                    if (kk < S.act_cap) S.act_list[nxt][kk] = tt;
+                    else atomicOr(&c->err, ERR_CAPACITY);
+                }
+            }
         }
         // per-tile reductions into the scenario's control block
         mnx = warp_min(mnx);
@@ -778,6 +858,8 @@ __global__ void __launch_bounds__(NCELL, 2) k_g2p(Shared sh, const double* __res
             n->seq += 1;
             n->vz_valid = n->outs;
         }
+        __syncthreads();
+        begin_scenarios(sh, 0);  // the next step's dt, stop rules and work list
     }
 }
 
