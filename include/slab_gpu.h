@@ -201,6 +201,40 @@ void slab_destroy(slab_ctx* ctx);
  * set; otherwise cap must be >= *n_out. */
 slab_status slab_poisson_disk(double Lx, double Ly, double r, int32_t k, uint64_t seed, double* out_xy, int64_t cap, int64_t* n_out);
 
+/* ---- frame-0 grid without allocation ----------------------------------- */
+
+/* Largest node box slab_initial_grid_static accepts (e.g. 256 x 256). */
+#define SLAB_STATIC_MAX_NODES 65536
+
+/* No counterpart in the reference: an addition of this library for callers
+ * that cannot allocate device memory -- a host framework that reserves the
+ * whole GPU heap itself and forbids cudaMalloc/cudaFree by libraries, or a
+ * real-time loop that may not allocate once running.
+ *
+ * Computes the grid of simulate()'s t=0 pass (P2G and the grid update with
+ * dt = 0) with the FP32 split arithmetic, from particle arrays the caller
+ * already has on the device, into device arrays the caller provides. It
+ * makes no allocation: its scratch is a fixed array compiled into the
+ * library (SLAB_STATIC_MAX_NODES nodes, about 3.9 MB per GPU, held by every
+ * GPU that loads the library until the process exits).
+ *  - d_z: terrain heights on the device, Nx*Ny, i*Ny + j.
+ *  - d_x_xy, d_v_xy (interleaved), d_vz, d_h, d_mass: Np particles.
+ *  - box = {i0, i1, j0, j1}: the inclusive node box of the outputs; every
+ *    particle's 3x3 stencil must lie inside it, at most
+ *    SLAB_STATIC_MAX_NODES nodes (larger boxes are rejected with SLAB_E_ARG).
+ *  - outputs (device, box nodes, flattened (i-i0)*(j1-j0+1) + (j-j0)):
+ *    normalised flow height, grid mass, velocity (interleaved), vz.
+ *  - stream: a cudaStream_t or NULL. The call waits for the stream.
+ * The first call on a device looks up the device address of the scratch
+ * array; make that first call before any stream capture. All calls share
+ * the scratch: calls that overlap on the GPU (other threads, other streams)
+ * race and must be serialised by the caller. On error slab_last_error(NULL)
+ * gives the message. */
+slab_status slab_initial_grid_static(const slab_terrain_desc* terrain, const double* d_z, const slab_params* params, int32_t Np,
+                                     const double* d_x_xy, const double* d_v_xy, const double* d_vz, const double* d_h, const double* d_mass,
+                                     const int32_t box[4], double* d_h_out, double* d_mass_out, double* d_v_out, double* d_vz_out,
+                                     void* stream);
+
 /* Library version string and status-code names. */
 const char* slab_version(void);
 const char* slab_status_name(slab_status s);

@@ -9,6 +9,12 @@
 
 using namespace slab;
 
+namespace slab {
+// message of the last failed context-free call on this thread (slab_last_error(NULL))
+static thread_local std::string t_last_error;
+void set_thread_error(const std::string& msg) { t_last_error = msg; }
+}  // namespace slab
+
 struct slab_ctx {
     Terrain terrain;
     slab_params params{};
@@ -369,7 +375,7 @@ int64_t slab_kernel_launches(const slab_ctx* c) {
     return c->extra_launches + (c->path ? c->path->launches() : 0);
 }
 
-const char* slab_last_error(const slab_ctx* c) { return c ? c->err.c_str() : "null context"; }
+const char* slab_last_error(const slab_ctx* c) { return c ? c->err.c_str() : slab::t_last_error.c_str(); }
 
 void slab_destroy(slab_ctx* c) {
     if (!c) return;
