@@ -189,6 +189,39 @@ int64_t slab_kernel_launches(const slab_ctx* ctx);
 const char* slab_last_error(const slab_ctx* ctx);
 void slab_destroy(slab_ctx* ctx);
 
+/* ---- batched ensembles ---------------------------------------------------
+ * Many release scenarios of uneven size on one shared terrain, each with its
+ * own slab_params (friction law and coefficients, total_time, dt_max, ...),
+ * advanced together by the FP32 split step: every kernel launch covers all
+ * running scenarios, each with its own adaptive dt (Simulation::updateDt per
+ * scenario), replayed from CUDA graphs. A scenario's results are bitwise the
+ * same as running it alone through slab_ctx with SLAB_FP32_SPLIT. There is
+ * no reference counterpart: the reference runs one scenario per process
+ * (src/main.cpp:29-57). */
+typedef struct slab_batch slab_batch;
+
+/* capacity_hint: node blocks (16x16 nodes, 9 KB each) to reserve up front,
+ * 0 = automatic; the pool grows as scenarios spread. */
+slab_status slab_batch_create(const slab_terrain_desc* terrain, const double* z, int32_t max_scenarios, int64_t capacity_hint,
+                              slab_batch** out);
+slab_status slab_batch_set_stream(slab_batch* b, void* cuda_stream);
+/* Add a scenario (arrays as slab_upload_particles); params->precision must be
+ * SLAB_FP32_SPLIT. Its t=0 pass runs with the next slab_batch_run. */
+slab_status slab_batch_add(slab_batch* b, const slab_params* params, int32_t Np, const double* x_xy, const double* v_xy,
+                           const double* vz, const double* h, const double* A, const double* mass, const double* z, int32_t* scenario_id);
+/* Advance every scenario until each has reached its total_time, or for at
+ * most max_steps steps of the batch. */
+slab_status slab_batch_run(slab_batch* b, int64_t max_steps, int64_t* steps_out);
+slab_status slab_batch_state(slab_batch* b, int32_t scenario_id, double* time, int32_t* frame, int64_t* steps);
+slab_status slab_batch_download_particles(slab_batch* b, int32_t scenario_id, double* x_xy, double* v_xy, double* vz, double* h,
+                                          double* A, double* mass, double* z);
+slab_status slab_batch_download_max(slab_batch* b, int32_t scenario_id, double* h_max, double* v_max2);
+/* out[0] = particle-steps, out[1] = active node-steps, over all scenarios. */
+slab_status slab_batch_work_counters(slab_batch* b, int64_t out[2]);
+int64_t slab_batch_kernel_launches(const slab_batch* b);
+const char* slab_batch_last_error(const slab_batch* b);
+void slab_batch_destroy(slab_batch* b);
+
 /* ---- setup utilities (host only; no device work) ---------------------- */
 
 /* Poisson-disk samples in [0,Lx] x [0,Ly] with minimum distance r and k

@@ -1,6 +1,7 @@
 // The C ABI of libslab_gpu.so (include/slab_gpu.h): context management,
 // argument checks, the host side of the step loop (arming the device control
 // block, replaying step graphs until a frame), and error translation.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -128,9 +129,22 @@ void advance(slab_ctx* c, int64_t nsteps, bool stop_at_frame, int64_t* steps_out
     pull_ctl(c);
     const int64_t s0 = c->h_ctl->steps;
     if (!stop_at_frame) {
-        // the step budget is on the device: enqueue enough chunks, sync once
-        enqueue_nsteps(c, nsteps);
-        pull_ctl(c);
+        // the step budget is on the device; enqueue up to 8 chunks, then look
+        // at the control block, so a run that stops at total_time long before
+        // the budget does not keep the host enqueueing empty steps
+        arm(c, nsteps, 0);
+        const int64_t poll = 8 * (int64_t)c->chunk;
+        int64_t k = 0;
+        while (k < nsteps) {
+            const int64_t end = std::min(nsteps, k + poll);
+            for (; k + c->chunk <= end; k += c->chunk) c->path->enqueue_steps(c->chunk);
+            if (k < end) {
+                c->path->enqueue_steps((int)(end - k));
+                k = end;
+            }
+            pull_ctl(c);
+            if (c->h_ctl->stop || c->h_ctl->err) break;
+        }
     } else {
         arm(c, nsteps, 1);
         double last_time = c->h_ctl->time;

@@ -22,10 +22,10 @@ class Engine32 {
         dptr<float2> f[2], v[2];
         dptr<float> h[2], m[2], vz[2], z[2];
         dptr<int32_t> act_stamp, slot_of, nxt_off, gt_stamp, gt_list, blk_of;
-        dptr<SCnt> cnt;
+        SCnt* cnt = nullptr;  // in the engine's counter array
     };
 
-    Engine32(const Terrain& t, cudaStream_t s, int max_scenarios, int64_t blk_cap);
+    Engine32(const Terrain& t, cudaStream_t s, int max_scenarios, int64_t blk_cap, bool batch = false);
     ~Engine32();
 
     int add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, const double* x, const double* v, const double* vz,
@@ -40,6 +40,10 @@ class Engine32 {
     void enqueue_steps(int chunk);
     PhaseTimer timer;
     SCnt counters(int sid);
+    // grow per-scenario tile lists and the node-block pool when half full;
+    // returns true if anything was reallocated
+    bool check_capacity();
+    void grow_blocks(int cap);
     void download_particles(int sid, double* x, double* v, double* vz, double* h, double* A, double* m, double* z, double rho);
     void download_grid(int sid, slab_grid_view* gv);
     void download_max(int sid, double* hmax, double* vmax2);
@@ -49,6 +53,7 @@ class Engine32 {
     const Terrain& T;
     cudaStream_t st;
     int max_scn;
+    bool batch = false;
     int nscn = 0;
     int TX = 0, TY = 0, ntiles = 0;
     int blk_cap = 0;
@@ -67,6 +72,8 @@ class Engine32 {
     dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz;
     dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_grid_pref;
     dptr<Scn> d_scn;
+    dptr<SCnt> d_cnt;
+    std::vector<SCnt> h_cnt;
     dptr<TileDesc> d_desc;
     dptr<float> d_part;
     StepGraphs graphs;

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 #include <cstring>
 #include <vector>
 
@@ -47,7 +48,8 @@ __global__ void k_gather_nodes(const int32_t* __restrict__ blk_of, const int32_t
 
 }  // namespace k32
 
-Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_cap) : T(t), st(s), max_scn(max_scn) {
+Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_cap, bool batch)
+    : T(t), st(s), max_scn(max_scn), batch(batch) {
     TX = (t.Nx + TILE - 1) / TILE;
     TY = (t.Ny + TILE - 1) / TILE;
     ntiles = TX * TY;
@@ -64,6 +66,8 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     d_work_pref = dalloc<int32_t>(max_scn + 1);
     d_grid_pref = dalloc<int32_t>(max_scn + 1);
     d_scn = dalloc<Scn>(max_scn);
+    d_cnt = dalloc<SCnt>(max_scn);
+    h_cnt.resize(max_scn);
     SLAB_CUDA(cudaMemsetAsync(d_hmax.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
     SLAB_CUDA(cudaMemsetAsync(d_vmax2.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
     SLAB_CUDA(cudaMemsetAsync(d_blk_stamp.get(), 0xff, (size_t)this->blk_cap * sizeof(int32_t), st));
@@ -135,7 +139,9 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     S.Np = Np;
     S.ctl = ctl;
     S.h_ctl = h_ctl;
-    S.act_cap = std::max(1, std::min(ntiles, Np));
+    // a single scenario gets the safe bound; in a batch the lists start at an
+    // estimate (>= 4 particles per active tile) and grow between chunks
+    S.act_cap = batch ? std::max(1, std::min(ntiles, Np / 4 + 256)) : std::max(1, std::min(ntiles, Np));
     for (int b = 0; b < 2; ++b) {
         S.cell[b] = dalloc<int32_t>(Np);
         S.f[b] = dalloc<float2>(Np);
@@ -155,7 +161,7 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     S.gt_stamp = dalloc<int32_t>(ntiles);
     S.gt_list = dalloc<int32_t>(ntiles);
     S.blk_of = dalloc<int32_t>(ntiles);
-    S.cnt = dalloc<SCnt>(1);
+    S.cnt = d_cnt.get() + sid;
     ensure_work_cap(work_cap_total + S.act_cap);
     work_cap_total += S.act_cap;
 
@@ -232,7 +238,7 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     c0.act_count[0] = (int)alist.size();
     c0.t0_pending = 1;
     c0.vz_valid = 1;
-    h2d(S.cnt.get(), &c0, 1, st);
+    h2d(S.cnt, &c0, 1, st);
     // particle box and max speed for the first step (Simulation::updateDt / remesh)
     h_ctl->pos_acc[0] = (uint64_t)__builtin_bit_cast(uint64_t, mnx);
     h_ctl->pos_acc[1] = (uint64_t)__builtin_bit_cast(uint64_t, mxx);
@@ -247,7 +253,7 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     Scn& D = host_scn[sid];
     D = Scn{};
     D.ctl = ctl;
-    D.cnt = S.cnt.get();
+    D.cnt = S.cnt;
     D.g = (float)p.gravity;
     D.rho = (float)p.rho;
     D.fr = (float)p.flip_ratio;
@@ -342,9 +348,64 @@ void Engine32::enqueue_steps(int chunk) {
 
 SCnt Engine32::counters(int sid) {
     SCnt c;
-    d2h(&c, stores[sid].cnt.get(), 1, st);
+    d2h(&c, stores[sid].cnt, 1, st);
     SLAB_CUDA(cudaStreamSynchronize(st));
     return c;
+}
+
+bool Engine32::check_capacity() {
+    if (!nscn) return false;
+    d2h(h_cnt.data(), d_cnt.get(), nscn, st);
+    int32_t used_blocks = 0;
+    d2h(&used_blocks, d_misc.get(), 1, st);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    bool grew = false;
+    for (int s = 0; s < nscn; ++s) {
+        const int need = std::max(h_cnt[s].act_count[0], h_cnt[s].act_count[1]);
+        Store& S = stores[s];
+        if (2 * need > S.act_cap && S.act_cap < ntiles) {
+            const int cap = std::min(ntiles, std::max(2 * S.act_cap, 4 * need));
+            for (int b = 0; b < 2; ++b) {
+                dptr<int32_t> nl = dalloc<int32_t>(cap);
+                SLAB_CUDA(cudaMemcpyAsync(nl.get(), S.act_list[b].get(), S.act_cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+                S.act_list[b] = std::move(nl);
+                host_scn[s].act_list[b] = S.act_list[b].get();
+            }
+            work_cap_total += cap - S.act_cap;
+            S.act_cap = cap;
+            host_scn[s].act_cap = cap;
+            h2d(d_scn.get() + s, &host_scn[s], 1, st);
+            grew = true;
+        }
+    }
+    if (grew) ensure_work_cap(work_cap_total);
+    if (2 * (int64_t)used_blocks > blk_cap) {
+        grow_blocks((int)std::min<int64_t>((int64_t)blk_cap * 2, INT32_MAX / NCELL));
+        grew = true;
+    }
+    if (grew) SLAB_CUDA(cudaStreamSynchronize(st));
+    return grew;
+}
+
+void Engine32::grow_blocks(int cap) {
+    if (cap <= blk_cap) return;
+    auto grow = [&](auto& p, size_t per, int fill) {
+        using E = typename std::remove_reference<decltype(*p.get())>::type;
+        auto np = dalloc<E>((size_t)cap * per);
+        SLAB_CUDA(cudaMemsetAsync(np.get(), fill, (size_t)cap * per * sizeof(E), st));
+        SLAB_CUDA(cudaMemcpyAsync(np.get(), p.get(), (size_t)blk_cap * per * sizeof(E), cudaMemcpyDeviceToDevice, st));
+        p = std::move(np);
+    };
+    grow(d_nv, NCELL, 0);
+    grow(d_hmax, NCELL, 0);
+    grow(d_vmax2, NCELL, 0);
+    grow(d_oh, NCELL, 0);
+    grow(d_om, NCELL, 0);
+    grow(d_ovz, NCELL, 0);
+    grow(d_blk_stamp, 1, 0xff);
+    grow(d_blk_owner, 1, 0xff);
+    blk_cap = cap;
+    graphs.clear();
 }
 
 void Engine32::download_particles(int sid, double* x, double* v, double* vz, double* h, double* A, double* m, double* z, double rho) {

@@ -240,3 +240,92 @@ class Slab:
         out = np.zeros(5)
         self._check(self.L.slab_get_phase_times(self.h, _dp(out)))
         return out
+
+
+class Batch:
+    """Many scenarios on one shared terrain, advanced together (FP32 split)."""
+
+    def __init__(self, z: np.ndarray, dx: float, max_scenarios: int, capacity_hint: int = 0):
+        self.L = L = lib()
+        vp = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.slab_batch_create.argtypes = [C.POINTER(TerrainDesc), dp, C.c_int32, C.c_int64, C.POINTER(vp)]
+        L.slab_batch_set_stream.argtypes = [vp, vp]
+        L.slab_batch_add.argtypes = [vp, C.POINTER(Params), C.c_int32] + [dp] * 7 + [C.POINTER(C.c_int32)]
+        L.slab_batch_run.argtypes = [vp, C.c_int64, C.POINTER(C.c_int64)]
+        L.slab_batch_state.argtypes = [vp, C.c_int32, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+        L.slab_batch_download_particles.argtypes = [vp, C.c_int32] + [dp] * 7
+        L.slab_batch_download_max.argtypes = [vp, C.c_int32, dp, dp]
+        L.slab_batch_work_counters.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.slab_batch_kernel_launches.argtypes = [vp]
+        L.slab_batch_kernel_launches.restype = C.c_int64
+        L.slab_batch_last_error.argtypes = [vp]
+        L.slab_batch_last_error.restype = C.c_char_p
+        L.slab_batch_destroy.argtypes = [vp]
+        self.Nx, self.Ny = z.shape
+        zz = np.ascontiguousarray(z, dtype=np.float64)
+        td = TerrainDesc(self.Nx, self.Ny, float(dx), 0.0, 0.0)
+        h = C.c_void_p()
+        code = L.slab_batch_create(C.byref(td), _dp(zz), int(max_scenarios), int(capacity_hint), C.byref(h))
+        if code:
+            raise SlabError(code, (L.slab_last_error(None) or b"").decode())
+        self.h = h
+        self.Np = []
+        self._params = []
+
+    def _check(self, code):
+        if code:
+            raise SlabError(code, (self.L.slab_batch_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.slab_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_stream(self, stream_handle: int):
+        self._check(self.L.slab_batch_set_stream(self.h, C.c_void_p(stream_handle)))
+
+    def add(self, cfg: dict, P: dict) -> int:
+        prm = make_params(cfg, FP32_SPLIT)
+        self._params.append(prm)
+        n = len(P["h"])
+        arrs = [np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "v", "vz", "h", "A", "mass", "z")]
+        sid = C.c_int32()
+        self._check(self.L.slab_batch_add(self.h, C.byref(prm), n, *[_dp(a) for a in arrs], C.byref(sid)))
+        self.Np.append(n)
+        return sid.value
+
+    def run(self, max_steps: int = 1 << 40) -> int:
+        s = C.c_int64()
+        self._check(self.L.slab_batch_run(self.h, int(max_steps), C.byref(s)))
+        return s.value
+
+    def state(self, sid: int):
+        t, f, s = C.c_double(), C.c_int32(), C.c_int64()
+        self._check(self.L.slab_batch_state(self.h, sid, C.byref(t), C.byref(f), C.byref(s)))
+        return t.value, f.value, s.value
+
+    def particles(self, sid: int) -> dict:
+        n = self.Np[sid]
+        out = {k: np.zeros(2 * n if k in ("x", "v") else n) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
+        self._check(self.L.slab_batch_download_particles(self.h, sid, *[_dp(out[k]) for k in ("x", "v", "vz", "h", "A", "mass", "z")]))
+        out["x"] = out["x"].reshape(n, 2)
+        out["v"] = out["v"].reshape(n, 2)
+        return out
+
+    def max_maps(self, sid: int):
+        hm = np.zeros(self.Nx * self.Ny)
+        vm = np.zeros(self.Nx * self.Ny)
+        self._check(self.L.slab_batch_download_max(self.h, sid, _dp(hm), _dp(vm)))
+        return hm.reshape(self.Nx, self.Ny), vm.reshape(self.Nx, self.Ny)
+
+    def work_counters(self):
+        out = (C.c_int64 * 2)()
+        self._check(self.L.slab_batch_work_counters(self.h, out))
+        return int(out[0]), int(out[1])
+
+    def kernel_launches(self) -> int:
+        return self.L.slab_batch_kernel_launches(self.h)
