@@ -222,6 +222,49 @@ int64_t slab_batch_kernel_launches(const slab_batch* b);
 const char* slab_batch_last_error(const slab_batch* b);
 void slab_batch_destroy(slab_batch* b);
 
+/* ---- serving -------------------------------------------------------------
+ * A request loop with continuous batching. Submitted scenario solves wait in
+ * a queue; a worker thread that owns the GPU admits them into free scenario
+ * slots while their estimated HBM footprint fits the budget, runs them in
+ * chunks of batched steps together with every other running scenario (each
+ * with its own dt and friction), keeps their state on the device until they
+ * reach total_time, then stores the result in host memory and frees the
+ * slot. Results are bitwise the same as a solo FP32_SPLIT run. No reference
+ * counterpart (the reference is a single-scenario CLI, src/main.cpp:29-57). */
+typedef struct slab_server slab_server;
+typedef struct slab_server_config {
+    int32_t max_scenarios;    /* concurrent scenario slots */
+    int32_t chunk_steps;      /* batched steps between admissions (0 = 32) */
+    int64_t hbm_budget_bytes; /* admission budget (0 = half the free memory at creation) */
+} slab_server_config;
+
+/* request states reported by slab_server_poll */
+enum { SLAB_REQ_QUEUED = 0, SLAB_REQ_RUNNING = 1, SLAB_REQ_DONE = 2, SLAB_REQ_CANCELLED = 3, SLAB_REQ_FAILED = 4 };
+
+slab_status slab_server_create(const slab_terrain_desc* terrain, const double* z, const slab_server_config* config, slab_server** out);
+/* Copy a scenario into the queue and return at once (params->precision must
+ * be SLAB_FP32_SPLIT; arrays as slab_upload_particles). */
+slab_status slab_server_submit(slab_server* s, const slab_params* params, int32_t Np, const double* x_xy, const double* v_xy,
+                               const double* vz, const double* h, const double* A, const double* mass, const double* z, int64_t* request_id);
+slab_status slab_server_poll(slab_server* s, int64_t request_id, int32_t* state, double* seconds_to_result);
+/* Block until the request is done (SLAB_E_TIMEOUT after timeout_s). */
+slab_status slab_server_wait(slab_server* s, int64_t request_id, double timeout_s);
+/* Result of a finished request: the node box {i0, i1, j0, j1} covered by its
+ * flow, h_max and v_max2 over that box ((i-i0)*(j1-j0+1) + (j-j0); at most
+ * cap_nodes), the final particles in upload order (any pointer may be NULL),
+ * and info = {steps, simulated time, seconds to result, seconds queued}. */
+slab_status slab_server_result(slab_server* s, int64_t request_id, int32_t box[4], double* h_max, double* v_max2, int64_t cap_nodes,
+                               double* x_xy, double* v_xy, double* h, double* mass, double* info);
+slab_status slab_server_cancel(slab_server* s, int64_t request_id);
+/* Wait until no request is queued or running. */
+slab_status slab_server_drain(slab_server* s, double timeout_s);
+/* out = {completed, p50 and p99 seconds to result, completed per second
+ * since the first submission, particle-steps, batched steps, seconds the
+ * worker was busy, bytes admitted now}. */
+slab_status slab_server_stats(slab_server* s, double out[8]);
+const char* slab_server_last_error(const slab_server* s);
+void slab_server_destroy(slab_server* s);
+
 /* ---- setup utilities (host only; no device work) ---------------------- */
 
 /* Poisson-disk samples in [0,Lx] x [0,Ly] with minimum distance r and k

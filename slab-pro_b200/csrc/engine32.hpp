@@ -3,6 +3,7 @@
 #pragma once
 
 #include <deque>
+#include <memory>
 #include <vector>
 
 #include "engine.hpp"
@@ -28,8 +29,9 @@ class Engine32 {
     Engine32(const Terrain& t, cudaStream_t s, int max_scenarios, int64_t blk_cap, bool batch = false);
     ~Engine32();
 
+    // want_slot >= 0: use that free slot (or the next unused one)
     int add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, const double* x, const double* v, const double* vz,
-                     const double* h, const double* m, const double* z);
+                     const double* h, const double* m, const double* z, int want_slot = -1);
     void launch_begin(int t0);
     void launch_t0();
     void launch_step();
@@ -44,6 +46,12 @@ class Engine32 {
     // returns true if anything was reallocated
     bool check_capacity();
     void grow_blocks(int cap);
+    // free a finished scenario's slot: its memory, its node blocks (back to
+    // the pool, zeroed) and its control block (replaced by empty_ctl)
+    void retire(int sid, const Ctl& empty_ctl);
+    // node box covered by the scenario's blocks; box[1] < box[0] if none
+    void box_of_blocks(int sid, int box[4]);
+    void download_max_box(int sid, const int box[4], double* hmax, double* vmax2);
     void download_particles(int sid, double* x, double* v, double* vz, double* h, double* A, double* m, double* z, double rho);
     void download_grid(int sid, slab_grid_view* gv);
     void download_max(int sid, double* hmax, double* vmax2);
@@ -62,7 +70,8 @@ class Engine32 {
     int64_t work_cap_total = 0;
     void ensure_work_cap(int64_t need);
     int64_t nlaunch = 0;
-    std::deque<Store> stores;
+    std::vector<std::unique_ptr<Store>> slots;  // scenario slots; empty after retire
+    std::vector<int> free_slots;
     std::vector<Scn> host_scn;
 
   private:
@@ -70,7 +79,7 @@ class Engine32 {
                                     bool with_v);
     dptr<float4> d_nv;
     dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz;
-    dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_grid_pref;
+    dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_grid_pref, d_free_blocks;
     dptr<Scn> d_scn;
     dptr<SCnt> d_cnt;
     std::vector<SCnt> h_cnt;

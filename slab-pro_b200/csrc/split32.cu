@@ -68,6 +68,8 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     d_scn = dalloc<Scn>(max_scn);
     d_cnt = dalloc<SCnt>(max_scn);
     h_cnt.resize(max_scn);
+    slots.resize(max_scn);
+    d_free_blocks = dalloc<int32_t>(this->blk_cap);
     SLAB_CUDA(cudaMemsetAsync(d_hmax.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
     SLAB_CUDA(cudaMemsetAsync(d_vmax2.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
     SLAB_CUDA(cudaMemsetAsync(d_blk_stamp.get(), 0xff, (size_t)this->blk_cap * sizeof(int32_t), st));
@@ -118,7 +120,99 @@ Shared Engine32::shared() const {
     sh.desc = d_desc.get();
     sh.part = d_part.get();
     sh.work_cap = work_cap;
+    sh.free_blocks = d_free_blocks.get();
+    sh.free_count = d_misc.get() + 4;
     return sh;
+}
+
+namespace k32 {
+// Blocks of a retired scenario: maxima and stamps reset before reuse.
+__global__ void k_release_blocks(const int32_t* ids, int n, float* hmax, float* vmax2, int32_t* stamp, int32_t* owner) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)n * NCELL; k += (int64_t)gridDim.x * blockDim.x) {
+        const int b = ids[k / NCELL];
+        const size_t e = (size_t)b * NCELL + (k % NCELL);
+        hmax[e] = 0.f;
+        vmax2[e] = 0.f;
+        if (k % NCELL == 0) {
+            stamp[b] = -1;
+            owner[b] = -1;
+        }
+    }
+}
+}  // namespace k32
+
+void Engine32::retire(int sid, const Ctl& empty_ctl) {
+    if (sid < 0 || sid >= nscn || !slots[sid]) throw Error{SLAB_E_NOTFOUND, "no scenario in this slot"};
+    Store& S = *slots[sid];
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    std::vector<int32_t> blk_of(ntiles);
+    d2h(blk_of.data(), S.blk_of.get(), ntiles, st);
+    int32_t free_count = 0;
+    d2h(&free_count, d_misc.get() + 4, 1, st);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    std::vector<int32_t> ids;
+    for (int32_t b : blk_of)
+        if (b >= 0) ids.push_back(b);
+    if (!ids.empty()) {
+        dptr<int32_t> d_ids = dalloc<int32_t>(ids.size());
+        h2d(d_ids.get(), ids.data(), ids.size(), st);
+        const int blocks = (int)std::min<int64_t>(((int64_t)ids.size() * NCELL + 255) / 256, 148 * 8);
+        k32::k_release_blocks<<<blocks, 256, 0, st>>>(d_ids.get(), (int)ids.size(), d_hmax.get(), d_vmax2.get(), d_blk_stamp.get(),
+                                                      d_blk_owner.get());
+        SLAB_CUDA(cudaGetLastError());
+        SLAB_CUDA(cudaMemcpyAsync(d_free_blocks.get() + free_count, d_ids.get(), ids.size() * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+        const int32_t nf = free_count + (int32_t)ids.size();
+        h2d(d_misc.get() + 4, &nf, 1, st);
+        SLAB_CUDA(cudaStreamSynchronize(st));
+    }
+    // an empty slot: a stopped control block and no tiles
+    SCnt zero{};
+    h2d(S.cnt, &zero, 1, st);
+    h2d(S.ctl, &empty_ctl, 1, st);
+    Scn D = Scn{};
+    D.ctl = S.ctl;
+    D.cnt = S.cnt;
+    h2d(d_scn.get() + sid, &D, 1, st);
+    host_scn[sid] = D;
+    work_cap_total -= S.act_cap;
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    slots[sid].reset();
+    free_slots.push_back(sid);
+}
+
+void Engine32::box_of_blocks(int sid, int box[4]) {
+    Store& S = *slots[sid];
+    std::vector<int32_t> blk_of(ntiles);
+    d2h(blk_of.data(), S.blk_of.get(), ntiles, st);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+    int ti0 = TX, ti1 = -1, tj0 = TY, tj1 = -1;
+    for (int t = 0; t < ntiles; ++t)
+        if (blk_of[t] >= 0) {
+            ti0 = std::min(ti0, t / TY);
+            ti1 = std::max(ti1, t / TY);
+            tj0 = std::min(tj0, t % TY);
+            tj1 = std::max(tj1, t % TY);
+        }
+    if (ti1 < 0) {
+        box[0] = box[2] = 0;
+        box[1] = box[3] = -1;
+        return;
+    }
+    box[0] = ti0 * TILE;
+    box[1] = std::min(T.Nx - 1, ti1 * TILE + TILE - 1);
+    box[2] = tj0 * TILE;
+    box[3] = std::min(T.Ny - 1, tj1 * TILE + TILE - 1);
+}
+
+void Engine32::download_max_box(int sid, const int box[4], double* hmax, double* vmax2) {
+    const int nI = box[1] - box[0] + 1, nJ = box[3] - box[2] + 1;
+    if (nI <= 0 || nJ <= 0) return;
+    const std::vector<float> f = gather_nodes(sid, -1, box[0], box[2], nI, nJ, {d_hmax.get(), d_vmax2.get()}, false);
+    const size_t n = (size_t)nI * nJ;
+    for (size_t k = 0; k < n; ++k) {
+        if (hmax) hmax[k] = f[k];
+        if (vmax2) vmax2[k] = f[n + k];
+    }
 }
 
 void Engine32::ensure_work_cap(int64_t need) {
@@ -132,10 +226,28 @@ void Engine32::ensure_work_cap(int64_t need) {
 }
 
 int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, const double* x, const double* v, const double* vz,
-                           const double* h, const double* m, const double* z) {
-    if (nscn >= max_scn) throw Error{SLAB_E_OOM, "scenario capacity exceeded"};
-    const int sid = nscn;
-    Store& S = stores.emplace_back();
+                           const double* h, const double* m, const double* z, int want_slot) {
+    int sid;
+    if (want_slot >= 0) {
+        auto it = std::find(free_slots.begin(), free_slots.end(), want_slot);
+        if (it != free_slots.end()) {
+            free_slots.erase(it);
+        } else if (want_slot == nscn && nscn < max_scn) {
+        } else {
+            throw Error{SLAB_E_STATE, "scenario slot is not free"};
+        }
+        sid = want_slot;
+        // slots between the high-water mark and want_slot would stay unused: not allowed
+        if (sid > nscn) throw Error{SLAB_E_STATE, "scenario slots must be filled in order"};
+    } else if (!free_slots.empty()) {
+        sid = free_slots.back();
+        free_slots.pop_back();
+    } else {
+        if (nscn >= max_scn) throw Error{SLAB_E_OOM, "scenario capacity exceeded"};
+        sid = nscn;
+    }
+    slots[sid].reset(new Store());
+    Store& S = *slots[sid];
     S.Np = Np;
     S.ctl = ctl;
     S.h_ctl = h_ctl;
@@ -282,8 +394,10 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     D.blk_of = S.blk_of.get();
     D.act_cap = S.act_cap;
     h2d(d_scn.get() + sid, &D, 1, st);
-    nscn += 1;
-    graphs.clear();
+    if (sid == nscn) {
+        nscn += 1;
+        graphs.clear();  // the step graphs carry the scenario count
+    }
     return sid;
 }
 
@@ -348,7 +462,7 @@ void Engine32::enqueue_steps(int chunk) {
 
 SCnt Engine32::counters(int sid) {
     SCnt c;
-    d2h(&c, stores[sid].cnt, 1, st);
+    d2h(&c, (*slots[sid]).cnt, 1, st);
     SLAB_CUDA(cudaStreamSynchronize(st));
     return c;
 }
@@ -361,8 +475,9 @@ bool Engine32::check_capacity() {
     SLAB_CUDA(cudaStreamSynchronize(st));
     bool grew = false;
     for (int s = 0; s < nscn; ++s) {
+        if (!slots[s]) continue;
         const int need = std::max(h_cnt[s].act_count[0], h_cnt[s].act_count[1]);
-        Store& S = stores[s];
+        Store& S = (*slots[s]);
         if (2 * need > S.act_cap && S.act_cap < ntiles) {
             const int cap = std::min(ntiles, std::max(2 * S.act_cap, 4 * need));
             for (int b = 0; b < 2; ++b) {
@@ -404,12 +519,13 @@ void Engine32::grow_blocks(int cap) {
     grow(d_ovz, NCELL, 0);
     grow(d_blk_stamp, 1, 0xff);
     grow(d_blk_owner, 1, 0xff);
+    grow(d_free_blocks, 1, 0);
     blk_cap = cap;
     graphs.clear();
 }
 
 void Engine32::download_particles(int sid, double* x, double* v, double* vz, double* h, double* A, double* m, double* z, double rho) {
-    Store& S = stores[sid];
+    Store& S = (*slots[sid]);
     const SCnt c = counters(sid);
     const int b = c.seq & 1;
     const int Np = S.Np;
@@ -452,7 +568,7 @@ void Engine32::download_particles(int sid, double* x, double* v, double* vz, dou
 
 std::vector<float> Engine32::gather_nodes(int sid, int stepid, int i0, int j0, int nI, int nJ, const std::vector<const float*>& fields,
                                           bool with_v) {
-    Store& S = stores[sid];
+    Store& S = (*slots[sid]);
     const int64_t total = (int64_t)nI * nJ;
     const int nout = (int)fields.size() + (with_v ? 2 : 0);
     std::vector<float> host((size_t)nout * total);
@@ -470,7 +586,7 @@ std::vector<float> Engine32::gather_nodes(int sid, int stepid, int i0, int j0, i
 }
 
 void Engine32::download_grid(int sid, slab_grid_view* gv) {
-    Store& S = stores[sid];
+    Store& S = (*slots[sid]);
     d2h(S.h_ctl, S.ctl, 1, st);
     const SCnt c = counters(sid);
     const int i0 = S.h_ctl->box[0], i1 = S.h_ctl->box[1], j0 = S.h_ctl->box[2], j1 = S.h_ctl->box[3];
@@ -503,7 +619,7 @@ void Engine32::download_max(int sid, double* hmax, double* vmax2) {
 }
 
 void Engine32::conservation(int sid, double out[4], double rho) {
-    Store& S = stores[sid];
+    Store& S = (*slots[sid]);
     std::vector<double> v(2 * (size_t)S.Np), m(S.Np);
     download_particles(sid, nullptr, v.data(), nullptr, nullptr, nullptr, m.data(), nullptr, rho);
     double M = 0, Px = 0, Py = 0;

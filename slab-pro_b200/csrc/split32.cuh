@@ -129,6 +129,8 @@ struct Shared {
     float* part;          // [work_cap][PART_STRIDE] P2G partial sums
     int32_t work_cap;
     int32_t pad_;
+    int32_t* free_blocks; // node blocks released by retired scenarios
+    int32_t* free_count;
 };
 
 }  // namespace slab

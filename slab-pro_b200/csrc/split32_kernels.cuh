@@ -504,7 +504,14 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
         } else if (tid == 32) {
             int blk = S.blk_of[gt];
             if (blk < 0) {
-                blk = atomicAdd(sh.blk_count, 1);
+                // a block released by a retired scenario, else a fresh one
+                const int f = atomicSub(sh.free_count, 1);
+                if (f > 0) {
+                    blk = sh.free_blocks[f - 1];
+                } else {
+                    atomicAdd(sh.free_count, 1);
+                    blk = atomicAdd(sh.blk_count, 1);
+                }
                 if (blk >= sh.blk_cap) {
                     atomicOr(&c->err, ERR_CAPACITY);
                     blk = -1;

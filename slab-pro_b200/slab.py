@@ -329,3 +329,95 @@ class Batch:
 
     def kernel_launches(self) -> int:
         return self.L.slab_batch_kernel_launches(self.h)
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("max_scenarios", C.c_int32), ("chunk_steps", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED, REQ_FAILED = range(5)
+
+
+class Server:
+    """Continuous-batching request loop on one GPU (a worker thread in the library)."""
+
+    def __init__(self, z: np.ndarray, dx: float, max_scenarios: int = 64, chunk_steps: int = 32, hbm_budget_bytes: int = 0):
+        self.L = L = lib()
+        vp = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.slab_server_create.argtypes = [C.POINTER(TerrainDesc), dp, C.POINTER(ServerConfig), C.POINTER(vp)]
+        L.slab_server_submit.argtypes = [vp, C.POINTER(Params), C.c_int32] + [dp] * 7 + [C.POINTER(C.c_int64)]
+        L.slab_server_poll.argtypes = [vp, C.c_int64, C.POINTER(C.c_int32), dp]
+        L.slab_server_wait.argtypes = [vp, C.c_int64, C.c_double]
+        L.slab_server_result.argtypes = [vp, C.c_int64, C.POINTER(C.c_int32), dp, dp, C.c_int64, dp, dp, dp, dp, dp]
+        L.slab_server_cancel.argtypes = [vp, C.c_int64]
+        L.slab_server_drain.argtypes = [vp, C.c_double]
+        L.slab_server_stats.argtypes = [vp, dp]
+        L.slab_server_last_error.argtypes = [vp]
+        L.slab_server_last_error.restype = C.c_char_p
+        L.slab_server_destroy.argtypes = [vp]
+        self.Nx, self.Ny = z.shape
+        zz = np.ascontiguousarray(z, dtype=np.float64)
+        td = TerrainDesc(self.Nx, self.Ny, float(dx), 0.0, 0.0)
+        cfg = ServerConfig(int(max_scenarios), int(chunk_steps), int(hbm_budget_bytes))
+        h = C.c_void_p()
+        code = L.slab_server_create(C.byref(td), _dp(zz), C.byref(cfg), C.byref(h))
+        if code:
+            raise SlabError(code, (L.slab_last_error(None) or b"").decode())
+        self.h = h
+        self.Np = {}
+
+    def _check(self, code):
+        if code:
+            raise SlabError(code, (self.L.slab_server_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.slab_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, cfg: dict, P: dict) -> int:
+        prm = make_params(cfg, FP32_SPLIT)
+        n = len(P["h"])
+        arrs = [np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "v", "vz", "h", "A", "mass", "z")]
+        rid = C.c_int64()
+        self._check(self.L.slab_server_submit(self.h, C.byref(prm), n, *[_dp(a) for a in arrs], C.byref(rid)))
+        self.Np[rid.value] = n
+        return rid.value
+
+    def poll(self, rid: int):
+        st, t = C.c_int32(), C.c_double()
+        self._check(self.L.slab_server_poll(self.h, rid, C.byref(st), C.byref(t)))
+        return st.value, t.value
+
+    def wait(self, rid: int, timeout: float = 600.0):
+        self._check(self.L.slab_server_wait(self.h, rid, timeout))
+
+    def result(self, rid: int) -> dict:
+        box = (C.c_int32 * 4)()
+        info = np.zeros(4)
+        self._check(self.L.slab_server_result(self.h, rid, box, None, None, 0, None, None, None, None, _dp(info)))
+        nI, nJ = box[1] - box[0] + 1, box[3] - box[2] + 1
+        cap = max(nI, 0) * max(nJ, 0)
+        n = self.Np[rid]
+        hm, vm = np.zeros(max(cap, 1)), np.zeros(max(cap, 1))
+        x, v, h, m = np.zeros(2 * n), np.zeros(2 * n), np.zeros(n), np.zeros(n)
+        self._check(self.L.slab_server_result(self.h, rid, box, _dp(hm), _dp(vm), cap, _dp(x), _dp(v), _dp(h), _dp(m), _dp(info)))
+        return {"box": list(box), "h_max": hm[:cap].reshape(max(nI, 0), max(nJ, 0)), "v_max2": vm[:cap].reshape(max(nI, 0), max(nJ, 0)),
+                "x": x.reshape(n, 2), "v": v.reshape(n, 2), "h": h, "mass": m, "steps": int(info[0]), "time": info[1],
+                "seconds_to_result": info[2], "seconds_queued": info[3]}
+
+    def cancel(self, rid: int):
+        self._check(self.L.slab_server_cancel(self.h, rid))
+
+    def drain(self, timeout: float = 600.0):
+        self._check(self.L.slab_server_drain(self.h, timeout))
+
+    def stats(self) -> dict:
+        out = np.zeros(8)
+        self._check(self.L.slab_server_stats(self.h, _dp(out)))
+        keys = ("completed", "p50_s", "p99_s", "scenarios_per_s", "particle_steps", "batched_steps", "busy_s", "bytes_admitted")
+        return dict(zip(keys, out.tolist()))
