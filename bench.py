@@ -205,6 +205,11 @@ def ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream()
+    if args.only in ("ensemble", "serving"):
+        if rank != 0:
+            return None
+        sec = ensemble(args, stream, dev) if args.only == "ensemble" else serving(args, stream, dev)
+        return {"section": args.only, args.only: sec}
     c = load_workload(args.workload)
     P0 = c["particles"]
     Np = len(P0["h"])
@@ -371,7 +376,234 @@ def ours(args, rank, world):
         "wall_s_timed": round(wall, 4),
         "sim_time_s": round(t32, 4),
     }
+    if world == 1 and not args.no_ensemble and args.only != "serving":
+        try:
+            line["ensemble"] = ensemble(args, stream, dev)
+        except Exception as e:  # reported in the line, the headline stands
+            line["ensemble"] = {"error": f"{type(e).__name__}: {e}"}
+    if world == 1 and not args.no_serving and args.only != "ensemble":
+        try:
+            line["serving"] = serving(args, stream, dev)
+        except Exception as e:
+            line["serving"] = {"error": f"{type(e).__name__}: {e}"}
     return line
+
+
+def _stratified(keys, k):
+    """k indices spread evenly over the order of keys (the middle of each of k strata)."""
+    order = np.argsort(np.asarray(keys), kind="stable")
+    n = len(order)
+    k = max(1, min(k, n))
+    return [int(order[(2 * q + 1) * n // (2 * k)]) for q in range(k)]
+
+
+def _solo_run(s, cfg, P, prec, stream):
+    """One scenario alone through a context: (device seconds of the t=0 pass
+    and the step loop, wall seconds from upload to max maps on the host, steps,
+    h_max, v_max2)."""
+    import torch
+    import slab
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    s.set_params(cfg, prec)
+    s.upload(P)
+    e0.record(stream)
+    s.initial_pass()
+    n = s.advance_steps(1 << 40)
+    e1.record(stream)
+    hm, vm = s.max_maps()
+    wall = time.perf_counter() - w0
+    return e0.elapsed_time(e1) * 1e-3, wall, n, hm, vm
+
+
+def ensemble(args, stream, dev):
+    """Batched ensemble: config-4 scenarios on a shared 2048^2 DEM, all in one
+    Batch (FP32 split), against the same scenarios one after another through
+    the plain FP64 path (a stratified sample of them, timed in full)."""
+    import torch
+    import slab
+    import workloads as W
+    import accuracy as Acc
+    g0 = time.perf_counter()
+    c = W.config4(args.c4_scenarios)
+    gen_s = time.perf_counter() - g0
+    z, dx, scen = c["z"], c["dx"], c["scenarios"]
+    n = len(scen)
+    Nps = np.array([len(P["h"]) for _, P in scen])
+    out = {"workload": c["name"], "scenarios": n, "particles": int(Nps.sum()), "particles_min_max": [int(Nps.min()), int(Nps.max())],
+           "generate_s": round(gen_s, 1)}
+    b = slab.Batch(z, dx, n)
+    b.set_stream(stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for cfg, P in scen:
+        b.add(cfg, P)
+    w_add = time.perf_counter()
+    l0 = b.kernel_launches()
+    run_err = None
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        try:
+            b.run()
+        except slab.SlabError as e:  # failed scenarios stop; the others run to the end
+            run_err = str(e)
+        e1.record(stream)
+        e1.synchronize()
+    w_run = time.perf_counter()
+    status = [b.scenario_status(i) for i in range(n)]
+    ok = [i for i in range(n) if status[i] == 0]
+    boxes = {i: b.max_box(i) for i in ok}
+    w_dl = time.perf_counter()
+    run_s = e0.elapsed_time(e1) * 1e-3
+    ps, ns = b.work_counters()
+    steps = np.array([b.state(i)[2] for i in ok] or [0])
+    out["fp32_batched"] = {
+        "completed": len(ok), "failed": n - len(ok), "first_error": run_err,
+        "scenarios_per_s": round(len(ok) / run_s, 3), "particle_steps_per_s": round(ps / run_s, 1), "device_s": round(run_s, 3),
+        "e2e_scenarios_per_s": round(len(ok) / (w_dl - w0), 3), "e2e_s": round(w_dl - w0, 3), "add_s": round(w_add - w0, 3),
+        "download_s": round(w_dl - w_run, 3), "particle_steps": int(ps), "active_node_steps": int(ns),
+        "steps_min_max": [int(steps.min()), int(steps.max())], "gpu_launches": int(b.kernel_launches() - l0),
+        "clocks": clk.summary()}
+    b_results = boxes
+    b.close()
+    # the same scenarios one after another (a sample of the completed ones, stratified by particle count)
+    pick = [ok[q] for q in _stratified(Nps[ok], args.c4_sample)] if ok else []
+    full = [0, z.shape[0] - 1, 0, z.shape[1] - 1]
+    seq = {}
+    for prec, name in ((slab.FP64_PLAIN, "fp64_sequential"), (slab.FP32_SPLIT, "fp32_sequential")):
+        s = slab.Slab(z, dx)
+        s.set_stream(stream.cuda_stream)
+        dev_s, wall_s, acc, same, nrun = 0.0, 0.0, [], True, 0
+        for i in pick:
+            cfg, P = scen[i]
+            try:
+                d, w, k, hm, _ = _solo_run(s, cfg, P, prec, stream)
+            except slab.SlabError:
+                continue
+            nrun += 1
+            dev_s += d
+            wall_s += w
+            box, hb, _ = b_results[i]
+            wb = Acc.wet_box(hm)
+            if prec == slab.FP64_PLAIN:
+                acc.append(Acc.compare_max_heights(box, hb, wb, Acc.crop(full, hm, wb), dx))
+            else:
+                same &= bool(np.array_equal(Acc.crop(full, hm, box), hb)) if box[1] >= box[0] else not (hm > 0).any()
+        s.close()
+        seq[name] = {"scenarios_per_s": round(nrun / max(dev_s, 1e-9), 3), "e2e_scenarios_per_s": round(nrun / max(wall_s, 1e-9), 3),
+                     "sample": len(pick), "completed": nrun, "device_s": round(dev_s, 3), "wall_s": round(wall_s, 3)}
+        if acc:
+            seq[name]["accuracy_of_batched_fp32"] = {
+                "min_within_1cm_1pct": round(min(a["within_1cm_1pct"] for a in acc), 5),
+                "max_abs_m": round(max(a["max_abs_m"] for a in acc), 4),
+                "max_runout_diff_m": max(a["runout_diff_m"] for a in acc), "dx": dx}
+        else:
+            seq[name]["batched_equals_alone_bitwise"] = same
+    out.update(seq)
+    f64 = seq["fp64_sequential"]
+    out["speedup_vs_fp64_sequential"] = {"device": round(out["fp32_batched"]["scenarios_per_s"] / f64["scenarios_per_s"], 2),
+                                         "e2e": round(out["fp32_batched"]["e2e_scenarios_per_s"] / f64["e2e_scenarios_per_s"], 2)}
+    out["note"] = ("scenarios/s: completed scenarios / device time of one batched run; sequential rates are the mean over a "
+                   "sample of the completed scenarios stratified by particle count, each run in full (t=0 pass to total_time); "
+                   "e2e includes host binning, uploads and max-map downloads; a scenario whose flow leaves the terrain fails")
+    return out
+
+
+def serving(args, stream, dev):
+    """Served request stream: Poisson arrivals on the config-3 DEM into the
+    continuous-batching server, time to result per request; against the same
+    stream through the plain FP64 path one request at a time (service times
+    measured on a stratified sample, modelled for the rest, FIFO queue)."""
+    import slab
+    import workloads as W
+    g0 = time.perf_counter()
+    dx = 0.5
+    z = W.fractal_slope_dem(8192, dx, seed=2027, rms=7.5)
+    reqs = W.config5_stream(z, dx, args.c5_window)
+    gen_s = time.perf_counter() - g0
+    n = len(reqs)
+    Nps = np.array([len(P["h"]) for _, _, P in reqs])
+    arr = np.array([t for t, _, _ in reqs])
+    out = {"workload": f"poisson{20}/s_window{args.c5_window:g}s_fractal8192_dx0.5", "requests": n,
+           "particles": int(Nps.sum()), "particles_median_max": [int(np.median(Nps)), int(Nps.max())], "generate_s": round(gen_s, 1),
+           "window_s": args.c5_window}
+    srv = slab.Server(z, dx, max_scenarios=args.c5_slots, chunk_steps=32)
+    ids = []
+    late = 0.0
+    with ClockSampler(dev) as clk:
+        t_start = time.perf_counter()
+        for ta, cfg, P in reqs:
+            now = time.perf_counter() - t_start
+            if ta > now:
+                time.sleep(ta - now)
+            late = max(late, time.perf_counter() - t_start - ta)
+            ids.append(srv.submit(cfg, P))
+        srv.drain(timeout=1800.0)
+        t_end = time.perf_counter()
+    st = srv.stats()
+    tm = srv.timing()
+    ttr, failed = [], 0
+    # steps of each request (failed ones: total_time / dt_max, the fewest it could take)
+    steps = np.array([cfg["total_time"] / cfg["dt_max"] for _, cfg, _ in reqs])
+    for q, rid in enumerate(ids):
+        state, _ = srv.poll(rid)
+        if state != slab.REQ_DONE:
+            failed += 1
+            continue
+        r = srv.result(rid)
+        ttr.append(r["seconds_to_result"])
+        steps[q] = r["steps"]
+    srv.close()
+    ttr = np.array(ttr) if ttr else np.array([np.nan])
+    out["fp32_served"] = {"completed": int(np.isfinite(ttr).sum()), "failed": failed, "p50_s": round(float(np.percentile(ttr, 50)), 3),
+                          "p99_s": round(float(np.percentile(ttr, 99)), 3),
+                          "scenarios_per_s": round(int(np.isfinite(ttr).sum()) / (t_end - t_start), 3),
+                          "particle_steps_per_s": round(st["particle_steps"] / (t_end - t_start), 1),
+                          "makespan_s": round(t_end - t_start, 3), "busy_s": round(st["busy_s"], 3),
+                          "max_submit_lateness_s": round(late, 4), "worker": {k: round(v, 3) for k, v in tm.items()},
+                          "clocks": clk.summary()}
+    # plain FP64, one request at a time: service time measured on a sample
+    pick = _stratified(Nps * np.array([cfg["total_time"] for _, cfg, _ in reqs]), args.c5_sample)
+    s = slab.Slab(z, dx)
+    s.set_stream(stream.cuda_stream)
+    meas = []
+    for i in pick:
+        _, cfg, P = reqs[i]
+        try:
+            d, w, k, _, _ = _solo_run(s, cfg, P, slab.FP64_PLAIN, stream)
+        except slab.SlabError:
+            continue
+        meas.append((i, d, w, k))
+    s.close()
+    if len(meas) < 2:
+        out["fp64_sequential"] = {"error": "fewer than 2 sample requests completed"}
+        return out
+    # service = a*steps + b*particle-steps, least squares on the sample (device seconds)
+    Asm = np.array([[k, k * Nps[i]] for i, _, _, k in meas], dtype=np.float64)
+    ysm = np.array([d for _, d, _, _ in meas])
+    coef, *_ = np.linalg.lstsq(Asm, ysm, rcond=None)
+    f64 = {"sample": len(pick), "service_model_s": {"per_step": float(coef[0]), "per_particle_step": float(coef[1])},
+           "sample_fit_max_rel_err": round(float(np.max(np.abs(Asm @ coef - ysm) / ysm)), 4),
+           "sample_particle_steps_per_s": round(float((Asm[:, 1]).sum() / ysm.sum()), 1)}
+    svc = np.maximum(steps * coef[0] + steps * Nps * coef[1], 0.0)
+    fin = np.empty(n)
+    t = 0.0
+    for q in range(n):
+        t = max(t, arr[q]) + svc[q]
+        fin[q] = t
+    lat = fin - arr
+    f64.update({"p50_s": round(float(np.percentile(lat, 50)), 3), "p99_s": round(float(np.percentile(lat, 99)), 3),
+                "scenarios_per_s": round(n / (fin[-1] - arr[0]), 3), "busy_s": round(float(svc.sum()), 3)})
+    if len(ttr):
+        out["speedup_vs_fp64_sequential"] = {"scenarios_per_s": round(out["fp32_served"]["scenarios_per_s"] / f64["scenarios_per_s"], 2),
+                                             "p50": round(f64["p50_s"] / out["fp32_served"]["p50_s"], 2),
+                                             "p99": round(f64["p99_s"] / out["fp32_served"]["p99_s"], 2)}
+    out["fp64_sequential"] = f64
+    out["note"] = ("time to result from submission to the result on the host; arrivals replayed in real time; the FP64 "
+                   "sequential queue uses device-only service times (upload and download excluded) fitted on the sample")
+    return out
 
 
 def reference_arm(args, rank, world):
@@ -409,7 +641,15 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-procs", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--only", default="", choices=["", "fp32"], help="fp32: only the FP32 path (profiling runs)")
+    ap.add_argument("--only", default="", choices=["", "fp32", "ensemble", "serving"],
+                    help="fp32: only the FP32 path (profiling runs); ensemble / serving: only that section")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble section (config 4)")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-stream section (config 5)")
+    ap.add_argument("--c4-scenarios", type=int, default=256)
+    ap.add_argument("--c4-sample", type=int, default=16, help="scenarios run one after another for the sequential rates")
+    ap.add_argument("--c5-window", type=float, default=20.0, help="seconds of Poisson arrivals (the full stream is 300 s)")
+    ap.add_argument("--c5-slots", type=int, default=512)
+    ap.add_argument("--c5-sample", type=int, default=12, help="requests timed on the plain FP64 path")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         log("warmup raised to 3")

@@ -213,9 +213,19 @@ slab_status slab_batch_add(slab_batch* b, const slab_params* params, int32_t Np,
  * most max_steps steps of the batch. */
 slab_status slab_batch_run(slab_batch* b, int64_t max_steps, int64_t* steps_out);
 slab_status slab_batch_state(slab_batch* b, int32_t scenario_id, double* time, int32_t* frame, int64_t* steps);
+/* The scenario's own outcome: SLAB_OK, or the error that stopped it
+ * (SLAB_E_DOMAIN, SLAB_E_NONFINITE, SLAB_E_OOM). A failed scenario stops at
+ * once; the others run on, and slab_batch_run reports the first failure. */
+slab_status slab_batch_scenario_status(slab_batch* b, int32_t scenario_id);
 slab_status slab_batch_download_particles(slab_batch* b, int32_t scenario_id, double* x_xy, double* v_xy, double* vz, double* h,
                                           double* A, double* mass, double* z);
 slab_status slab_batch_download_max(slab_batch* b, int32_t scenario_id, double* h_max, double* v_max2);
+/* The node box {i0, i1, j0, j1} a scenario's flow has touched and, when the
+ * map pointers are not NULL and the box has at most cap_nodes nodes, h_max
+ * and v_max2 over that box ((i-i0)*(j1-j0+1) + (j-j0)); an empty box has
+ * i1 < i0. */
+slab_status slab_batch_download_max_box(slab_batch* b, int32_t scenario_id, int32_t box[4], double* h_max, double* v_max2,
+                                        int64_t cap_nodes);
 /* out[0] = particle-steps, out[1] = active node-steps, over all scenarios. */
 slab_status slab_batch_work_counters(slab_batch* b, int64_t out[2]);
 int64_t slab_batch_kernel_launches(const slab_batch* b);
@@ -262,6 +272,12 @@ slab_status slab_server_drain(slab_server* s, double timeout_s);
  * since the first submission, particle-steps, batched steps, seconds the
  * worker was busy, bytes admitted now}. */
 slab_status slab_server_stats(slab_server* s, double out[8]);
+/* Where the worker thread's time went: out = {seconds admitting requests
+ * (host binning and uploads), seconds in chunks of batched steps (enqueue to
+ * completion), seconds retiring finished requests (downloads, releases),
+ * chunks run, mean and max scenarios running per chunk, capacity growths,
+ * kernel launches}. */
+slab_status slab_server_timing(slab_server* s, double out[8]);
 const char* slab_server_last_error(const slab_server* s);
 void slab_server_destroy(slab_server* s);
 

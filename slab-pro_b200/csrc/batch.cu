@@ -63,14 +63,26 @@ void pull_all(slab_batch* b) {
     SLAB_CUDA(cudaStreamSynchronize(b->stream));
 }
 
+slab_status status_of(int e) {
+    if (e & ERR_NONFINITE) return SLAB_E_NONFINITE;
+    if (e & (ERR_DOMAIN | ERR_MOVE)) return SLAB_E_DOMAIN;
+    if (e & ERR_CAPACITY) return SLAB_E_OOM;
+    return SLAB_OK;
+}
+
 void raise_errors(slab_batch* b) {
-    for (int s = 0; s < b->E->nscn; ++s) {
-        const int e = b->h_ctl[s].err;
-        const std::string who = "scenario " + std::to_string(s) + ": ";
-        if (e & ERR_NONFINITE) throw Error{SLAB_E_NONFINITE, who + "non-finite particle state"};
-        if (e & (ERR_DOMAIN | ERR_MOVE)) throw Error{SLAB_E_DOMAIN, who + "a particle stencil left the terrain"};
-        if (e & ERR_CAPACITY) throw Error{SLAB_E_OOM, who + "device capacity exceeded"};
-    }
+    int nfail = 0, first = -1;
+    for (int s = 0; s < b->E->nscn; ++s)
+        if (status_of(b->h_ctl[s].err) != SLAB_OK) {
+            if (first < 0) first = s;
+            ++nfail;
+        }
+    if (first < 0) return;
+    const slab_status code = status_of(b->h_ctl[first].err);
+    const char* what = code == SLAB_E_NONFINITE ? "non-finite particle state"
+                       : code == SLAB_E_DOMAIN  ? "a particle stencil left the terrain"
+                                                : "device capacity exceeded";
+    throw Error{code, "scenario " + std::to_string(first) + ": " + what + " (" + std::to_string(nfail) + " scenario(s) failed)"};
 }
 
 void run_t0(slab_batch* b) {
@@ -185,6 +197,17 @@ slab_status slab_batch_state(slab_batch* b, int32_t sid, double* time, int32_t* 
     });
 }
 
+slab_status slab_batch_scenario_status(slab_batch* b, int32_t sid) {
+    if (!b) return SLAB_E_ARG;
+    slab_status st = SLAB_OK;
+    const slab_status g = bguard(b, [&] {
+        bneed(sid >= 0 && sid < b->E->nscn, SLAB_E_NOTFOUND, "unknown scenario");
+        pull_all(b);
+        st = status_of(b->h_ctl[sid].err);
+    });
+    return g != SLAB_OK ? g : st;
+}
+
 slab_status slab_batch_download_particles(slab_batch* b, int32_t sid, double* x, double* v, double* vz, double* h, double* A, double* m,
                                           double* z) {
     if (!b) return SLAB_E_ARG;
@@ -199,6 +222,20 @@ slab_status slab_batch_download_max(slab_batch* b, int32_t sid, double* h_max, d
     return bguard(b, [&] {
         bneed(sid >= 0 && sid < b->E->nscn, SLAB_E_NOTFOUND, "unknown scenario");
         b->E->download_max(sid, h_max, v_max2);
+    });
+}
+
+slab_status slab_batch_download_max_box(slab_batch* b, int32_t sid, int32_t box[4], double* h_max, double* v_max2, int64_t cap_nodes) {
+    if (!b || !box) return SLAB_E_ARG;
+    return bguard(b, [&] {
+        bneed(sid >= 0 && sid < b->E->nscn, SLAB_E_NOTFOUND, "unknown scenario");
+        int bx[4];
+        b->E->box_of_blocks(sid, bx);
+        for (int k = 0; k < 4; ++k) box[k] = bx[k];
+        const int64_t nI = bx[1] - bx[0] + 1, nJ = bx[3] - bx[2] + 1;
+        if (!h_max || !v_max2 || nI <= 0 || nJ <= 0) return;
+        bneed(nI * nJ <= cap_nodes, SLAB_E_ARG, "cap_nodes smaller than the box");
+        b->E->download_max_box(sid, bx, h_max, v_max2);
     });
 }
 

@@ -38,7 +38,7 @@ class Engine32 {
     void launch_kernel(int k, const Shared& sh);
     void launch_p2g(const Shared& sh);
     void arm(int64_t steps_left, int stop_at_frame);
-    int acc_mode = 1;  // fixed-point scheme of P2G (k32::ACC_*)
+    int acc_mode = 3;  // P2G scheme (k32::ACC_*): cell-sorted FP32 sums by default
     void enqueue_steps(int chunk);
     PhaseTimer timer;
     SCnt counters(int sid);
@@ -65,6 +65,7 @@ class Engine32 {
     int nscn = 0;
     int TX = 0, TY = 0, ntiles = 0;
     int blk_cap = 0;
+    int64_t pending_blocks = 0;  // node blocks of scenarios added since the last t=0 pass (an estimate)
     int grid_p2g = 0, grid_g2p = 0, grid_grid = 0, grid_prep = 0;
     int work_cap = 0;
     int64_t work_cap_total = 0;

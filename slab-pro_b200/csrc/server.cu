@@ -87,6 +87,9 @@ struct slab_server {
     clk::time_point t_first_submit, t_last_done;
     bool any_submit = false;
     double busy_s = 0;
+    // where the worker's time goes
+    double admit_s = 0, chunk_s = 0, retire_s = 0;
+    int64_t chunks = 0, running_sum = 0, running_max = 0, grown = 0;
 };
 
 namespace {
@@ -182,6 +185,7 @@ void worker_loop(slab_server* s) {
         }
         const auto t0 = clk::now();
         bool new_ones = false;
+        auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
         for (int64_t id : admit) {
             Request* r;
             {
@@ -224,15 +228,27 @@ void worker_loop(slab_server* s) {
             }
         }
         try {
+            const auto t1 = clk::now();
+            s->admit_s += secs(t0, t1);
             if (new_ones) s->E->launch_t0();
             // ---- one chunk of batched steps for every running scenario
             s->E->arm(s->chunk, 0);
             s->E->enqueue_steps(s->chunk);
-            s->E->check_capacity();
+            if (s->E->check_capacity()) s->grown += 1;
             const int n = s->E->nscn;
             SLAB_CUDA(cudaMemcpyAsync(s->h_ctl, s->d_ctl, n * sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
             SLAB_CUDA(cudaStreamSynchronize(s->stream));
+            const auto t2 = clk::now();
+            s->chunk_s += secs(t1, t2);
             s->batched_steps += s->chunk;
+            {
+                int running = 0;
+                std::lock_guard<std::mutex> lk(s->mu);
+                for (int64_t r : s->slot_req) running += r >= 0;
+                s->chunks += 1;
+                s->running_sum += running;
+                s->running_max = std::max<int64_t>(s->running_max, running);
+            }
             // ---- retire finished / failed / cancelled scenarios
             for (int k = 0; k < n; ++k) {
                 int64_t id;
@@ -259,6 +275,7 @@ void worker_loop(slab_server* s) {
                     finish(s, k, REQ_DONE, "");
                 }
             }
+            s->retire_s += secs(t2, clk::now());
         } catch (const Error& e) {
             std::lock_guard<std::mutex> lk(s->mu);
             s->err = e.msg;
@@ -483,6 +500,21 @@ slab_status slab_server_stats(slab_server* s, double out[8]) {
         out[5] = (double)s->batched_steps;
         out[6] = s->busy_s;
         out[7] = (double)s->used;
+    });
+}
+
+slab_status slab_server_timing(slab_server* s, double out[8]) {
+    if (!s || !out) return SLAB_E_ARG;
+    return sguard(s, [&] {
+        std::lock_guard<std::mutex> lk(s->mu);
+        out[0] = s->admit_s;
+        out[1] = s->chunk_s;
+        out[2] = s->retire_s;
+        out[3] = (double)s->chunks;
+        out[4] = s->chunks ? (double)s->running_sum / (double)s->chunks : 0.0;
+        out[5] = (double)s->running_max;
+        out[6] = (double)s->grown;
+        out[7] = (double)s->E->nlaunch;
     });
 }
 

@@ -80,11 +80,15 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_cell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2CSmem)));
     if (const char* e = std::getenv("SLAB_P2G_ACC")) acc_mode = std::atoi(e);
     int dev = 0, sms = 0, occ_p = 0, occ_g = 0, occ_u = 0;
     SLAB_CUDA(cudaGetDevice(&dev));
     SLAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g<k32::ACC_HILO>, k32::P2G_THREADS, sizeof(k32::P2GSmem)));
+    if (acc_mode == k32::ACC_CELL)
+        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem)));
+    else
+        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g<k32::ACC_HILO>, k32::P2G_THREADS, sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, k32::k_g2p, NCELL, 0));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k32::k_grid, NCELL, 0));
     grid_p2g = sms * std::max(occ_p, 1);
@@ -331,6 +335,26 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
         alist.push_back(t);
     }
     if ((int)alist.size() > S.act_cap) throw Error{SLAB_E_OOM, "active tile capacity"};
+    // node blocks the t=0 pass will take (the grid tiles of the active tiles'
+    // node windows): grow the pool now, as the pass runs before any check
+    {
+        std::vector<char> touched(ntiles, 0);
+        int64_t est = 0;
+        for (int t : alist)
+            for (int k = 0; k < 4; ++k) {
+                const int gi = t / TY + (k >> 1), gj = t % TY + (k & 1);
+                if (gi < TX && gj < TY && !touched[gi * TY + gj]) {
+                    touched[gi * TY + gj] = 1;
+                    ++est;
+                }
+            }
+        int32_t misc[8];
+        d2h(misc, d_misc.get(), 8, st);
+        SLAB_CUDA(cudaStreamSynchronize(st));
+        pending_blocks += est;
+        const int64_t need = (int64_t)(misc[0] - misc[4]) + pending_blocks;
+        if (2 * need > blk_cap) grow_blocks((int)std::min<int64_t>(std::max<int64_t>(2 * (int64_t)blk_cap, 2 * need), INT32_MAX / NCELL));
+    }
     h2d(S.cell[0].get(), o_cell.data(), Np, st);
     h2d(S.f[0].get(), o_f.data(), Np, st);
     h2d(S.v[0].get(), o_v.data(), Np, st);
@@ -409,15 +433,18 @@ void Engine32::launch_begin(int t0) {
 void Engine32::launch_t0() {
     const Shared sh = shared();
     k32::k_begin<<<1, 1024, 0, st>>>(sh, 1);
-    k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
+    if (acc_mode != k32::ACC_CELL) k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
     launch_p2g(sh);
     k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
     SLAB_CUDA(cudaGetLastError());
-    nlaunch += 4;
+    nlaunch += acc_mode != k32::ACC_CELL ? 4 : 3;
+    pending_blocks = 0;  // later reads of the pool count see these blocks
 }
 
 void Engine32::launch_p2g(const Shared& sh) {
-    if (acc_mode == k32::ACC_I32)
+    if (acc_mode == k32::ACC_CELL)
+        k32::k_p2g_cell<<<grid_p2g, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh);
+    else if (acc_mode == k32::ACC_I32)
         k32::k_p2g<k32::ACC_I32><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
     else if (acc_mode == k32::ACC_I64)
         k32::k_p2g<k32::ACC_I64><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
@@ -427,7 +454,9 @@ void Engine32::launch_p2g(const Shared& sh) {
 
 void Engine32::launch_kernel(int k, const Shared& sh) {
     switch (k) {
-        case 0: k32::k_prep<<<grid_prep, 256, 0, st>>>(sh); break;
+        case 0:  // the cell P2G kernel builds its own descriptors
+            if (acc_mode != k32::ACC_CELL) k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
+            break;
         case 1: launch_p2g(sh); break;
         case 2: k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh); break;
         case 3: k32::k_g2p<<<grid_g2p, NCELL, 0, st>>>(sh, T.z.get()); break;
@@ -457,7 +486,7 @@ void Engine32::enqueue_steps(int chunk) {
     } else {
         graphs.launch(chunk, st, [&] { launch_step(); });
     }
-    nlaunch += 4 * chunk;
+    nlaunch += (acc_mode != k32::ACC_CELL ? 4 : 3) * (int64_t)chunk;
 }
 
 SCnt Engine32::counters(int sid) {

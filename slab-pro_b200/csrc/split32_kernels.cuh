@@ -283,7 +283,8 @@ constexpr int P2G_THREADS = 256;
 //            part below one quantum -- each contribution keeps about FP32
 //            precision relative to itself; two plain (non-returning) atomics
 //  ACC_I64   one int64 per sum at 2^-52 of the bound
-enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2 };
+//  ACC_CELL  no fixed point: k_p2g_cell, FP32 sums over cell-sorted particles
+enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2, ACC_CELL = 3 };
 
 struct P2GSmem {
     long long node[NQ * TN * TN];  // fixed-point sums of the (TILE+2)^2 window (int32 pairs / int64)
@@ -469,6 +470,297 @@ __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(Shared sh) {
     }
 }
 
+// ------------------------------------------------ P2G over cell-sorted particles
+
+// K1 for one work item, by warp 0 of a CTA (lane d < 9 reads direction d):
+// the tile's 9 candidate ranges and exact count, its segment in the next
+// buffer, and the grid tiles of its node window on the grid-tile list. The
+// descriptor goes to shared memory and to sh.desc[w] for G2P.
+__device__ void prep_tile(const Shared& sh, int w, TileDesc* sd) {
+    const int lane = threadIdx.x & 31;
+    int sid = 0, loc = 0;
+    find_work(sh.work_pref, sh.nscn, w, sid, loc);
+    const Scn& S = sh.scn[sid];
+    SCnt* n = S.cnt;
+    const int seq = n->seq, cur = seq & 1;
+    const int t = S.act_list[cur][loc];
+    const int ti = t / sh.TY, tj = t % sh.TY;
+    int rs = 0, rl = 0, cnt = 0;
+    if (lane < 9) {
+        const int si = ti - dir_i(lane), sj = tj - dir_j(lane);
+        if (si >= 0 && sj >= 0 && si < sh.TX && sj < sh.TY) {
+            const int sidx = si * sh.TY + sj;
+            if (S.grp_stamp[cur][sidx] == seq) {
+                const int32_t* G = S.grp[cur] + sidx * GRP_STRIDE;
+                if (lane == 4) {
+                    rs = G[0];
+                    rl = G[1] - G[0];
+                } else {
+                    rs = G[1];
+                    rl = G[2] - G[1];
+                }
+                cnt = G[3 + lane];
+            }
+        }
+    }
+    int incl = rl, tot = cnt;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    tot += __shfl_xor_sync(0xffffffffu, tot, 16);
+    if (lane < 9) {
+        sd->rstart[lane] = rs;
+        sd->rpref[lane] = incl - rl;
+    }
+    if (lane == 8) sd->rpref[9] = incl;
+    // grid tiles of the node window: the ones not yet listed this step
+    const int stamp = n->stepid;
+    bool fresh = false;
+    int gt = 0;
+    if (lane < 4) {
+        const int gi = ti + (lane >> 1), gj = tj + (lane & 1);
+        if (gi < sh.TX && gj < sh.TY) {
+            gt = gi * sh.TY + gj;
+            fresh = atomicMax(&S.gt_stamp[gt], stamp) < stamp;
+        }
+    }
+    const unsigned fm = __ballot_sync(0xffffffffu, fresh);
+    int at = 0, off = 0;
+    if (lane == 0) {
+        if (fm) at = atomicAdd(&n->gt_count, __popc(fm));
+        off = atomicAdd(&n->cursor, tot);
+        S.slot_of[t] = w;
+        sd->t = t;
+        sd->sid = sid;
+        sd->total = tot;
+        sd->nxt_off = off;
+        sd->pad_ = 0;
+    }
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (fresh) S.gt_list[at + __popc(fm & ((1u << lane) - 1u))] = gt;
+    __syncwarp();
+    if (lane < (int)(sizeof(TileDesc) / 4)) reinterpret_cast<int*>(sh.desc + w)[lane] = reinterpret_cast<const int*>(sd)[lane];
+}
+
+// After the last CTA of a launch has listed its grid tiles: the prefix of
+// grid tiles over scenarios (the work list of k_grid). Call with the whole
+// CTA; s_warp needs 33 ints.
+__device__ void close_grid_list(const Shared& sh, int* s_warp) {
+    __shared__ int s_last, s_tot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&sh.done[0], 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    int total = 0;
+    for (int base = 0; base < sh.nscn; base += blockDim.x) {
+        const int s = base + threadIdx.x;
+        const int cnt = (s < sh.nscn && sh.scn[s].ctl->active) ? *(volatile int*)&sh.scn[s].cnt->gt_count : 0;
+        const int ex = block_exclusive_scan(cnt, s_warp);
+        if (s < sh.nscn) sh.grid_pref[s] = total + ex;
+        if (threadIdx.x == blockDim.x - 1) s_tot = ex + cnt;
+        __syncthreads();
+        total += s_tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sh.grid_pref[sh.nscn] = total;
+}
+
+
+constexpr int P2C_THREADS = NCELL;  // one thread per cell of the tile
+constexpr int P2C_WARPS = P2C_THREADS / 32;
+constexpr int NSLOT = 9;            // nodes a cell's particles reach (3 x 3)
+
+struct P2CSmem {
+    float part[NQ * NSLOT][NCELL];  // per-cell sums: [q * 9 + a * 3 + b][cell]
+    float4 dem[(TILE + 1) * (TILE + 1)];
+    int wcur[P2C_WARPS][NCELL];     // per-warp cell counts, then per-warp write cursors
+    int s_warp[33];
+    TileDesc d;
+};
+
+// Sums of one cell's particles, in their sorted order, over the 9 nodes of
+// the cell's stencil (src/simulation.cpp:758-795); OUTS adds m vz.
+template <bool OUTS>
+__device__ __forceinline__ void cell_sums(float (&acc)[NQ][NSLOT], const int32_t* __restrict__ order, int c0, int nn, const PBuf& B,
+                                          int li, int lj, const float4* dem, float g, float hod) {
+    int nsrc = nn > 0 ? order[c0] : 0;
+    for (int r = 0; r < nn; ++r) {
+        const int src = nsrc;
+        if (r + 1 < nn) nsrc = order[c0 + r + 1];
+        const PQ p = load_pq(B, src, li, lj, dem, g, hod, OUTS);
+        float wx[3], wy[3], dwx[3], dwy[3];
+        bspline3(p.fx, wx, dwx);
+        bspline3(p.fy, wy, dwy);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const int s = a * 3 + b;
+                const float wgt = wx[a] * wy[b];
+                if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
+                    acc[0][s] += p.m * wgt;
+                    acc[1][s] += p.mvx * wgt;
+                    acc[2][s] += p.mvy * wgt;
+                    acc[3][s] += p.mh * wgt;
+                    acc[4][s] += p.Khh * (dwx[a] * wy[b]) - p.Kgx * wgt;
+                    acc[5][s] += p.Khh * (dwy[b] * wx[a]) - p.Kgy * wgt;
+                    if (OUTS) acc[6][s] += p.mvz * wgt;
+                }
+            }
+        }
+    }
+}
+
+// K1 + K2: the tile's descriptor (prep_tile), then P2G of the tile
+// (src/simulation.cpp:726-798) as a segmented reduction over cell-sorted
+// particles, with no atomics on floats:
+//  1. each warp walks a contiguous block of the tile's candidates and counts
+//     particles per cell (lanes of one cell are grouped by __match_any_sync);
+//  2. thread = cell: per-warp write cursors and the cell's range (a scan);
+//  3. the warps walk their blocks again and write each particle's index at
+//     its cursor: a stable counting sort by cell, into the tile's segment of
+//     the next particle buffer (unused until G2P of this step);
+//  4. thread = cell: FP32 sums of the cell's particles, in sorted order, for
+//     the 9 nodes of its stencil;
+//  5. thread = node: the node's sums over its <= 9 cells, in a fixed order.
+// The candidates of a tile come in an order fixed by the previous step's G2P
+// (ordered placement), so every sum has a fixed order: results are bitwise
+// reproducible and the same alone or inside a batch.
+__global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P2CSmem& sm = *reinterpret_cast<P2CSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int li = tid / TILE, lj = tid % TILE;
+    const int nwork = sh.work_pref[sh.nscn];
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        if (warp == 0) prep_tile(sh, w, &sm.d);
+        for (int k = tid; k < P2C_WARPS * NCELL; k += P2C_THREADS) (&sm.wcur[0][0])[k] = 0;
+        __syncthreads();
+        const Scn& S = sh.scn[sm.d.sid];
+        const int t = sm.d.t;
+        const int ti = t / sh.TY, tj = t % sh.TY;
+        SCnt* n = S.cnt;
+        const int cur = n->seq & 1;
+        const bool outs = n->outs != 0;
+        for (int k = tid; k < (TILE + 1) * (TILE + 1); k += P2C_THREADS) {
+            const int i = ti * TILE + k / (TILE + 1), j = tj * TILE + k % (TILE + 1);
+            sm.dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
+        }
+        const int ncand = sm.d.rpref[9];
+        const int total = sm.d.total;
+        const PBuf B = S.buf[cur];
+        int32_t* order = S.buf[cur ^ 1].cell + sm.d.nxt_off;
+        const int per = (ncand + P2C_WARPS - 1) / P2C_WARPS;
+        const int k_lo = min(warp * per, ncand), k_hi = min(k_lo + per, ncand);
+        // 1. counts per (warp, cell)
+        for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+            const int k = k0 + lane;
+            int lc = -1;
+            if (k < k_hi) {
+                int d;
+                const int src = cand_to_index(k, sm.d, d);
+                const int32_t cell = B.cell[src];
+                const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
+                if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
+                else if (d == 4) atomicOr(&S.ctl->err, ERR_MOVE);  // a stayer outside its tile
+            }
+            const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
+            if (lc >= 0) {
+                const unsigned peers = __match_any_sync(vm, lc);
+                if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        // 2. cursors: cell-major, warp-minor
+        int n_c = 0;
+#pragma unroll
+        for (int q = 0; q < P2C_WARPS; ++q) {
+            const int x = sm.wcur[q][tid];
+            sm.wcur[q][tid] = n_c;
+            n_c += x;
+        }
+        const int c0 = block_exclusive_scan(n_c, sm.s_warp);
+        if (tid == P2C_THREADS - 1 && c0 + n_c != total) atomicOr(&S.ctl->err, ERR_CAPACITY);
+#pragma unroll
+        for (int q = 0; q < P2C_WARPS; ++q) sm.wcur[q][tid] += c0;
+        __syncthreads();
+        // 3. stable placement by cell
+        for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+            const int k = k0 + lane;
+            int lc = -1, src = 0;
+            if (k < k_hi) {
+                int d;
+                src = cand_to_index(k, sm.d, d);
+                const int32_t cell = B.cell[src];
+                const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
+                if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
+            }
+            const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
+            unsigned peers = 0;
+            if (lc >= 0) {
+                peers = __match_any_sync(vm, lc);
+                const int pos = sm.wcur[warp][lc] + __popc(peers & lt);
+                if (pos < total) order[pos] = src;
+                else atomicOr(&S.ctl->err, ERR_CAPACITY);
+            }
+            __syncwarp();
+            if (lc >= 0 && (peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        // 4. per-cell sums
+        {
+            float acc[NQ][NSLOT];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+#pragma unroll
+                for (int s = 0; s < NSLOT; ++s) acc[q][s] = 0.f;
+            const int nn = max(0, min(n_c, total - c0));
+            const float g = S.g, hod = 0.5f * S.ood;
+            if (outs) cell_sums<true>(acc, order, c0, nn, B, li, lj, sm.dem, g, hod);
+            else cell_sums<false>(acc, order, c0, nn, B, li, lj, sm.dem, g, hod);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+#pragma unroll
+                for (int s = 0; s < NSLOT; ++s) sm.part[q * NSLOT + s][tid] = acc[q][s];
+        }
+        __syncthreads();
+        // 5. node sums over the cells that reach the node, (a, b) ascending
+        float* P = sh.part + (size_t)w * PART_STRIDE;
+        for (int k = tid; k < TN * TN; k += P2C_THREADS) {
+            const int A = k / TN, Bn = k % TN;
+            float v[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) v[q] = 0.f;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int ci = A - a;
+                if ((unsigned)ci >= TILE) continue;
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const int cj = Bn - b;
+                    if ((unsigned)cj >= TILE) continue;
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) v[q] += sm.part[q * NSLOT + a * 3 + b][ci * TILE + cj];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) P[q * TN * TN + k] = v[q];
+        }
+        __syncthreads();
+    }
+    close_grid_list(sh, sm.s_warp);
+}
+
 // ------------------------------------------------------------ grid update
 
 // K3 + K6: computeGridVelocity (src/simulation.cpp:800-875) for the TILE^2
@@ -622,6 +914,7 @@ struct G2PSmem {
     float4 nv[TN * TN];
     float4 dem[(TILE + 1) * (TILE + 1)];
     int front, back;
+    int wst[2][NCELL / 32], wmv[2][NCELL / 32];  // per-warp stayer / mover counts of a chunk (double buffered)
     int dcnt[9];
     int blk4[4];
     TileDesc d;
@@ -686,6 +979,7 @@ __global__ void __launch_bounds__(NCELL, 3) k_g2p(Shared sh, const double* __res
         const float dt_ood = dt * S.ood;
         const double dx = c->dx;
         double mnx = INFINITY, mxx = 0.0, mny = INFINITY, mxy = 0.0, vv = 0.0;
+        int front = 0, back = 0;  // stayers / movers placed so far (same in every thread)
         for (int k0 = 0; k0 < ncand; k0 += NCELL) {
             const int k = k0 + tid;
             bool valid = k < ncand;
@@ -766,16 +1060,28 @@ __global__ void __launch_bounds__(NCELL, 3) k_g2p(Shared sh, const double* __res
                 if (!isfinite(vn.x) || !isfinite(vn.y) || !isfinite(hn) || !isfinite(fn.x) || !isfinite(fn.y))
                     atomicOr(&c->err, ERR_NONFINITE);
             }
-            // stayers to the front of the segment, movers to the back
+            // stayers to the front of the segment, movers to the back, both in
+            // candidate order (a block prefix of the warps' counts), so the next
+            // step sees the tile's particles in an order fixed by the data
             const bool stay = valid && d == 4, move = valid && d != 4;
             const unsigned ms = __ballot_sync(0xffffffffu, stay), mm = __ballot_sync(0xffffffffu, move);
-            int bs = 0, bm = 0;
+            const int par = (k0 / NCELL) & 1;
             if (lane == 0) {
-                if (ms) bs = atomicAdd(&sm.front, __popc(ms));
-                if (mm) bm = atomicAdd(&sm.back, __popc(mm));
+                sm.wst[par][warp] = __popc(ms);
+                sm.wmv[par][warp] = __popc(mm);
             }
-            bs = __shfl_sync(0xffffffffu, bs, 0);
-            bm = __shfl_sync(0xffffffffu, bm, 0);
+            __syncthreads();
+            int bs = front, bm = back;
+#pragma unroll
+            for (int q = 0; q < NCELL / 32; ++q) {
+                const int a = sm.wst[par][q], b = sm.wmv[par][q];
+                if (q < warp) {
+                    bs += a;
+                    bm += b;
+                }
+                front += a;
+                back += b;
+            }
             const unsigned lt = (1u << lane) - 1u;
             if (valid) {
                 int pos;
@@ -794,6 +1100,10 @@ __global__ void __launch_bounds__(NCELL, 3) k_g2p(Shared sh, const double* __res
                 if (need_vz) O.vz[pos] = vzp;
                 if (outs) O.z[pos] = (float)zp;
             }
+        }
+        if (tid == 0) {
+            sm.front = front;
+            sm.back = back;
         }
         __syncthreads();
         if (tid < 9) {

@@ -254,8 +254,10 @@ class Batch:
         L.slab_batch_add.argtypes = [vp, C.POINTER(Params), C.c_int32] + [dp] * 7 + [C.POINTER(C.c_int32)]
         L.slab_batch_run.argtypes = [vp, C.c_int64, C.POINTER(C.c_int64)]
         L.slab_batch_state.argtypes = [vp, C.c_int32, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+        L.slab_batch_scenario_status.argtypes = [vp, C.c_int32]
         L.slab_batch_download_particles.argtypes = [vp, C.c_int32] + [dp] * 7
         L.slab_batch_download_max.argtypes = [vp, C.c_int32, dp, dp]
+        L.slab_batch_download_max_box.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), dp, dp, C.c_int64]
         L.slab_batch_work_counters.argtypes = [vp, C.POINTER(C.c_int64)]
         L.slab_batch_kernel_launches.argtypes = [vp]
         L.slab_batch_kernel_launches.restype = C.c_int64
@@ -308,6 +310,10 @@ class Batch:
         self._check(self.L.slab_batch_state(self.h, sid, C.byref(t), C.byref(f), C.byref(s)))
         return t.value, f.value, s.value
 
+    def scenario_status(self, sid: int) -> int:
+        """0 (OK) or the status code of the error that stopped the scenario."""
+        return int(self.L.slab_batch_scenario_status(self.h, sid))
+
     def particles(self, sid: int) -> dict:
         n = self.Np[sid]
         out = {k: np.zeros(2 * n if k in ("x", "v") else n) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
@@ -321,6 +327,15 @@ class Batch:
         vm = np.zeros(self.Nx * self.Ny)
         self._check(self.L.slab_batch_download_max(self.h, sid, _dp(hm), _dp(vm)))
         return hm.reshape(self.Nx, self.Ny), vm.reshape(self.Nx, self.Ny)
+
+    def max_box(self, sid: int):
+        """(box {i0, i1, j0, j1}, h_max, v_max2) over the nodes the flow touched."""
+        box = (C.c_int32 * 4)()
+        self._check(self.L.slab_batch_download_max_box(self.h, sid, box, None, None, 0))
+        nI, nJ = max(box[1] - box[0] + 1, 0), max(box[3] - box[2] + 1, 0)
+        hm, vm = np.zeros(max(nI * nJ, 1)), np.zeros(max(nI * nJ, 1))
+        self._check(self.L.slab_batch_download_max_box(self.h, sid, box, _dp(hm), _dp(vm), nI * nJ))
+        return list(box), hm[:nI * nJ].reshape(nI, nJ), vm[:nI * nJ].reshape(nI, nJ)
 
     def work_counters(self):
         out = (C.c_int64 * 2)()
@@ -353,6 +368,7 @@ class Server:
         L.slab_server_cancel.argtypes = [vp, C.c_int64]
         L.slab_server_drain.argtypes = [vp, C.c_double]
         L.slab_server_stats.argtypes = [vp, dp]
+        L.slab_server_timing.argtypes = [vp, dp]
         L.slab_server_last_error.argtypes = [vp]
         L.slab_server_last_error.restype = C.c_char_p
         L.slab_server_destroy.argtypes = [vp]
@@ -420,4 +436,10 @@ class Server:
         out = np.zeros(8)
         self._check(self.L.slab_server_stats(self.h, _dp(out)))
         keys = ("completed", "p50_s", "p99_s", "scenarios_per_s", "particle_steps", "batched_steps", "busy_s", "bytes_admitted")
+        return dict(zip(keys, out.tolist()))
+
+    def timing(self) -> dict:
+        out = np.zeros(8)
+        self._check(self.L.slab_server_timing(self.h, _dp(out)))
+        keys = ("admit_s", "chunk_s", "retire_s", "chunks", "mean_running", "max_running", "capacity_growths", "kernel_launches")
         return dict(zip(keys, out.tolist()))

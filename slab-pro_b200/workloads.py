@@ -82,7 +82,7 @@ def terrain_theta(z: np.ndarray, dx: float) -> np.ndarray:
 
 
 def release_particles(z: np.ndarray, dx: float, release: dict, rho: float, sampling: str = "UNIFORM",
-                      samples: np.ndarray | None = None, fast_theta: bool = False) -> dict:
+                      samples: np.ndarray | None = None, fast_theta: bool = False, grad_norm: np.ndarray | None = None) -> dict:
     """Simulation::initializeParticles for RECTANGLE/ELLIPSE/RASTER releases.
 
     release: {"type": "RECTANGLE", "center": (x, y), "Lx", "Ly", "rotation_deg", "h0"}
@@ -160,7 +160,7 @@ def release_particles(z: np.ndarray, dx: float, release: dict, rho: float, sampl
     A_init = volume / sum_h
     A = np.full(n, A_init)
     mass = rho * h * A
-    gn = terrain_gradient_norm(z, dx)
+    gn = terrain_gradient_norm(z, dx) if grad_norm is None else grad_norm
     ci = np.floor(x[:, 0] * ood).astype(np.int64)
     cj = np.floor(x[:, 1] * ood).astype(np.int64)
     if fast_theta:  # numpy's arctan (may differ from libm in the last bit); theta is recomputed by the step anyway
@@ -370,3 +370,71 @@ def config3(seed: int = 2027):
     rel = {"type": "ELLIPSE", "center": (800.0, 2048.0), "rx": 600.0, "ry": 400.0, "rotation_deg": 0.0, "h0": 3.0}
     P = release_particles(z, dx, rel, cfg["rho"], fast_theta=True)
     return {"name": "fractal8192_dx05_ellipse_uniform_mui", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}
+
+
+def config4(n_scenarios: int = 256, seed: int = 2028):
+    """Ensemble on a shared 2048^2 DEM at 2 m (fractal-slope construction,
+    roughness 7.5 m RMS): elliptical releases with semi-axes U(20, 300) m,
+    centres uniform in the upper third, h0 U(0.5, 3) m, UNIFORM 2x2 sampling
+    (1.9 k - 265 k particles, 20.7 M in all), Voellmy with mu U(0.1, 0.4),
+    xi U(500, 3000), total_time 60 s; the other parameters as the 35-degree
+    slope case (rho 300, C_cfl 0.5, dt_max 0.01 s, flip_ratio 0.95)."""
+    dx = 2.0
+    n = 2048
+    z = fractal_slope_dem(n, dx, seed=seed, rms=7.5)
+    gn = terrain_gradient_norm(z, dx)
+    rng = np.random.default_rng(seed + 1)
+    L = n * dx
+    out = []
+    for k in range(n_scenarios):
+        rx, ry = rng.uniform(20.0, 300.0, 2)
+        rot = rng.uniform(0.0, 180.0)
+        r = max(rx, ry) + 4 * dx
+        cx = rng.uniform(r, max(r + 1.0, L / 3.0))
+        cy = rng.uniform(r, L - r)
+        cfg = dict(gravity=9.81, rho=300.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=60.0,
+                   friction="VOELLMY", voellmy_mu=float(rng.uniform(0.1, 0.4)), voellmy_xi=float(rng.uniform(500.0, 3000.0)))
+        rel = {"type": "ELLIPSE", "center": (float(cx), float(cy)), "rx": float(rx), "ry": float(ry), "rotation_deg": float(rot),
+               "h0": float(rng.uniform(0.5, 3.0))}
+        out.append((cfg, release_particles(z, dx, rel, cfg["rho"], fast_theta=True, grad_norm=gn)))
+    return {"name": f"ensemble{n_scenarios}_fractal2048_dx2_voellmy", "z": z, "dx": dx, "scenarios": out}
+
+
+def config5_stream(z: np.ndarray, dx: float, window_s: float, seed: int = 2029, rate: float = 20.0, median: float = 20000.0,
+                   sigma_log: float = 1.0, cap: int = 2_000_000, t_range=(30.0, 120.0)):
+    """Poisson arrivals at `rate` per second over `window_s` seconds of requests
+    on DEM z: particle count lognormal (median, sigma_log) capped at `cap`, an
+    ellipse of area N/16 m^2 (UNIFORM at 0.5 m) with random aspect and
+    position in the upper third, friction law uniform over COULOMB / VOELLMY /
+    MU_I with coefficients from the ranges of the other workloads, total_time
+    uniform in t_range. Yields (arrival time, cfg, particles)."""
+    rng = np.random.default_rng(seed)
+    gn = terrain_gradient_norm(z, dx)
+    L = z.shape[0] * dx
+    t = 0.0
+    reqs = []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > window_s:
+            break
+        N = int(min(cap, rng.lognormal(math.log(median), sigma_log)))
+        area = N / (4.0 / (dx * dx))
+        aspect = rng.uniform(1.0, 2.5)
+        rx = math.sqrt(area * aspect / math.pi)
+        ry = area / (math.pi * rx)
+        r = max(rx, ry) + 4 * dx
+        cx = rng.uniform(r, max(r + 1.0, L / 3.0))
+        cy = rng.uniform(r, z.shape[1] * dx - r)
+        law = ["COULOMB", "VOELLMY", "MU_I"][int(rng.integers(3))]
+        cfg = dict(gravity=9.81, rho=1500.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0,
+                   total_time=float(rng.uniform(*t_range)), friction=law)
+        if law == "COULOMB":
+            cfg["coulomb_mu"] = float(rng.uniform(0.3, 0.6))
+        elif law == "VOELLMY":
+            cfg.update(voellmy_mu=float(rng.uniform(0.1, 0.4)), voellmy_xi=float(rng.uniform(500.0, 3000.0)))
+        else:
+            cfg.update(mui_mu1=float(rng.uniform(0.3, 0.45)), mui_mu2=float(rng.uniform(0.55, 0.7)), mui_I0=0.279, mui_d=5e-4, mui_phi=0.6)
+        rel = {"type": "ELLIPSE", "center": (float(cx), float(cy)), "rx": rx, "ry": ry, "rotation_deg": float(rng.uniform(0, 180)),
+               "h0": float(rng.uniform(0.5, 3.0))}
+        reqs.append((t, cfg, release_particles(z, dx, rel, cfg["rho"], fast_theta=True, grad_norm=gn)))
+    return reqs
