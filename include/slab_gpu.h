@@ -157,7 +157,8 @@ slab_status slab_synchronize(slab_ctx* ctx);
 slab_status slab_download_particles(slab_ctx* ctx, double* x_xy, double* v_xy, double* vz, double* h, double* A, double* mass, double* z);
 
 /* The grid fields of the last step over the reference's remeshed bounding
- * box (src/simulation.cpp:603-612). */
+ * box (src/simulation.cpp:603-612). With all four field pointers NULL only
+ * the box (Nx, Ny, i_off, j_off) is filled in, to size the buffers. */
 slab_status slab_download_grid(slab_ctx* ctx, slab_grid_view* view);
 
 /* Full-terrain maxima (Grid::h_max, Grid::v_max2), as written by

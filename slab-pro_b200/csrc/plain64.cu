@@ -437,6 +437,7 @@ struct Plain64 final : Path {
         gv_->Ny = gNy;
         gv_->i_off = i0;
         gv_->j_off = j0;
+        if (!gv_->h && !gv_->mass && !gv_->v && !gv_->vz) return;  // box only
         if ((int64_t)gNx * gNy > gv_->cap_nodes) throw Error{SLAB_E_ARG, "grid view capacity too small"};
         N64 n = nodes();
         std::vector<double> row(2 * (size_t)gNy);

@@ -624,6 +624,7 @@ void Engine32::download_grid(int sid, slab_grid_view* gv) {
     gv->Ny = gNy;
     gv->i_off = i0;
     gv->j_off = j0;
+    if (!gv->h && !gv->mass && !gv->v && !gv->vz) return;  // box only
     if ((int64_t)gNx * gNy > gv->cap_nodes) throw Error{SLAB_E_ARG, "grid view capacity too small"};
     const std::vector<float> f = gather_nodes(sid, c.stepid, i0, j0, gNx, gNy, {d_oh.get(), d_om.get(), d_ovz.get()}, true);
     const size_t n = (size_t)gNx * gNy;

@@ -3,6 +3,7 @@ reference's own step-loop sources (oracle/_ref/slab_ref, built by
 `make -C oracle ref` from the reference tree) on the cases in cases.py.
 
     python tests/golden/make_golden.py [case ...]
+    python tests/golden/make_golden.py setup_poisson
 
 Each fixture holds, from the reference run:
   frame0_digest   sha256 of the initial particle arrays (setup parity)
@@ -118,8 +119,35 @@ def _frame_file(sim_dir: str, k: int) -> str:
     raise FileNotFoundError(f"frame {k} in {sim_dir}")
 
 
+def make_setup_poisson():
+    """setup_poisson.json: sha256 of the reference's initial particles for
+    every case with POISSON sampling (the reference's own sampler and
+    std::rand), written by the reference binary's --init-only run."""
+    out = {}
+    for name in cases.CASES:
+        c = cases.CASES[name]()
+        with tempfile.TemporaryDirectory() as d:
+            cfg_path = write_inputs(c, d)
+            with open(cfg_path) as f:
+                j = json.load(f)
+            j["numerical_params"]["sampling_method"] = "POISSON"
+            with open(cfg_path, "w") as f:
+                json.dump(j, f, indent=1)
+            run_ref(cfg_path, "--init-only")
+            sim_dir = os.path.join(d, "out", c["name"])
+            P = O.read_particles_bin(sorted(glob.glob(os.path.join(sim_dir, "particles", "particles_frame_*.bin")))[0])
+            out[name] = {"Np": int(len(P["h"])), "digest": cases.particle_digest(P)}
+    with open(os.path.join(HERE, "setup_poisson.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("setup_poisson.json:", {k: v["Np"] for k, v in out.items()})
+
+
 if __name__ == "__main__":
     if not os.path.exists(O.REF_BIN):
         sys.exit("oracle/_ref/slab_ref is not built (make -C oracle ref)")
-    for n in (sys.argv[1:] or list(cases.CASES)):
-        make(n)
+    args = sys.argv[1:]
+    if args == ["setup_poisson"]:
+        make_setup_poisson()
+    else:
+        for n in (args or list(cases.CASES)):
+            make(n)

@@ -10,9 +10,16 @@ import slab
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
+# header -> the library that implements it
+LIBS = {"slab_gpu.h": os.path.join(ROOT, "slab-pro_b200", "lib", "libslab_gpu.so"),
+        "slab_host.h": os.path.join(ROOT, "slab-pro_b200", "lib", "libslab_sim.so")}
+
+
+def declared_functions(header=None):
     names = set()
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        if header and os.path.basename(h) != header:
+            continue
         txt = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
         txt = re.sub(r"//[^\n]*", "", txt)
         for m in re.finditer(r"\b(slab_[A-Za-z0-9_]+)\s*\(", txt):
@@ -28,9 +35,12 @@ def test_header_declares_entry_points():
 
 
 def test_library_exports_every_declared_symbol():
-    L = ctypes.CDLL(slab.LIB_PATH)
-    missing = [n for n in declared_functions() if not hasattr(L, n)]
-    assert not missing, missing
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        name = os.path.basename(h)
+        assert name in LIBS, f"no library recorded for {name}"
+        L = ctypes.CDLL(LIBS[name])
+        missing = [n for n in declared_functions(name) if not hasattr(L, n)]
+        assert not missing, (name, missing)
 
 
 def test_version_and_status_names_without_gpu():
