@@ -172,8 +172,9 @@ slab_status slab_conservation(slab_ctx* ctx, double out[4]);
 /* time, dt, frame and steps so far (Simulation members time, dt, frame). */
 slab_status slab_get_state(slab_ctx* ctx, double* time, double* dt, int32_t* frame, int64_t* steps);
 
-/* Device-time breakdown of the last advance call in milliseconds, per kernel
- * family: out[0] dt/control, [1] bin/sort, [2] P2G, [3] grid update, [4] G2P.
+/* Device-time breakdown since profiling was switched on, in milliseconds, per
+ * kernel family: out[0] dt/control, [1] binning (tile descriptors), [2] P2G,
+ * [3] grid update, [4] G2P (the next step's dt runs at its end).
  * Mirrors the reference's per-phase timers (src/simulation.cpp:512-519).
  * Enabled by slab_set_profiling(ctx, 1); adds event records per step. */
 slab_status slab_set_profiling(slab_ctx* ctx, int32_t on);
@@ -230,6 +231,10 @@ slab_status slab_batch_download_max_box(slab_batch* b, int32_t scenario_id, int3
 /* out[0] = particle-steps, out[1] = active node-steps, over all scenarios. */
 slab_status slab_batch_work_counters(slab_batch* b, int64_t out[2]);
 int64_t slab_batch_kernel_launches(const slab_batch* b);
+/* Per-kernel device times of the batch's steps, as slab_set_profiling /
+ * slab_get_phase_times (adds event records per step while on). */
+slab_status slab_batch_set_profiling(slab_batch* b, int32_t on);
+slab_status slab_batch_phase_times(slab_batch* b, double out[5]);
 const char* slab_batch_last_error(const slab_batch* b);
 void slab_batch_destroy(slab_batch* b);
 

@@ -263,6 +263,23 @@ slab_status slab_batch_set_stream(slab_batch* b, void* stream) {
 
 int64_t slab_batch_kernel_launches(const slab_batch* b) { return b && b->E ? b->E->nlaunch : 0; }
 
+slab_status slab_batch_set_profiling(slab_batch* b, int32_t on) {
+    if (!b) return SLAB_E_ARG;
+    return bguard(b, [&] {
+        b->E->timer.collect();
+        b->E->timer.reset();
+        b->E->timer.on = on != 0;
+    });
+}
+
+slab_status slab_batch_phase_times(slab_batch* b, double out[5]) {
+    if (!b || !out) return SLAB_E_ARG;
+    return bguard(b, [&] {
+        b->E->timer.collect();
+        for (int k = 0; k < 5; ++k) out[k] = b->E->timer.acc[k];
+    });
+}
+
 const char* slab_batch_last_error(const slab_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 void slab_batch_destroy(slab_batch* b) {

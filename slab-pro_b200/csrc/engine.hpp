@@ -125,7 +125,7 @@ struct PhaseTimer {
     void collect() {
         if (pending.empty()) return;
         SLAB_CUDA(cudaEventSynchronize(pool[pending.back()[4]]));
-        static const int phase_of[4] = {0, 2, 3, 4};
+        static const int phase_of[4] = {1, 2, 3, 4};  // tile descriptors, P2G, grid update, G2P
         for (auto& ev : pending) {
             for (int k = 0; k < 4; ++k) {
                 float ms = 0;

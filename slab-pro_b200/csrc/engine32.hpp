@@ -19,7 +19,7 @@ class Engine32 {
         Ctl* ctl = nullptr;
         Ctl* h_ctl = nullptr;
         double mass_fp64 = 0;
-        dptr<int32_t> cell[2], id[2], grp[2], grp_stamp[2], act_list[2];
+        dptr<int32_t> cell[2], id[2], grp[2], act_list[2];
         dptr<float2> f[2], v[2];
         dptr<float> h[2], m[2], vz[2], z[2];
         dptr<int32_t> act_stamp, slot_of, nxt_off, gt_stamp, gt_list, blk_of;

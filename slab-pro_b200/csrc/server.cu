@@ -98,7 +98,8 @@ int64_t footprint_of(const slab_server* s, int Np) {
     const int64_t TX = (s->terrain.Nx + TILE - 1) / TILE, TY = (s->terrain.Ny + TILE - 1) / TILE, nt = TX * TY;
     const int64_t act = std::min<int64_t>(nt, Np / 4 + 256);
     // particle buffers, tile metadata, work descriptors and partials, node blocks
-    return (int64_t)Np * 80 + nt * 132 + act * (PART_STRIDE * 4 + (int64_t)sizeof(TileDesc) + 8) + act * NCELL * 36;
+    return (int64_t)Np * 80 + nt * (2 * GRP_STRIDE * 4 + 7 * 4) + act * (PART_STRIDE * 4 + (int64_t)sizeof(TileDesc) + 8) +
+           act * NCELL * 36;
 }
 
 Ctl empty_ctl(const slab_server* s) {

@@ -81,11 +81,16 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_cell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2CSmem)));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(k32::P2W_WARPS * sizeof(k32::P2WWarp))));
     if (const char* e = std::getenv("SLAB_P2G_ACC")) acc_mode = std::atoi(e);
     int dev = 0, sms = 0, occ_p = 0, occ_g = 0, occ_u = 0;
     SLAB_CUDA(cudaGetDevice(&dev));
     SLAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    if (acc_mode == k32::ACC_CELL)
+    if (acc_mode == k32::ACC_WARP)
+        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g_warp, k32::P2W_THREADS,
+                                                                k32::P2W_WARPS * sizeof(k32::P2WWarp)));
+    else if (acc_mode == k32::ACC_CELL)
         SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem)));
     else
         SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g<k32::ACC_HILO>, k32::P2G_THREADS, sizeof(k32::P2GSmem)));
@@ -94,7 +99,7 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     grid_p2g = sms * std::max(occ_p, 1);
     grid_g2p = sms * std::max(occ_g, 1);
     grid_grid = sms * std::max(occ_u, 1);
-    grid_prep = sms * 2;
+    grid_prep = sms * 8;  // one thread per active tile: room for ~300 k tiles in one sweep
 }
 
 Engine32::~Engine32() {}
@@ -131,6 +136,16 @@ Shared Engine32::shared() const {
 
 namespace k32 {
 // Blocks of a retired scenario: maxima and stamps reset before reuse.
+// initial segment records of the occupied tiles of a new scenario (stamp 0)
+__global__ void k_scatter_tiles(const int32_t* __restrict__ tiles, const int32_t* __restrict__ recs, int n, int32_t* grp,
+                                int32_t* act_stamp) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int t = tiles[q];
+    for (int k = 0; k < GRP_STRIDE; ++k) grp[(size_t)t * GRP_STRIDE + k] = recs[(size_t)q * GRP_STRIDE + k];
+    act_stamp[t] = 0;
+}
+
 __global__ void k_release_blocks(const int32_t* ids, int n, float* hmax, float* vmax2, int32_t* stamp, int32_t* owner) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)n * NCELL; k += (int64_t)gridDim.x * blockDim.x) {
         const int b = ids[k / NCELL];
@@ -268,7 +283,6 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
         S.vz[b] = dalloc<float>(Np);
         S.z[b] = dalloc<float>(Np);
         S.grp[b] = dalloc<int32_t>((size_t)ntiles * GRP_STRIDE);
-        S.grp_stamp[b] = dalloc<int32_t>(ntiles);
         S.act_list[b] = dalloc<int32_t>(S.act_cap);
     }
     S.act_stamp = dalloc<int32_t>(ntiles);
@@ -322,16 +336,18 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
         o_z[k] = (float)z[q];
         o_id[k] = q;
     }
-    std::vector<int32_t> grp((size_t)ntiles * GRP_STRIDE, 0), gstamp(ntiles, -1), astamp(ntiles, -1), alist;
+    // segment records of the occupied tiles only (the stamps mark every other
+    // tile's record as stale, so nothing of size ntiles crosses the bus)
+    std::vector<int32_t> recs, alist;
     for (int t = 0; t < ntiles; ++t) {
         if (!cnt[t]) continue;
-        int32_t* G = grp.data() + (size_t)t * GRP_STRIDE;
+        int32_t G[GRP_STRIDE] = {0};
         G[0] = start[t];
         G[1] = start[t + 1];
         G[2] = start[t + 1];
         G[3 + 4] = cnt[t];
-        gstamp[t] = 0;
-        astamp[t] = 0;
+        G[GRP_STAMP] = 0;
+        recs.insert(recs.end(), G, G + GRP_STRIDE);
         alist.push_back(t);
     }
     if ((int)alist.size() > S.act_cap) throw Error{SLAB_E_OOM, "active tile capacity"};
@@ -363,11 +379,18 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     h2d(S.id[0].get(), o_id.data(), Np, st);
     h2d(S.vz[0].get(), o_vz.data(), Np, st);
     h2d(S.z[0].get(), o_z.data(), Np, st);
-    h2d(S.grp[0].get(), grp.data(), grp.size(), st);
-    h2d(S.grp_stamp[0].get(), gstamp.data(), ntiles, st);
-    SLAB_CUDA(cudaMemsetAsync(S.grp_stamp[1].get(), 0xff, ntiles * sizeof(int32_t), st));
-    h2d(S.act_stamp.get(), astamp.data(), ntiles, st);
+    for (int b = 0; b < 2; ++b)  // every record stale (stamp -1)
+        SLAB_CUDA(cudaMemsetAsync(S.grp[b].get(), 0xff, (size_t)ntiles * GRP_STRIDE * sizeof(int32_t), st));
+    SLAB_CUDA(cudaMemsetAsync(S.act_stamp.get(), 0xff, ntiles * sizeof(int32_t), st));
     h2d(S.act_list[0].get(), alist.data(), alist.size(), st);
+    if (!alist.empty()) {
+        dptr<int32_t> d_recs = dalloc<int32_t>(recs.size());
+        h2d(d_recs.get(), recs.data(), recs.size(), st);
+        const int n = (int)alist.size();
+        k32::k_scatter_tiles<<<(n + 127) / 128, 128, 0, st>>>(S.act_list[0].get(), d_recs.get(), n, S.grp[0].get(), S.act_stamp.get());
+        SLAB_CUDA(cudaGetLastError());
+        SLAB_CUDA(cudaStreamSynchronize(st));  // d_recs is freed on return
+    }
     SLAB_CUDA(cudaMemsetAsync(S.gt_stamp.get(), 0xff, ntiles * sizeof(int32_t), st));
     SLAB_CUDA(cudaMemsetAsync(S.blk_of.get(), 0xff, ntiles * sizeof(int32_t), st));
     SCnt c0{};
@@ -407,7 +430,6 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     for (int b = 0; b < 2; ++b) {
         D.buf[b] = PBuf{S.cell[b].get(), S.f[b].get(), S.v[b].get(), S.h[b].get(), S.m[b].get(), S.id[b].get(), S.vz[b].get(), S.z[b].get()};
         D.grp[b] = S.grp[b].get();
-        D.grp_stamp[b] = S.grp_stamp[b].get();
         D.act_list[b] = S.act_list[b].get();
     }
     D.act_stamp = S.act_stamp.get();
@@ -433,16 +455,18 @@ void Engine32::launch_begin(int t0) {
 void Engine32::launch_t0() {
     const Shared sh = shared();
     k32::k_begin<<<1, 1024, 0, st>>>(sh, 1);
-    if (acc_mode != k32::ACC_CELL) k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
+    k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
     launch_p2g(sh);
     k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
     SLAB_CUDA(cudaGetLastError());
-    nlaunch += acc_mode != k32::ACC_CELL ? 4 : 3;
+    nlaunch += 4;
     pending_blocks = 0;  // later reads of the pool count see these blocks
 }
 
 void Engine32::launch_p2g(const Shared& sh) {
-    if (acc_mode == k32::ACC_CELL)
+    if (acc_mode == k32::ACC_WARP)
+        k32::k_p2g_warp<<<grid_p2g, k32::P2W_THREADS, k32::P2W_WARPS * sizeof(k32::P2WWarp), st>>>(sh);
+    else if (acc_mode == k32::ACC_CELL)
         k32::k_p2g_cell<<<grid_p2g, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh);
     else if (acc_mode == k32::ACC_I32)
         k32::k_p2g<k32::ACC_I32><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
@@ -454,9 +478,7 @@ void Engine32::launch_p2g(const Shared& sh) {
 
 void Engine32::launch_kernel(int k, const Shared& sh) {
     switch (k) {
-        case 0:  // the cell P2G kernel builds its own descriptors
-            if (acc_mode != k32::ACC_CELL) k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
-            break;
+        case 0: k32::k_prep<<<grid_prep, 256, 0, st>>>(sh); break;
         case 1: launch_p2g(sh); break;
         case 2: k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh); break;
         case 3: k32::k_g2p<<<grid_g2p, NCELL, 0, st>>>(sh, T.z.get()); break;
@@ -486,7 +508,7 @@ void Engine32::enqueue_steps(int chunk) {
     } else {
         graphs.launch(chunk, st, [&] { launch_step(); });
     }
-    nlaunch += (acc_mode != k32::ACC_CELL ? 4 : 3) * (int64_t)chunk;
+    nlaunch += 4 * (int64_t)chunk;
 }
 
 SCnt Engine32::counters(int sid) {
@@ -712,3 +734,12 @@ std::unique_ptr<Path> make_split32(const Terrain& t, const slab_params& p, cudaS
 }
 
 }  // namespace slab
+
+#ifdef SLAB_PHASE_CLOCKS
+// per-phase cycle sums of the P2G kernel (instrumented builds only); reading clears them
+extern "C" int slab_debug_phase_clocks(unsigned long long* out16) {
+    if (cudaMemcpyFromSymbol(out16, slab::k32::g_phase_clk, 16 * sizeof(unsigned long long)) != cudaSuccess) return 1;
+    const unsigned long long z[16] = {0};
+    return cudaMemcpyToSymbol(slab::k32::g_phase_clk, z, sizeof(z)) == cudaSuccess ? 0 : 1;
+}
+#endif

@@ -28,7 +28,11 @@
 
 namespace slab {
 
-constexpr int TILE = 16;              // base cells per tile edge
+#ifndef SLAB_TILE
+#define SLAB_TILE 8
+#endif
+constexpr int TILE = SLAB_TILE;       // base cells per tile edge (8 or 16)
+static_assert(TILE == 8 || TILE == 16, "tile edge must be 8 or 16 cells");
 constexpr int TN = TILE + 2;          // node window edge of a tile
 constexpr int NCELL = TILE * TILE;    // cells per tile = threads per CTA
 constexpr int NQ = 7;                 // P2G sums: m, m vx, m vy, m h, Fx, Fy, m vz
@@ -77,10 +81,13 @@ struct TileDesc {
     int32_t pad_;
 };
 
-// Segment record of a tile in a particle buffer (GRP_STRIDE ints): [0] first
-// stayer, [1] first mover (= end of stayers), [2] end, [3 + d] number of
-// particles that moved in direction d (d = 4: the stayers).
-constexpr int GRP_STRIDE = 12;
+// Segment record of a tile in a particle buffer (GRP_STRIDE ints, one
+// 64-byte line): [0] first stayer, [1] first mover (= end of stayers),
+// [2] end, [3 + d] number of particles that moved in direction d (d = 4: the
+// stayers), [GRP_STAMP] the step (seq) the record belongs to -- a record
+// with another stamp is stale.
+constexpr int GRP_STRIDE = 16;
+constexpr int GRP_STAMP = 12;
 
 // Device descriptor of one scenario.
 struct Scn {
@@ -93,7 +100,6 @@ struct Scn {
     int32_t Np;
     PBuf buf[2];
     int32_t* grp[2];        // [ntiles][GRP_STRIDE] segment records (see GRP_STRIDE)
-    int32_t* grp_stamp[2];  // [ntiles] seq at which grp was written
     int32_t* act_stamp;     // [ntiles] last seq the tile was put on an active list
     int32_t* act_list[2];   // active tiles of each parity
     int32_t* slot_of;       // [ntiles] work index (partial slot) of the tile in the running step

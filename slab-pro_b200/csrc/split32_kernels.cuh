@@ -176,6 +176,33 @@ __global__ void k_arm_begin(Shared sh, int64_t steps_left, int stop_at_frame) {
     begin_scenarios(sh, 0);
 }
 
+// After the last CTA of a launch has listed its grid tiles: the prefix of
+// grid tiles over scenarios (the work list of k_grid). Call with the whole
+// CTA; s_warp needs 33 ints.
+__device__ void close_grid_list(const Shared& sh, int* s_warp) {
+    __shared__ int s_last, s_tot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&sh.done[0], 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    int total = 0;
+    for (int base = 0; base < sh.nscn; base += blockDim.x) {
+        const int s = base + threadIdx.x;
+        const int cnt = (s < sh.nscn && sh.scn[s].ctl->active) ? *(volatile int*)&sh.scn[s].cnt->gt_count : 0;
+        const int ex = block_exclusive_scan(cnt, s_warp);
+        if (s < sh.nscn) sh.grid_pref[s] = total + ex;
+        if (threadIdx.x == blockDim.x - 1) s_tot = ex + cnt;
+        __syncthreads();
+        total += s_tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sh.grid_pref[sh.nscn] = total;
+}
+
 // K1 (bookkeeping half): one thread per active tile t. Its particles are
 // the stayers of its own segment in the current buffer plus the movers of
 // the 8 neighbour segments that moved to t (those are filtered by cell when
@@ -207,8 +234,8 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
             rs[d] = rl[d] = 0;
             if (si >= 0 && sj >= 0 && si < sh.TX && sj < sh.TY) {
                 const int s = si * sh.TY + sj;
-                if (S.grp_stamp[cur][s] == seq) {
-                    const int32_t* G = S.grp[cur] + s * GRP_STRIDE;
+                const int32_t* G = S.grp[cur] + (size_t)s * GRP_STRIDE;
+                if (G[GRP_STAMP] == seq) {
                     if (d == 4) {
                         rs[d] = G[0];
                         rl[d] = G[1] - G[0];
@@ -248,29 +275,8 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
         sh.desc[w] = D;
     }
     // the last CTA builds the grid-tile work list prefix for k_grid
-    __shared__ int s_last, s_tot;
     __shared__ int s_warp[33];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = (atomicAdd(&sh.done[0], 1u) == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (s_last) {
-        __threadfence();
-        int total = 0;
-        for (int base = 0; base < sh.nscn; base += blockDim.x) {
-            const int s = base + threadIdx.x;
-            const int cnt = (s < sh.nscn && sh.scn[s].ctl->active) ? *(volatile int*)&sh.scn[s].cnt->gt_count : 0;
-            const int ex = block_exclusive_scan(cnt, s_warp);
-            if (s < sh.nscn) sh.grid_pref[s] = total + ex;
-            if (threadIdx.x == blockDim.x - 1) s_tot = ex + cnt;
-            __syncthreads();
-            total += s_tot;
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) sh.grid_pref[sh.nscn] = total;
-    }
+    close_grid_list(sh, s_warp);
 }
 
 // ------------------------------------------------------------------- P2G
@@ -284,7 +290,8 @@ constexpr int P2G_THREADS = 256;
 //            precision relative to itself; two plain (non-returning) atomics
 //  ACC_I64   one int64 per sum at 2^-52 of the bound
 //  ACC_CELL  no fixed point: k_p2g_cell, FP32 sums over cell-sorted particles
-enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2, ACC_CELL = 3 };
+//  ACC_WARP  k_p2g_warp: ACC_HILO sums with one warp per tile
+enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2, ACC_CELL = 3, ACC_WARP = 4 };
 
 struct P2GSmem {
     long long node[NQ * TN * TN];  // fixed-point sums of the (TILE+2)^2 window (int32 pairs / int64)
@@ -470,180 +477,370 @@ __global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(Shared sh) {
     }
 }
 
-// ------------------------------------------------ P2G over cell-sorted particles
+// --------------------------------------- P2G, one warp per tile (fixed point)
 
-// K1 for one work item, by warp 0 of a CTA (lane d < 9 reads direction d):
-// the tile's 9 candidate ranges and exact count, its segment in the next
-// buffer, and the grid tiles of its node window on the grid-tile list. The
-// descriptor goes to shared memory and to sh.desc[w] for G2P.
-__device__ void prep_tile(const Shared& sh, int w, TileDesc* sd) {
-    const int lane = threadIdx.x & 31;
-    int sid = 0, loc = 0;
-    find_work(sh.work_pref, sh.nscn, w, sid, loc);
-    const Scn& S = sh.scn[sid];
-    SCnt* n = S.cnt;
-    const int seq = n->seq, cur = seq & 1;
-    const int t = S.act_list[cur][loc];
-    const int ti = t / sh.TY, tj = t % sh.TY;
-    int rs = 0, rl = 0, cnt = 0;
-    if (lane < 9) {
-        const int si = ti - dir_i(lane), sj = tj - dir_j(lane);
-        if (si >= 0 && sj >= 0 && si < sh.TX && sj < sh.TY) {
-            const int sidx = si * sh.TY + sj;
-            if (S.grp_stamp[cur][sidx] == seq) {
-                const int32_t* G = S.grp[cur] + sidx * GRP_STRIDE;
-                if (lane == 4) {
-                    rs = G[0];
-                    rl = G[1] - G[0];
-                } else {
-                    rs = G[1];
-                    rl = G[2] - G[1];
-                }
-                cnt = G[3 + lane];
-            }
-        }
+constexpr int P2W_WARPS = TILE == 8 ? 8 : 2;  // tiles in flight per CTA
+constexpr int P2W_THREADS = 32 * P2W_WARPS;
+constexpr int P2W_REG = 1;                     // chunks of 32 candidates a lane keeps between the passes
+
+struct P2WWarp {
+    int node[2 * NQ * TN * TN];  // fixed-point sums of the tile's node window: hi [q][node], then lo
+    int ccnt[NCELL];             // particles per cell
+    TileDesc d;
+};
+
+// P2G quantities of one candidate of tile (ti, tj), with the slope of its
+// containing cell read from the FP32 terrain copy; valid = in the tile
+__device__ __forceinline__ PQ warp_pq(const Shared& sh, const PBuf& B, const TileDesc& D, int k, int ti, int tj, float g, float hod, bool outs,
+                                      bool& valid, bool& stayer) {
+    int d;
+    const int src = cand_to_index(k, D, d);
+    const int32_t cell = B.cell[src];
+    const float2 f = B.f[src], v = B.v[src];
+    const float h = B.h[src], m = B.m[src];
+    const float vz = outs ? B.vz[src] : 0.f;
+    const int ci = cell_i(cell), cj = cell_j(cell);
+    const int li = ci - ti * TILE, lj = cj - tj * TILE;
+    valid = (unsigned)li < TILE && (unsigned)lj < TILE;
+    stayer = d == 4;
+    PQ p;
+    p.li = li;
+    p.lj = lj;
+    p.fx = f.x;
+    p.fy = f.y;
+    if (!valid) {
+        p.m = p.mvx = p.mvy = p.mh = p.mvz = p.Kgx = p.Kgy = p.Khh = 0.f;
+        return p;
     }
-    int incl = rl, tot = cnt;
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-        tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    }
-    tot += __shfl_xor_sync(0xffffffffu, tot, 16);
-    if (lane < 9) {
-        sd->rstart[lane] = rs;
-        sd->rpref[lane] = incl - rl;
-    }
-    if (lane == 8) sd->rpref[9] = incl;
-    // grid tiles of the node window: the ones not yet listed this step
-    const int stamp = n->stepid;
-    bool fresh = false;
-    int gt = 0;
-    if (lane < 4) {
-        const int gi = ti + (lane >> 1), gj = tj + (lane & 1);
-        if (gi < sh.TX && gj < sh.TY) {
-            gt = gi * sh.TY + gj;
-            fresh = atomicMax(&S.gt_stamp[gt], stamp) < stamp;
-        }
-    }
-    const unsigned fm = __ballot_sync(0xffffffffu, fresh);
-    int at = 0, off = 0;
-    if (lane == 0) {
-        if (fm) at = atomicAdd(&n->gt_count, __popc(fm));
-        off = atomicAdd(&n->cursor, tot);
-        S.slot_of[t] = w;
-        sd->t = t;
-        sd->sid = sid;
-        sd->total = tot;
-        sd->nxt_off = off;
-        sd->pad_ = 0;
-    }
-    at = __shfl_sync(0xffffffffu, at, 0);
-    if (fresh) S.gt_list[at + __popc(fm & ((1u << lane) - 1u))] = gt;
-    __syncwarp();
-    if (lane < (int)(sizeof(TileDesc) / 4)) reinterpret_cast<int*>(sh.desc + w)[lane] = reinterpret_cast<const int*>(sd)[lane];
+    const float4 dm = sh.dem[(int64_t)(ci + (f.x >= 1.f ? 1 : 0)) * sh.Ny + (cj + (f.y >= 1.f ? 1 : 0))];
+    const float K = m * g * dm.z * dm.z;
+    p.m = m;
+    p.mvx = m * v.x;
+    p.mvy = m * v.y;
+    p.mh = m * h;
+    p.mvz = m * vz;
+    p.Kgx = K * dm.x;
+    p.Kgy = K * dm.y;
+    p.Khh = K * h * hod;
+    return p;
 }
 
-// After the last CTA of a launch has listed its grid tiles: the prefix of
-// grid tiles over scenarios (the work list of k_grid). Call with the whole
-// CTA; s_warp needs 33 ints.
-__device__ void close_grid_list(const Shared& sh, int* s_warp) {
-    __shared__ int s_last, s_tot;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = (atomicAdd(&sh.done[0], 1u) == gridDim.x - 1);
+// K2 variant: P2G of one tile (src/simulation.cpp:726-798) by one warp, so
+// that many tiles are in flight on an SM with no block-wide barrier. The
+// sums are 32-bit fixed-point pairs in the warp's shared-memory node window,
+// added with integer atomics: exact and associative, so the result does not
+// depend on the order of the particles (bitwise reproducible, the same alone
+// or inside a batch). Pass A bounds one contribution per quantity (b) and the
+// particles of one cell (mcc); a node's sum stays below 9 * mcc * 0.75 * b,
+// and the scale is the largest power of two that keeps that below 2^30; the
+// hi word is the rounded contribution, the lo word the rest at 2^-20.
+__global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P2WWarp& sw = reinterpret_cast<P2WWarp*>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * P2W_WARPS + (threadIdx.x >> 5), nw = gridDim.x * P2W_WARPS;
+    const int nwork = sh.work_pref[sh.nscn];
+    const int per = (nwork + nw - 1) / nw;
+    const int w0 = min(gw * per, nwork), w1 = min(w0 + per, nwork);
+    int* hi = sw.node;
+    int* lo = sw.node + NQ * TN * TN;
+    for (int w = w0; w < w1; ++w) {
+        if (lane < (int)(sizeof(TileDesc) / 4)) reinterpret_cast<int*>(&sw.d)[lane] = reinterpret_cast<const int*>(sh.desc + w)[lane];
+        for (int k = lane; k < 2 * NQ * TN * TN; k += 32) sw.node[k] = 0;
+        for (int k = lane; k < NCELL; k += 32) sw.ccnt[k] = 0;
+        __syncwarp();
+        const TileDesc& D = sw.d;
+        const Scn& S = sh.scn[D.sid];
+        const SCnt* n = S.cnt;
+        const int cur = n->seq & 1;
+        const bool outs = n->outs != 0;
+        const int ti = D.t / sh.TY, tj = D.t % sh.TY;
+        const int ncand = D.rpref[9];
+        const PBuf B = S.buf[cur];
+        const float g = S.g, hod = 0.5f * S.ood;
+        // pass A: bounds and cell counts (the first chunks stay in registers)
+        PQ keep[P2W_REG];
+        bool kval[P2W_REG];
+        float bm = 0.f, bvx = 0.f, bvy = 0.f, bh = 0.f, bvz = 0.f, bF = 0.f;
+        int mcc = 0;
+        for (int c = 0, k0 = 0; k0 < ncand; ++c, k0 += 32) {
+            const int k = k0 + lane;
+            bool valid = false, stayer = false;
+            PQ p;
+            if (k < ncand) p = warp_pq(sh, B, D, k, ti, tj, g, hod, outs, valid, stayer);
+            if (k < ncand && !valid && stayer) atomicOr(&S.ctl->err, ERR_MOVE);  // a stayer outside its tile
+#pragma unroll
+            for (int r = 0; r < P2W_REG; ++r)
+                if (c == r) {
+                    keep[r] = p;
+                    kval[r] = valid;
+                }
+            if (valid) {
+                mcc = max(mcc, atomicAdd(&sw.ccnt[p.li * TILE + p.lj], 1) + 1);
+                bm = fmaxf(bm, p.m);
+                bvx = fmaxf(bvx, fabsf(p.mvx));
+                bvy = fmaxf(bvy, fabsf(p.mvy));
+                bh = fmaxf(bh, p.mh);
+                bvz = fmaxf(bvz, fabsf(p.mvz));
+                bF = fmaxf(bF, p.Khh + fmaxf(fabsf(p.Kgx), fabsf(p.Kgy)));
+            }
+        }
+        bm = warp_max(bm);
+        bvx = warp_max(bvx);
+        bvy = warp_max(bvy);
+        bh = warp_max(bh);
+        bvz = warp_max(bvz);
+        bF = warp_max(bF);
+        for (int o = 16; o > 0; o >>= 1) mcc = max(mcc, __shfl_xor_sync(0xffffffffu, mcc, o));
+        const float bq[NQ] = {bm, bvx, bvy, bh, bF, bF, bvz};
+        float sc[NQ], isc[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const float bound = 9.f * (float)mcc * 0.75f * bq[q];
+            int e = 0;
+            if (bound > 0.f) {
+                int E;
+                frexpf(bound, &E);  // bound < 2^E
+                e = min(max(30 - E, -120), 120);
+            }
+            sc[q] = ldexpf(1.f, e);
+            isc[q] = ldexpf(1.f, -e);
+        }
+        // pass B: fixed-point contributions
+        for (int c = 0, k0 = 0; k0 < ncand; ++c, k0 += 32) {
+            const int k = k0 + lane;
+            bool valid = false, stayer = false;
+            PQ p;
+            if (c < P2W_REG) {
+#pragma unroll
+                for (int r = 0; r < P2W_REG; ++r)
+                    if (c == r) {
+                        p = keep[r];
+                        valid = kval[r];
+                    }
+            } else if (k < ncand) {
+                p = warp_pq(sh, B, D, k, ti, tj, g, hod, outs, valid, stayer);
+            }
+            if (!valid) continue;
+            float wx[3], wy[3], dwx[3], dwy[3];
+            bspline3(p.fx, wx, dwx);
+            bspline3(p.fy, wy, dwy);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const float wgt = wx[a] * wy[b];
+                    if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
+                        const int nd = (p.li + a) * TN + (p.lj + b);
+                        const float cq[NQ] = {p.m * wgt, p.mvx * wgt, p.mvy * wgt, p.mh * wgt, p.Khh * (dwx[a] * wy[b]) - p.Kgx * wgt,
+                                              p.Khh * (dwy[b] * wx[a]) - p.Kgy * wgt, p.mvz * wgt};
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            if (q == 6 && !outs) continue;
+                            const float x = cq[q] * sc[q];
+                            const int h_ = __float2int_rn(x);
+                            atomicAdd(hi + q * TN * TN + nd, h_);
+                            const int l_ = __float2int_rn((x - (float)h_) * 1048576.f);
+                            if (l_) atomicAdd(lo + q * TN * TN + nd, l_);
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        float* P = sh.part + (size_t)w * PART_STRIDE;
+        for (int k = lane; k < PART_STRIDE; k += 32) {
+            const int q = k / (TN * TN);
+            float is = isc[0];
+#pragma unroll
+            for (int r = 1; r < NQ; ++r)
+                if (q == r) is = isc[r];
+            P[k] = (float)(((double)hi[k] + (double)lo[k] * (1.0 / 1048576.0)) * (double)is);
+        }
+        __syncwarp();
     }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    int total = 0;
-    for (int base = 0; base < sh.nscn; base += blockDim.x) {
-        const int s = base + threadIdx.x;
-        const int cnt = (s < sh.nscn && sh.scn[s].ctl->active) ? *(volatile int*)&sh.scn[s].cnt->gt_count : 0;
-        const int ex = block_exclusive_scan(cnt, s_warp);
-        if (s < sh.nscn) sh.grid_pref[s] = total + ex;
-        if (threadIdx.x == blockDim.x - 1) s_tot = ex + cnt;
-        __syncthreads();
-        total += s_tot;
-        __syncthreads();
+}
+
+// ------------------------------------------------ P2G over cell-sorted particles
+
+// Optional per-phase cycle counters of the P2G kernel (builds with
+// -DSLAB_PHASE_CLOCKS only): thread 0 of each CTA adds the clock64 cycles of
+// each phase of each tile to g_phase_clk[phase]; g_phase_clk[15] counts tiles.
+#ifdef SLAB_PHASE_CLOCKS
+__device__ unsigned long long g_phase_clk[16];
+#define SLAB_PHASE_BEGIN long long t_prev_ = clock64()
+#define SLAB_PHASE_MARK(k)                                                  \
+    do {                                                                    \
+        if (threadIdx.x == 0) {                                             \
+            const long long c_ = clock64();                                 \
+            atomicAdd(&g_phase_clk[k], (unsigned long long)(c_ - t_prev_)); \
+            t_prev_ = c_;                                                   \
+        }                                                                   \
+    } while (0)
+#define SLAB_PHASE_TILE()                                         \
+    do {                                                          \
+        if (threadIdx.x == 0) atomicAdd(&g_phase_clk[15], 1ull); \
+    } while (0)
+#else
+#define SLAB_PHASE_BEGIN
+#define SLAB_PHASE_MARK(k)
+#define SLAB_PHASE_TILE()
+#endif
+
+// The work items of one CTA: a contiguous range of the flat work list, so
+// that consecutive items mostly belong to the same scenario.
+__device__ __forceinline__ void work_range(int nwork, int& w0, int& w1) {
+    const int per = (nwork + (int)gridDim.x - 1) / (int)gridDim.x;
+    w0 = min((int)blockIdx.x * per, nwork);
+    w1 = min(w0 + per, nwork);
+}
+
+// Scenario of the last work item looked up, with the step fields that do not
+// change during a launch (so a new item of the same scenario costs no loads).
+struct WorkCache {
+    int sid = -1, lo = 0, hi = 0, seq = 0, stepid = 0;
+};
+
+// index of work item w in its scenario's list (pref: the prefix over scenarios)
+__device__ __forceinline__ int cached_work(const Shared& sh, const int32_t* pref, int w, WorkCache& c) {
+    if (w < c.lo || w >= c.hi) {
+        int loc;
+        find_work(pref, sh.nscn, w, c.sid, loc);
+        c.lo = pref[c.sid];
+        c.hi = pref[c.sid + 1];
+        const SCnt* n = sh.scn[c.sid].cnt;
+        c.seq = n->seq;
+        c.stepid = n->stepid;
     }
-    if (threadIdx.x == 0) sh.grid_pref[sh.nscn] = total;
+    return w - c.lo;
 }
 
 
 constexpr int P2C_THREADS = NCELL;  // one thread per cell of the tile
+constexpr int P2C_MIN_BLOCKS = NCELL == 64 ? 8 : 2;  // resident CTAs per SM the register budget is cut for
 constexpr int P2C_WARPS = P2C_THREADS / 32;
 constexpr int NSLOT = 9;            // nodes a cell's particles reach (3 x 3)
+constexpr int P2C_CAP = 6 * NCELL;  // candidates of a tile staged in shared memory (more go through global memory)
+
+struct P2CStage {
+    float4 sa[P2C_CAP];  // staged candidates, by candidate index: f.x, f.y, m, h
+    float4 sb[P2C_CAP];  //                                        v.x, v.y, vz, -
+};
 
 struct P2CSmem {
-    float part[NQ * NSLOT][NCELL];  // per-cell sums: [q * 9 + a * 3 + b][cell]
+    union {
+        P2CStage st;                    // while the sums are taken
+        float part[NQ * NSLOT][NCELL];  // then the per-cell sums: [q * 9 + a * 3 + b][cell]
+    } u;
+    int16_t lc[P2C_CAP];   // local cell of each staged candidate (-1: not in the tile)
+    int16_t idx[P2C_CAP];  // sorted position -> candidate index
     float4 dem[(TILE + 1) * (TILE + 1)];
-    int wcur[P2C_WARPS][NCELL];     // per-warp cell counts, then per-warp write cursors
+    int wcur[P2C_WARPS][NCELL];  // per-warp cell counts, then per-warp write cursors
     int s_warp[33];
     TileDesc d;
 };
 
-// Sums of one cell's particles, in their sorted order, over the 9 nodes of
-// the cell's stencil (src/simulation.cpp:758-795); OUTS adds m vz.
+// P2G quantities of a staged particle (as load_pq)
+__device__ __forceinline__ PQ staged_pq(float4 a, float4 b, int li, int lj, const float4* dem, float g, float hod) {
+    PQ p;
+    const float4 dm = dem[(li + (a.x >= 1.f ? 1 : 0)) * (TILE + 1) + (lj + (a.y >= 1.f ? 1 : 0))];
+    const float K = a.z * g * dm.z * dm.z;
+    p.fx = a.x;
+    p.fy = a.y;
+    p.m = a.z;
+    p.mvx = a.z * b.x;
+    p.mvy = a.z * b.y;
+    p.mh = a.z * a.w;
+    p.mvz = a.z * b.z;
+    p.Kgx = K * dm.x;
+    p.Kgy = K * dm.y;
+    p.Khh = K * a.w * hod;
+    p.li = li;
+    p.lj = lj;
+    return p;
+}
+
+// Sums of one particle over the 9 nodes of its cell's stencil
+// (src/simulation.cpp:758-795); OUTS adds m vz.
 template <bool OUTS>
-__device__ __forceinline__ void cell_sums(float (&acc)[NQ][NSLOT], const int32_t* __restrict__ order, int c0, int nn, const PBuf& B,
-                                          int li, int lj, const float4* dem, float g, float hod) {
-    int nsrc = nn > 0 ? order[c0] : 0;
-    for (int r = 0; r < nn; ++r) {
-        const int src = nsrc;
-        if (r + 1 < nn) nsrc = order[c0 + r + 1];
-        const PQ p = load_pq(B, src, li, lj, dem, g, hod, OUTS);
-        float wx[3], wy[3], dwx[3], dwy[3];
-        bspline3(p.fx, wx, dwx);
-        bspline3(p.fy, wy, dwy);
+__device__ __forceinline__ void add_particle(float (&acc)[NQ][NSLOT], const PQ& p) {
+    float wx[3], wy[3], dwx[3], dwy[3];
+    bspline3(p.fx, wx, dwx);
+    bspline3(p.fy, wy, dwy);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
+    for (int a = 0; a < 3; ++a) {
 #pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const int s = a * 3 + b;
-                const float wgt = wx[a] * wy[b];
-                if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
-                    acc[0][s] += p.m * wgt;
-                    acc[1][s] += p.mvx * wgt;
-                    acc[2][s] += p.mvy * wgt;
-                    acc[3][s] += p.mh * wgt;
-                    acc[4][s] += p.Khh * (dwx[a] * wy[b]) - p.Kgx * wgt;
-                    acc[5][s] += p.Khh * (dwy[b] * wx[a]) - p.Kgy * wgt;
-                    if (OUTS) acc[6][s] += p.mvz * wgt;
-                }
+        for (int b = 0; b < 3; ++b) {
+            const int s = a * 3 + b;
+            const float wgt = wx[a] * wy[b];
+            if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
+                acc[0][s] += p.m * wgt;
+                acc[1][s] += p.mvx * wgt;
+                acc[2][s] += p.mvy * wgt;
+                acc[3][s] += p.mh * wgt;
+                acc[4][s] += p.Khh * (dwx[a] * wy[b]) - p.Kgx * wgt;
+                acc[5][s] += p.Khh * (dwy[b] * wx[a]) - p.Kgy * wgt;
+                if (OUTS) acc[6][s] += p.mvz * wgt;
             }
         }
     }
 }
 
-// K1 + K2: the tile's descriptor (prep_tile), then P2G of the tile
-// (src/simulation.cpp:726-798) as a segmented reduction over cell-sorted
-// particles, with no atomics on floats:
-//  1. each warp walks a contiguous block of the tile's candidates and counts
-//     particles per cell (lanes of one cell are grouped by __match_any_sync);
+// Sums of one cell's particles in sorted order: staged in shared memory, or
+// (tiles over P2C_CAP candidates) read through the sorted index list in
+// global memory.
+template <bool OUTS>
+__device__ __forceinline__ void cell_sums(float (&acc)[NQ][NSLOT], bool staged, const P2CSmem& sm, const int32_t* __restrict__ order,
+                                          int c0, int nn, const PBuf& B, int li, int lj, float g, float hod) {
+    if (staged) {
+        for (int r = c0; r < c0 + nn; ++r) {
+            const int k = sm.idx[r];
+            add_particle<OUTS>(acc, staged_pq(sm.u.st.sa[k], sm.u.st.sb[k], li, lj, sm.dem, g, hod));
+        }
+        return;
+    }
+    int nsrc = nn > 0 ? order[c0] : 0;
+    for (int r = 0; r < nn; ++r) {
+        const int src = nsrc;
+        if (r + 1 < nn) nsrc = order[c0 + r + 1];
+        add_particle<OUTS>(acc, load_pq(B, src, li, lj, sm.dem, g, hod, OUTS));
+    }
+}
+
+// K2: P2G of one tile (src/simulation.cpp:726-798) as a segmented reduction
+// over cell-sorted particles, with no atomics on floats. The tile's
+// descriptor comes from k_prep; then
+//  1. each warp walks a contiguous block of the tile's candidates, loads them
+//     (into shared memory, unless the tile has more than P2C_CAP candidates)
+//     and counts particles per cell (lanes of one cell are grouped by
+//     __match_any_sync);
 //  2. thread = cell: per-warp write cursors and the cell's range (a scan);
-//  3. the warps walk their blocks again and write each particle's index at
-//     its cursor: a stable counting sort by cell, into the tile's segment of
-//     the next particle buffer (unused until G2P of this step);
+//  3. the warps walk their blocks again and give each particle its place --
+//     a stable counting sort by cell -- as an index in shared memory (large
+//     tiles: an index into the tile's segment of the next particle buffer,
+//     unused until G2P);
 //  4. thread = cell: FP32 sums of the cell's particles, in sorted order, for
 //     the 9 nodes of its stencil;
 //  5. thread = node: the node's sums over its <= 9 cells, in a fixed order.
 // The candidates of a tile come in an order fixed by the previous step's G2P
 // (ordered placement), so every sum has a fixed order: results are bitwise
-// reproducible and the same alone or inside a batch.
-__global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
+// reproducible and the same alone or inside a batch. A tile costs two
+// dependent rounds of global loads (descriptor, candidates); each CTA takes
+// a contiguous run of work items.
+__global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared sh) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P2CSmem& sm = *reinterpret_cast<P2CSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const int li = tid / TILE, lj = tid % TILE;
-    const int nwork = sh.work_pref[sh.nscn];
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        if (warp == 0) prep_tile(sh, w, &sm.d);
+    int w0, w1;
+    work_range(sh.work_pref[sh.nscn], w0, w1);
+    SLAB_PHASE_BEGIN;
+    for (int w = w0; w < w1; ++w) {
+        load_desc(sh.desc + w, &sm.d);
         for (int k = tid; k < P2C_WARPS * NCELL; k += P2C_THREADS) (&sm.wcur[0][0])[k] = 0;
         __syncthreads();
+        SLAB_PHASE_MARK(0);
         const Scn& S = sh.scn[sm.d.sid];
         const int t = sm.d.t;
         const int ti = t / sh.TY, tj = t % sh.TY;
@@ -656,11 +853,11 @@ __global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
         }
         const int ncand = sm.d.rpref[9];
         const int total = sm.d.total;
+        const bool staged = ncand <= P2C_CAP;
         const PBuf B = S.buf[cur];
-        int32_t* order = S.buf[cur ^ 1].cell + sm.d.nxt_off;
         const int per = (ncand + P2C_WARPS - 1) / P2C_WARPS;
         const int k_lo = min(warp * per, ncand), k_hi = min(k_lo + per, ncand);
-        // 1. counts per (warp, cell)
+        // 1. load (stage) and count per (warp, cell)
         for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
             const int k = k0 + lane;
             int lc = -1;
@@ -668,9 +865,25 @@ __global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
                 int d;
                 const int src = cand_to_index(k, sm.d, d);
                 const int32_t cell = B.cell[src];
+                float2 f, v;
+                float m, h, vz = 0.f;
+                if (staged) {  // issued together with the cell load
+                    f = B.f[src];
+                    v = B.v[src];
+                    m = B.m[src];
+                    h = B.h[src];
+                    if (outs) vz = B.vz[src];
+                }
                 const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
                 if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
                 else if (d == 4) atomicOr(&S.ctl->err, ERR_MOVE);  // a stayer outside its tile
+                if (staged) {
+                    sm.lc[k] = (int16_t)lc;
+                    if (lc >= 0) {
+                        sm.u.st.sa[k] = make_float4(f.x, f.y, m, h);
+                        sm.u.st.sb[k] = make_float4(v.x, v.y, vz, 0.f);
+                    }
+                }
             }
             const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
             if (lc >= 0) {
@@ -680,6 +893,7 @@ __global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
             __syncwarp();
         }
         __syncthreads();
+        SLAB_PHASE_MARK(1);
         // 2. cursors: cell-major, warp-minor
         int n_c = 0;
 #pragma unroll
@@ -693,31 +907,39 @@ __global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
 #pragma unroll
         for (int q = 0; q < P2C_WARPS; ++q) sm.wcur[q][tid] += c0;
         __syncthreads();
+        SLAB_PHASE_MARK(2);
         // 3. stable placement by cell
+        int32_t* order = S.buf[cur ^ 1].cell + sm.d.nxt_off;
         for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
             const int k = k0 + lane;
             int lc = -1, src = 0;
             if (k < k_hi) {
-                int d;
-                src = cand_to_index(k, sm.d, d);
-                const int32_t cell = B.cell[src];
-                const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
-                if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
+                if (staged) {
+                    lc = sm.lc[k];
+                } else {
+                    int d;
+                    src = cand_to_index(k, sm.d, d);
+                    const int32_t cell = B.cell[src];
+                    const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
+                    if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
+                }
             }
             const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
             unsigned peers = 0;
             if (lc >= 0) {
                 peers = __match_any_sync(vm, lc);
                 const int pos = sm.wcur[warp][lc] + __popc(peers & lt);
-                if (pos < total) order[pos] = src;
-                else atomicOr(&S.ctl->err, ERR_CAPACITY);
+                if (pos >= total) atomicOr(&S.ctl->err, ERR_CAPACITY);
+                else if (staged) sm.idx[pos] = (int16_t)k;
+                else order[pos] = src;
             }
             __syncwarp();
             if (lc >= 0 && (peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
             __syncwarp();
         }
         __syncthreads();
-        // 4. per-cell sums
+        SLAB_PHASE_MARK(3);
+        // 4. per-cell sums (the staged data is then overwritten by them)
         {
             float acc[NQ][NSLOT];
 #pragma unroll
@@ -726,14 +948,16 @@ __global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
                 for (int s = 0; s < NSLOT; ++s) acc[q][s] = 0.f;
             const int nn = max(0, min(n_c, total - c0));
             const float g = S.g, hod = 0.5f * S.ood;
-            if (outs) cell_sums<true>(acc, order, c0, nn, B, li, lj, sm.dem, g, hod);
-            else cell_sums<false>(acc, order, c0, nn, B, li, lj, sm.dem, g, hod);
+            if (outs) cell_sums<true>(acc, staged, sm, order, c0, nn, B, li, lj, g, hod);
+            else cell_sums<false>(acc, staged, sm, order, c0, nn, B, li, lj, g, hod);
+            __syncthreads();
 #pragma unroll
             for (int q = 0; q < NQ; ++q)
 #pragma unroll
-                for (int s = 0; s < NSLOT; ++s) sm.part[q * NSLOT + s][tid] = acc[q][s];
+                for (int s = 0; s < NSLOT; ++s) sm.u.part[q * NSLOT + s][tid] = acc[q][s];
         }
         __syncthreads();
+        SLAB_PHASE_MARK(4);
         // 5. node sums over the cells that reach the node, (a, b) ascending
         float* P = sh.part + (size_t)w * PART_STRIDE;
         for (int k = tid; k < TN * TN; k += P2C_THREADS) {
@@ -750,15 +974,17 @@ __global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
                     const int cj = Bn - b;
                     if ((unsigned)cj >= TILE) continue;
 #pragma unroll
-                    for (int q = 0; q < NQ; ++q) v[q] += sm.part[q * NSLOT + a * 3 + b][ci * TILE + cj];
+                    for (int q = 0; q < NQ; ++q) v[q] += sm.u.part[q * NSLOT + a * 3 + b][ci * TILE + cj];
                 }
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) P[q * TN * TN + k] = v[q];
         }
         __syncthreads();
+        SLAB_PHASE_MARK(5);
+        SLAB_PHASE_TILE();
     }
-    close_grid_list(sh, sm.s_warp);
+    SLAB_PHASE_MARK(6);
 }
 
 // ------------------------------------------------------------ grid update
@@ -769,20 +995,27 @@ __global__ void __launch_bounds__(P2C_THREADS, 2) k_p2g_cell(Shared sh) {
 // h_max / v_max2 are updated in the node block; the FP64 grid mass sum is
 // the conservation diagnostic.
 __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
-    __shared__ int s_sid, s_loc, s_blk;
+    __shared__ int s_sid, s_gt, s_seq, s_blk;
     __shared__ int s_slot[4];
     __shared__ double s_red[NCELL / 32];
     __shared__ unsigned s_act[NCELL / 32];
     const int tid = threadIdx.x;
     const int li = tid / TILE, lj = tid % TILE;
-    const int nwork = sh.grid_pref[sh.nscn];
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        if (tid == 0) find_work(sh.grid_pref, sh.nscn, w, s_sid, s_loc);
+    int w0, w1;
+    work_range(sh.grid_pref[sh.nscn], w0, w1);
+    WorkCache wc;
+    for (int w = w0; w < w1; ++w) {
+        if (tid == 0) {
+            const int loc = cached_work(sh, sh.grid_pref, w, wc);
+            s_sid = wc.sid;
+            s_seq = wc.seq;
+            s_gt = sh.scn[wc.sid].gt_list[loc];
+        }
         __syncthreads();
         const Scn& S = sh.scn[s_sid];
         SCnt* n = S.cnt;
         Ctl* c = S.ctl;
-        const int gt = S.gt_list[s_loc];
+        const int gt = s_gt;
         const int gi = gt / sh.TY, gj = gt % sh.TY;
         if (tid < 4) {
             // contributor k: tile (gi - (k>>1), gj - (k&1)); slot if active this step
@@ -790,7 +1023,8 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
             int slot = -1;
             if (ti_ >= 0 && tj_ >= 0) {
                 const int tt = ti_ * sh.TY + tj_;
-                if (S.act_stamp[tt] == n->seq) slot = S.slot_of[tt];
+                const int st_ = S.act_stamp[tt], sl = S.slot_of[tt];  // both loads in flight together
+                if (st_ == s_seq) slot = sl;
             }
             s_slot[tid] = slot;
         } else if (tid == 32) {
@@ -910,6 +1144,8 @@ __device__ __forceinline__ int dir_of(int ib, int jb, int ti, int tj) {
     return (di + 1) * 3 + (dj + 1);
 }
 
+constexpr int G2P_MIN_BLOCKS = NCELL == 64 ? 12 : 3;
+
 struct G2PSmem {
     float4 nv[TN * TN];
     float4 dem[(TILE + 1) * (TILE + 1)];
@@ -927,11 +1163,13 @@ struct G2PSmem {
 // to a neighbour tile from the back, with per-direction counts. The block
 // max of |v|^2 and the particle bounding box feed the next step's dt and
 // remesh box (K5).
-__global__ void __launch_bounds__(NCELL, 3) k_g2p(Shared sh, const double* __restrict__ z64) {
+__global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const double* __restrict__ z64) {
     __shared__ G2PSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwork = sh.work_pref[sh.nscn];
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    int w0, w1;
+    work_range(nwork, w0, w1);
+    for (int w = w0; w < w1; ++w) {
         load_desc(sh.desc + w, &sm.d);
         if (tid < 9) sm.dcnt[tid] = 0;
         if (tid == 32) {
@@ -1107,14 +1345,14 @@ __global__ void __launch_bounds__(NCELL, 3) k_g2p(Shared sh, const double* __res
         }
         __syncthreads();
         if (tid < 9) {
-            int32_t* G = S.grp[nxt] + t * GRP_STRIDE;
+            int32_t* G = S.grp[nxt] + (size_t)t * GRP_STRIDE;
             const int cnt = tid == 4 ? sm.front : sm.dcnt[tid];
             G[3 + tid] = cnt;
             if (tid == 0) {
                 G[0] = base;
                 G[1] = base + sm.front;
                 G[2] = base + sm.front + sm.back;
-                S.grp_stamp[nxt][t] = seq + 1;
+                G[GRP_STAMP] = seq + 1;
                 if (sm.front + sm.back != total) atomicOr(&c->err, ERR_CAPACITY);
             }
             if (cnt) {

@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libslab_gpu.so")
+# SLAB_GPU_LIB selects another build of the library (e.g. an instrumented one)
+LIB_PATH = os.environ.get("SLAB_GPU_LIB") or os.path.join(HERE, "lib", "libslab_gpu.so")
 
 COULOMB, VOELLMY, MU_I = 0, 1, 2
 FRICTION_NAMES = {"COULOMB": COULOMB, "VOELLMY": VOELLMY, "MU_I": MU_I}
@@ -260,6 +261,8 @@ class Batch:
         L.slab_batch_download_max_box.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32), dp, dp, C.c_int64]
         L.slab_batch_work_counters.argtypes = [vp, C.POINTER(C.c_int64)]
         L.slab_batch_kernel_launches.argtypes = [vp]
+        L.slab_batch_set_profiling.argtypes = [vp, C.c_int32]
+        L.slab_batch_phase_times.argtypes = [vp, dp]
         L.slab_batch_kernel_launches.restype = C.c_int64
         L.slab_batch_last_error.argtypes = [vp]
         L.slab_batch_last_error.restype = C.c_char_p
@@ -344,6 +347,15 @@ class Batch:
 
     def kernel_launches(self) -> int:
         return self.L.slab_batch_kernel_launches(self.h)
+
+    def set_profiling(self, on: bool):
+        self._check(self.L.slab_batch_set_profiling(self.h, int(on)))
+
+    def phase_times(self):
+        """ms per kernel family since profiling was switched on: control, binning, P2G, grid, G2P."""
+        out = np.zeros(5)
+        self._check(self.L.slab_batch_phase_times(self.h, _dp(out)))
+        return out.tolist()
 
 
 class ServerConfig(C.Structure):
