@@ -90,7 +90,7 @@ struct StepGraphs {
 struct PhaseTimer {
     bool on = false;
     std::vector<cudaEvent_t> pool;
-    std::vector<std::array<int, 5>> pending;
+    std::vector<std::array<int, 6>> pending;
     size_t used = 0;
     double acc[5] = {0, 0, 0, 0, 0};
     int64_t steps = 0;
@@ -112,11 +112,14 @@ struct PhaseTimer {
         SLAB_CUDA(cudaEventRecord(pool[used], st));
         return (int)used++;
     }
-    // launches: 4 callables, one per kernel of the step
+    // the kernels of one step and the phase (out[] slot) each one counts to
+    int nk = 4;
+    int phase_of[5] = {0, 2, 3, 4, 0};
+    // launches: nk callables, one per kernel of the step
     void profiled_step(cudaStream_t st, const std::function<void(int)>& launch_kernel) {
-        std::array<int, 5> ev;
+        std::array<int, 6> ev{};
         ev[0] = mark(st);
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < nk; ++k) {
             launch_kernel(k);
             ev[k + 1] = mark(st);
         }
@@ -124,10 +127,9 @@ struct PhaseTimer {
     }
     void collect() {
         if (pending.empty()) return;
-        SLAB_CUDA(cudaEventSynchronize(pool[pending.back()[4]]));
-        static const int phase_of[4] = {1, 2, 3, 4};  // tile descriptors, P2G, grid update, G2P
+        SLAB_CUDA(cudaEventSynchronize(pool[pending.back()[nk]]));
         for (auto& ev : pending) {
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < nk; ++k) {
                 float ms = 0;
                 SLAB_CUDA(cudaEventElapsedTime(&ms, pool[ev[k]], pool[ev[k + 1]]));
                 acc[phase_of[k]] += ms;

@@ -22,7 +22,7 @@ class Engine32 {
         dptr<int32_t> cell[2], id[2], grp[2], act_list[2];
         dptr<float2> f[2], v[2];
         dptr<float> h[2], m[2], vz[2], z[2];
-        dptr<int32_t> act_stamp, slot_of, nxt_off, gt_stamp, gt_list, blk_of;
+        dptr<int32_t> act_stamp, slot_of, nxt_off, gt_stamp, blk_of;
         SCnt* cnt = nullptr;  // in the engine's counter array
     };
 
@@ -80,7 +80,7 @@ class Engine32 {
                                     bool with_v);
     dptr<float4> d_nv;
     dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz;
-    dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_grid_pref, d_free_blocks;
+    dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_gflat, d_free_blocks;
     dptr<Scn> d_scn;
     dptr<SCnt> d_cnt;
     std::vector<SCnt> h_cnt;

@@ -64,7 +64,6 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     d_blk_owner = dalloc<int32_t>(this->blk_cap);
     d_misc = dalloc<int32_t>(8);
     d_work_pref = dalloc<int32_t>(max_scn + 1);
-    d_grid_pref = dalloc<int32_t>(max_scn + 1);
     d_scn = dalloc<Scn>(max_scn);
     d_cnt = dalloc<SCnt>(max_scn);
     h_cnt.resize(max_scn);
@@ -75,7 +74,6 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaMemsetAsync(d_blk_stamp.get(), 0xff, (size_t)this->blk_cap * sizeof(int32_t), st));
     SLAB_CUDA(cudaMemsetAsync(d_misc.get(), 0, 8 * sizeof(int32_t), st));
     SLAB_CUDA(cudaMemsetAsync(d_work_pref.get(), 0, (max_scn + 1) * sizeof(int32_t), st));
-    SLAB_CUDA(cudaMemsetAsync(d_grid_pref.get(), 0, (max_scn + 1) * sizeof(int32_t), st));
     host_scn.resize(max_scn);
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
@@ -99,7 +97,12 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     grid_p2g = sms * std::max(occ_p, 1);
     grid_g2p = sms * std::max(occ_g, 1);
     grid_grid = sms * std::max(occ_u, 1);
-    grid_prep = sms * 8;  // one thread per active tile: room for ~300 k tiles in one sweep
+    int occ_d = 0;
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k32::k_prep, 256, 0));
+    grid_prep = sms * std::max(occ_d, 1);  // one resident wave, one thread per active tile
+    timer.nk = 5;  // k_prep, P2G, grid update, G2P, k_end
+    const int phase_map[5] = {1, 2, 3, 4, 0};
+    for (int k = 0; k < 5; ++k) timer.phase_of[k] = phase_map[k];
 }
 
 Engine32::~Engine32() {}
@@ -124,8 +127,9 @@ Shared Engine32::shared() const {
     sh.nscn = nscn;
     sh.scn = d_scn.get();
     sh.work_pref = d_work_pref.get();
-    sh.grid_pref = d_grid_pref.get();
-    sh.done = reinterpret_cast<uint32_t*>(d_misc.get() + 2);
+    sh.gflat = d_gflat.get();
+    sh.gcount = d_misc.get() + 6;
+    sh.gcap = 4 * work_cap;
     sh.desc = d_desc.get();
     sh.part = d_part.get();
     sh.work_cap = work_cap;
@@ -240,6 +244,7 @@ void Engine32::ensure_work_cap(int64_t need) {
     SLAB_CUDA(cudaStreamSynchronize(st));
     d_desc = dalloc<TileDesc>(cap);
     d_part = dalloc<float>((size_t)cap * PART_STRIDE);
+    d_gflat = dalloc<int32_t>((size_t)8 * cap);  // up to 4 grid tiles per active tile, 2 ints each
     work_cap = (int)cap;
     graphs.clear();
 }
@@ -289,7 +294,6 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     S.slot_of = dalloc<int32_t>(ntiles);
     S.nxt_off = dalloc<int32_t>(ntiles);
     S.gt_stamp = dalloc<int32_t>(ntiles);
-    S.gt_list = dalloc<int32_t>(ntiles);
     S.blk_of = dalloc<int32_t>(ntiles);
     S.cnt = d_cnt.get() + sid;
     ensure_work_cap(work_cap_total + S.act_cap);
@@ -436,7 +440,6 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     D.slot_of = S.slot_of.get();
     D.nxt_off = S.nxt_off.get();
     D.gt_stamp = S.gt_stamp.get();
-    D.gt_list = S.gt_list.get();
     D.blk_of = S.blk_of.get();
     D.act_cap = S.act_cap;
     h2d(d_scn.get() + sid, &D, 1, st);
@@ -482,6 +485,7 @@ void Engine32::launch_kernel(int k, const Shared& sh) {
         case 1: launch_p2g(sh); break;
         case 2: k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh); break;
         case 3: k32::k_g2p<<<grid_g2p, NCELL, 0, st>>>(sh, T.z.get()); break;
+        case 4: k32::k_end<<<1, 1024, 0, st>>>(sh); break;
     }
 }
 
@@ -493,7 +497,7 @@ void Engine32::arm(int64_t steps_left, int stop_at_frame) {
 
 void Engine32::launch_step() {
     const Shared sh = shared();
-    for (int k = 0; k < 4; ++k) launch_kernel(k, sh);
+    for (int k = 0; k < 5; ++k) launch_kernel(k, sh);
 }
 
 void Engine32::enqueue_steps(int chunk) {
@@ -508,7 +512,7 @@ void Engine32::enqueue_steps(int chunk) {
     } else {
         graphs.launch(chunk, st, [&] { launch_step(); });
     }
-    nlaunch += 4 * (int64_t)chunk;
+    nlaunch += 5 * (int64_t)chunk;
 }
 
 SCnt Engine32::counters(int sid) {

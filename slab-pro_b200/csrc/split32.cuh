@@ -57,7 +57,6 @@ struct PBuf {
 // Per-scenario counters (device).
 struct SCnt {
     int32_t act_count[2];  // active tiles of the list of each parity
-    int32_t gt_count;      // grid tiles of the running step
     int32_t cursor;        // particles placed in the next buffer
     int32_t seq;           // completed G2P passes (buffer parity = seq & 1)
     int32_t stepid;        // P2G passes so far (stamps grid tiles / blocks)
@@ -105,7 +104,6 @@ struct Scn {
     int32_t* slot_of;       // [ntiles] work index (partial slot) of the tile in the running step
     int32_t* nxt_off;       // [ntiles] start of the tile's segment in the next buffer
     int32_t* gt_stamp;      // [ntiles] stepid at which the tile joined the grid list
-    int32_t* gt_list;       // grid tiles of the running step
     int32_t* blk_of;        // [ntiles] node block of the tile, -1 if none yet
     int32_t act_cap;
     int32_t pad_;
@@ -129,8 +127,10 @@ struct Shared {
     int32_t nscn;
     const Scn* scn;
     int32_t* work_pref;   // [nscn+1] prefix of active tiles (P2G / G2P work)
-    int32_t* grid_pref;   // [nscn+1] prefix of grid tiles
-    uint32_t* done;       // last-block-done counters [2]
+    int32_t* gflat;       // [gcap][2] grid tiles of the running step: (scenario, grid tile)
+    int32_t* gcount;      // entries in gflat
+    int32_t gcap;
+    int32_t pad2_;
     TileDesc* desc;       // [work_cap] descriptors of the running step
     float* part;          // [work_cap][PART_STRIDE] P2G partial sums
     int32_t work_cap;

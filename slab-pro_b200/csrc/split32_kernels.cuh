@@ -1,22 +1,25 @@
-// Kernels of the FP32 split-precision step loop (K1-K6), shared by the
+// Kernels of the FP32 split-precision step loop, shared by the
 // single-scenario path and the batched / served paths. One step is
-//   (begin)            per-scenario dt / stop rules, work-list prefix: run by
-//                      the last CTA of the previous step's k_g2p, or by
-//                      k_arm_begin at the start of an advance call
-//   k_prep   (grid)    one thread per active tile: where its particles are,
-//                      its segment in the next buffer, grid-tile list
-//   k_p2g    (grid)    one CTA per active tile: P2G partial sums
+//   k_prep   (grid)    one thread per active tile: its 9 candidate ranges,
+//                      its segment in the next buffer, its grid tiles on the
+//                      flat grid-tile list
+//   k_p2g_*  (grid)    one CTA (or warp) per active tile: P2G partial sums
 //   k_grid   (grid)    one CTA per grid tile: grid update + friction
 //   k_g2p    (grid)    one CTA per active tile: G2P, advection, regrouping
-// The CTAs stride over a flat list of work items of all scenarios, so one
-// launch advances every running scenario by one step, each with its own dt
-// and friction law.
+//   k_end    (1 CTA)   per scenario: end of the step, then the next step's
+//                      dt / stop rules and work-list prefix (k_arm_begin does
+//                      the same at the start of an advance call)
+// The CTAs take contiguous runs of a flat list of work items of all
+// scenarios, so one launch advances every running scenario by one step, each
+// with its own dt and friction law.
 //
-// Every result is independent of the order of the particles inside a tile:
-// P2G adds fixed-point integers (exact, associative), the grid update adds
-// the partials of a node's tiles in a fixed order, and everything else is
-// per particle or a max/min. So placement can use atomics freely and the
-// step is still bitwise reproducible, alone or inside a batch.
+// Every result is independent of the timing of the threads: the default P2G
+// sorts a tile's particles by cell in a stable, data-determined order and
+// sums in that order (the fixed-point variants add integers, exact and
+// associative); the grid update adds the partials of a node's tiles in a
+// fixed order; G2P places particles by block prefix sums in candidate order;
+// everything else is per particle or a max/min. So a step is bitwise
+// reproducible, alone or inside a batch.
 #pragma once
 
 #include "split32.cuh"
@@ -135,7 +138,6 @@ __device__ void begin_scenarios(const Shared& sh, int t0_pass) {
             if (c->active) {
                 n->stepid += 1;
                 n->act_count[(n->seq + 1) & 1] = 0;
-                n->gt_count = 0;
                 n->cursor = 0;
                 n->grid_mass = 0.0;
                 n->outs = c->write_outputs;
@@ -155,8 +157,7 @@ __device__ void begin_scenarios(const Shared& sh, int t0_pass) {
     if (tid == 0) {
         sh.work_pref[sh.nscn] = min(total, sh.work_cap);
         if (total > sh.work_cap) atomicOr(&sh.scn[0].ctl->err, ERR_CAPACITY);
-        sh.done[0] = 0;
-        sh.done[1] = 0;
+        *sh.gcount = 0;
     }
 }
 
@@ -176,32 +177,6 @@ __global__ void k_arm_begin(Shared sh, int64_t steps_left, int stop_at_frame) {
     begin_scenarios(sh, 0);
 }
 
-// After the last CTA of a launch has listed its grid tiles: the prefix of
-// grid tiles over scenarios (the work list of k_grid). Call with the whole
-// CTA; s_warp needs 33 ints.
-__device__ void close_grid_list(const Shared& sh, int* s_warp) {
-    __shared__ int s_last, s_tot;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = (atomicAdd(&sh.done[0], 1u) == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    int total = 0;
-    for (int base = 0; base < sh.nscn; base += blockDim.x) {
-        const int s = base + threadIdx.x;
-        const int cnt = (s < sh.nscn && sh.scn[s].ctl->active) ? *(volatile int*)&sh.scn[s].cnt->gt_count : 0;
-        const int ex = block_exclusive_scan(cnt, s_warp);
-        if (s < sh.nscn) sh.grid_pref[s] = total + ex;
-        if (threadIdx.x == blockDim.x - 1) s_tot = ex + cnt;
-        __syncthreads();
-        total += s_tot;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) sh.grid_pref[sh.nscn] = total;
-}
 
 // K1 (bookkeeping half): one thread per active tile t. Its particles are
 // the stayers of its own segment in the current buffer plus the movers of
@@ -270,13 +245,18 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (old[k] < stamp) gl[ng++] = (ti + (k >> 1)) * sh.TY + (tj + (k & 1));
-        const int at = warp_atomic_add(&n->gt_count, ng, vmask);
-        for (int k = 0; k < ng; ++k) S.gt_list[at + k] = gl[k];
+        const int at = warp_atomic_add(sh.gcount, ng, vmask);
+        for (int k = 0; k < ng; ++k) {
+            if (at + k < sh.gcap) {
+                sh.gflat[2 * (at + k)] = sid;
+                sh.gflat[2 * (at + k) + 1] = gl[k];
+            } else {
+                atomicOr(&S.ctl->err, ERR_CAPACITY);
+            }
+        }
         sh.desc[w] = D;
     }
-    // the last CTA builds the grid-tile work list prefix for k_grid
-    __shared__ int s_warp[33];
-    close_grid_list(sh, s_warp);
+
 }
 
 // ------------------------------------------------------------------- P2G
@@ -1002,14 +982,18 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
     const int tid = threadIdx.x;
     const int li = tid / TILE, lj = tid % TILE;
     int w0, w1;
-    work_range(sh.grid_pref[sh.nscn], w0, w1);
-    WorkCache wc;
+    work_range(min(*sh.gcount, sh.gcap), w0, w1);
+    int csid = -1, cseq = 0;  // scenario of the last item and its step (thread 0)
     for (int w = w0; w < w1; ++w) {
         if (tid == 0) {
-            const int loc = cached_work(sh, sh.grid_pref, w, wc);
-            s_sid = wc.sid;
-            s_seq = wc.seq;
-            s_gt = sh.scn[wc.sid].gt_list[loc];
+            const int2 e = reinterpret_cast<const int2*>(sh.gflat)[w];
+            if (e.x != csid) {
+                csid = e.x;
+                cseq = sh.scn[csid].cnt->seq;
+            }
+            s_sid = e.x;
+            s_seq = cseq;
+            s_gt = e.y;
         }
         __syncthreads();
         const Scn& S = sh.scn[s_sid];
@@ -1394,28 +1378,24 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         }
         __syncthreads();
     }
-    // the last CTA closes the step of every running scenario
-    __shared__ int s_last;
-    if (tid == 0) {
-        __threadfence();
-        s_last = (atomicAdd(&sh.done[1], 1u) == gridDim.x - 1);
+}
+
+// K5: end of the step for every running scenario (the per-step reductions
+// of G2P into dt, time and the remesh box), then the next step's dt, stop
+// rules and work list. One CTA, after G2P.
+__global__ void k_end(Shared sh) {
+    for (int s = threadIdx.x; s < sh.nscn; s += blockDim.x) {
+        const Scn& S = sh.scn[s];
+        Ctl* c = S.ctl;
+        if (!c->active) continue;
+        SCnt* n = S.cnt;
+        if (n->cursor != S.Np) atomicOr(&c->err, ERR_CAPACITY);
+        ctl_end(c);
+        n->seq += 1;
+        n->vz_valid = n->outs;
     }
     __syncthreads();
-    if (s_last) {
-        __threadfence();
-        for (int s = tid; s < sh.nscn; s += blockDim.x) {
-            const Scn& S = sh.scn[s];
-            Ctl* c = S.ctl;
-            if (!c->active) continue;
-            SCnt* n = S.cnt;
-            if (*(volatile int*)&n->cursor != S.Np) atomicOr(&c->err, ERR_CAPACITY);
-            ctl_end(c);
-            n->seq += 1;
-            n->vz_valid = n->outs;
-        }
-        __syncthreads();
-        begin_scenarios(sh, 0);  // the next step's dt, stop rules and work list
-    }
+    begin_scenarios(sh, 0);
 }
 
 // Particle z and vz at the current positions (for downloads between output
