@@ -16,6 +16,8 @@ class Engine32 {
     struct Store {
         int Np = 0;
         int act_cap = 0;
+        int Np_alloc = 0;   // particle buffer length
+        int act_alloc = 0;  // tile list length
         Ctl* ctl = nullptr;
         Ctl* h_ctl = nullptr;
         double mass_fp64 = 0;
@@ -38,7 +40,8 @@ class Engine32 {
     void launch_kernel(int k, const Shared& sh);
     void launch_p2g(const Shared& sh);
     void arm(int64_t steps_left, int stop_at_frame);
-    int acc_mode = 3;  // P2G scheme (k32::ACC_*): cell-sorted FP32 sums by default
+    int acc_mode = 5;  // P2G scheme (k32::ACC_*): dense tiles cell-sorted, sparse tiles fixed point
+    int split_min = 3 * NCELL / 4;  // ACC_MIXED: tiles with more particles take the cell-sorted P2G (measured)
     void enqueue_steps(int chunk);
     PhaseTimer timer;
     SCnt counters(int sid);
@@ -66,12 +69,20 @@ class Engine32 {
     int TX = 0, TY = 0, ntiles = 0;
     int blk_cap = 0;
     int64_t pending_blocks = 0;  // node blocks of scenarios added since the last t=0 pass (an estimate)
-    int grid_p2g = 0, grid_g2p = 0, grid_grid = 0, grid_prep = 0;
+    int grid_p2g = 0, grid_p2g_cell = 0, grid_p2g_hilo = 0, grid_g2p = 0, grid_grid = 0, grid_prep = 0;
     int work_cap = 0;
     int64_t work_cap_total = 0;
     void ensure_work_cap(int64_t need);
     int64_t nlaunch = 0;
     std::vector<std::unique_ptr<Store>> slots;  // scenario slots; empty after retire
+    std::vector<std::unique_ptr<Store>> spare;  // a retired slot's arrays, for its next scenario
+    dptr<int32_t> d_collect;                    // [ntiles + 8]: node blocks of one scenario, count and box
+    dptr<float> d_gather;                       // node-field downloads
+    size_t gather_cap = 0;
+    dptr<const float*> d_gather_fp;
+    // node blocks of scenario sid: their ids into d_collect[8...], count and
+    // tile box {ti0, ti1, tj0, tj1} to the host; returns the count
+    int collect_blocks(int sid, int tbox[4]);
     std::vector<int> free_slots;
     std::vector<Scn> host_scn;
 
@@ -80,7 +91,7 @@ class Engine32 {
                                     bool with_v);
     dptr<float4> d_nv;
     dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz;
-    dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_gflat, d_free_blocks;
+    dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_gflat, d_wlist, d_free_blocks;
     dptr<Scn> d_scn;
     dptr<SCnt> d_cnt;
     std::vector<SCnt> h_cnt;

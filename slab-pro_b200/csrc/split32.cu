@@ -68,6 +68,8 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     d_cnt = dalloc<SCnt>(max_scn);
     h_cnt.resize(max_scn);
     slots.resize(max_scn);
+    spare.resize(max_scn);
+    d_collect = dalloc<int32_t>((size_t)ntiles + 8);
     d_free_blocks = dalloc<int32_t>(this->blk_cap);
     SLAB_CUDA(cudaMemsetAsync(d_hmax.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
     SLAB_CUDA(cudaMemsetAsync(d_vmax2.get(), 0, (size_t)this->blk_cap * NCELL * sizeof(float), st));
@@ -82,19 +84,20 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(k32::P2W_WARPS * sizeof(k32::P2WWarp))));
     if (const char* e = std::getenv("SLAB_P2G_ACC")) acc_mode = std::atoi(e);
+    if (const char* e = std::getenv("SLAB_P2G_SPLIT")) split_min = std::atoi(e);
     int dev = 0, sms = 0, occ_p = 0, occ_g = 0, occ_u = 0;
     SLAB_CUDA(cudaGetDevice(&dev));
     SLAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    if (acc_mode == k32::ACC_WARP)
-        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g_warp, k32::P2W_THREADS,
-                                                                k32::P2W_WARPS * sizeof(k32::P2WWarp)));
-    else if (acc_mode == k32::ACC_CELL)
-        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem)));
-    else
-        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g<k32::ACC_HILO>, k32::P2G_THREADS, sizeof(k32::P2GSmem)));
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g_warp, k32::P2W_THREADS,
+                                                            k32::P2W_WARPS * sizeof(k32::P2WWarp)));
+    int occ_c = 0, occ_h = 0;
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k32::k_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem)));
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k32::k_p2g<k32::ACC_HILO>, k32::P2G_THREADS, sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, k32::k_g2p, NCELL, 0));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k32::k_grid, NCELL, 0));
     grid_p2g = sms * std::max(occ_p, 1);
+    grid_p2g_cell = sms * std::max(occ_c, 1);
+    grid_p2g_hilo = sms * std::max(occ_h, 1);
     grid_g2p = sms * std::max(occ_g, 1);
     grid_grid = sms * std::max(occ_u, 1);
     int occ_d = 0;
@@ -127,6 +130,9 @@ Shared Engine32::shared() const {
     sh.nscn = nscn;
     sh.scn = d_scn.get();
     sh.work_pref = d_work_pref.get();
+    sh.wlist = d_wlist.get();
+    sh.wcount = d_misc.get() + 2;
+    sh.split_min = acc_mode == k32::ACC_MIXED ? split_min : -1;
     sh.gflat = d_gflat.get();
     sh.gcount = d_misc.get() + 6;
     sh.gcap = 4 * work_cap;
@@ -150,6 +156,28 @@ __global__ void k_scatter_tiles(const int32_t* __restrict__ tiles, const int32_t
     act_stamp[t] = 0;
 }
 
+// node blocks of one scenario: ids into out[8...], count into out[0], tile
+// box {ti0, ti1, tj0, tj1} into out[1..4] (out[0..4] preset to 0, big, -1, big, -1)
+__global__ void k_collect_blocks(const int32_t* __restrict__ blk_of, int ntiles, int TY, int32_t* out) {
+    const int lane = threadIdx.x & 31;
+    for (int t0 = blockIdx.x * blockDim.x; t0 < ntiles; t0 += gridDim.x * blockDim.x) {
+        const int t = t0 + threadIdx.x;
+        const int b = t < ntiles ? blk_of[t] : -1;
+        const unsigned m = __ballot_sync(0xffffffffu, b >= 0);
+        if (!m) continue;
+        int base = 0;
+        if (lane == __ffs(m) - 1) base = atomicAdd(out, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+        if (b >= 0) {
+            out[8 + base + __popc(m & ((1u << lane) - 1u))] = b;
+            atomicMin(out + 1, t / TY);
+            atomicMax(out + 2, t / TY);
+            atomicMin(out + 3, t % TY);
+            atomicMax(out + 4, t % TY);
+        }
+    }
+}
+
 __global__ void k_release_blocks(const int32_t* ids, int n, float* hmax, float* vmax2, int32_t* stamp, int32_t* owner) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)n * NCELL; k += (int64_t)gridDim.x * blockDim.x) {
         const int b = ids[k / NCELL];
@@ -167,24 +195,18 @@ __global__ void k_release_blocks(const int32_t* ids, int n, float* hmax, float* 
 void Engine32::retire(int sid, const Ctl& empty_ctl) {
     if (sid < 0 || sid >= nscn || !slots[sid]) throw Error{SLAB_E_NOTFOUND, "no scenario in this slot"};
     Store& S = *slots[sid];
-    SLAB_CUDA(cudaStreamSynchronize(st));
-    std::vector<int32_t> blk_of(ntiles);
-    d2h(blk_of.data(), S.blk_of.get(), ntiles, st);
-    int32_t free_count = 0;
-    d2h(&free_count, d_misc.get() + 4, 1, st);
-    SLAB_CUDA(cudaStreamSynchronize(st));
-    std::vector<int32_t> ids;
-    for (int32_t b : blk_of)
-        if (b >= 0) ids.push_back(b);
-    if (!ids.empty()) {
-        dptr<int32_t> d_ids = dalloc<int32_t>(ids.size());
-        h2d(d_ids.get(), ids.data(), ids.size(), st);
-        const int blocks = (int)std::min<int64_t>(((int64_t)ids.size() * NCELL + 255) / 256, 148 * 8);
-        k32::k_release_blocks<<<blocks, 256, 0, st>>>(d_ids.get(), (int)ids.size(), d_hmax.get(), d_vmax2.get(), d_blk_stamp.get(),
-                                                      d_blk_owner.get());
+    int tb[4];
+    const int nblk = collect_blocks(sid, tb);  // ids in d_collect[8...], on the device
+    if (nblk > 0) {
+        int32_t free_count = 0;
+        d2h(&free_count, d_misc.get() + 4, 1, st);
+        SLAB_CUDA(cudaStreamSynchronize(st));
+        const int32_t* ids = d_collect.get() + 8;
+        const int blocks = (int)std::min<int64_t>(((int64_t)nblk * NCELL + 255) / 256, 148 * 8);
+        k32::k_release_blocks<<<blocks, 256, 0, st>>>(ids, nblk, d_hmax.get(), d_vmax2.get(), d_blk_stamp.get(), d_blk_owner.get());
         SLAB_CUDA(cudaGetLastError());
-        SLAB_CUDA(cudaMemcpyAsync(d_free_blocks.get() + free_count, d_ids.get(), ids.size() * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-        const int32_t nf = free_count + (int32_t)ids.size();
+        SLAB_CUDA(cudaMemcpyAsync(d_free_blocks.get() + free_count, ids, (size_t)nblk * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+        const int32_t nf = free_count + nblk;
         h2d(d_misc.get() + 4, &nf, 1, st);
         SLAB_CUDA(cudaStreamSynchronize(st));
     }
@@ -199,32 +221,35 @@ void Engine32::retire(int sid, const Ctl& empty_ctl) {
     host_scn[sid] = D;
     work_cap_total -= S.act_cap;
     SLAB_CUDA(cudaStreamSynchronize(st));
-    slots[sid].reset();
+    spare[sid] = std::move(slots[sid]);
     free_slots.push_back(sid);
 }
 
-void Engine32::box_of_blocks(int sid, int box[4]) {
+int Engine32::collect_blocks(int sid, int tbox[4]) {
     Store& S = *slots[sid];
-    std::vector<int32_t> blk_of(ntiles);
-    d2h(blk_of.data(), S.blk_of.get(), ntiles, st);
+    const int32_t init[5] = {0, INT32_MAX, -1, INT32_MAX, -1};
+    h2d(d_collect.get(), init, 5, st);
+    const int blocks = (int)std::min<int64_t>(((int64_t)ntiles + 255) / 256, 148 * 8);
+    k32::k_collect_blocks<<<blocks, 256, 0, st>>>(S.blk_of.get(), ntiles, TY, d_collect.get());
+    SLAB_CUDA(cudaGetLastError());
+    int32_t res[5];
+    d2h(res, d_collect.get(), 5, st);
     SLAB_CUDA(cudaStreamSynchronize(st));
-    int ti0 = TX, ti1 = -1, tj0 = TY, tj1 = -1;
-    for (int t = 0; t < ntiles; ++t)
-        if (blk_of[t] >= 0) {
-            ti0 = std::min(ti0, t / TY);
-            ti1 = std::max(ti1, t / TY);
-            tj0 = std::min(tj0, t % TY);
-            tj1 = std::max(tj1, t % TY);
-        }
-    if (ti1 < 0) {
+    for (int k = 0; k < 4; ++k) tbox[k] = res[1 + k];
+    return res[0];
+}
+
+void Engine32::box_of_blocks(int sid, int box[4]) {
+    int tb[4];
+    if (collect_blocks(sid, tb) == 0) {
         box[0] = box[2] = 0;
         box[1] = box[3] = -1;
         return;
     }
-    box[0] = ti0 * TILE;
-    box[1] = std::min(T.Nx - 1, ti1 * TILE + TILE - 1);
-    box[2] = tj0 * TILE;
-    box[3] = std::min(T.Ny - 1, tj1 * TILE + TILE - 1);
+    box[0] = tb[0] * TILE;
+    box[1] = std::min(T.Nx - 1, tb[1] * TILE + TILE - 1);
+    box[2] = tb[2] * TILE;
+    box[3] = std::min(T.Ny - 1, tb[3] * TILE + TILE - 1);
 }
 
 void Engine32::download_max_box(int sid, const int box[4], double* hmax, double* vmax2) {
@@ -245,6 +270,7 @@ void Engine32::ensure_work_cap(int64_t need) {
     d_desc = dalloc<TileDesc>(cap);
     d_part = dalloc<float>((size_t)cap * PART_STRIDE);
     d_gflat = dalloc<int32_t>((size_t)8 * cap);  // up to 4 grid tiles per active tile, 2 ints each
+    d_wlist = dalloc<int32_t>((size_t)2 * cap);
     work_cap = (int)cap;
     graphs.clear();
 }
@@ -270,7 +296,11 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
         if (nscn >= max_scn) throw Error{SLAB_E_OOM, "scenario capacity exceeded"};
         sid = nscn;
     }
-    slots[sid].reset(new Store());
+    // a retired scenario's arrays stay with its slot and are reused: the
+    // terrain-sized tile arrays always, particle buffers and tile lists when
+    // large enough (admission then allocates nothing in the common case)
+    if (spare[sid]) slots[sid] = std::move(spare[sid]);
+    else slots[sid].reset(new Store());
     Store& S = *slots[sid];
     S.Np = Np;
     S.ctl = ctl;
@@ -278,23 +308,31 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     // a single scenario gets the safe bound; in a batch the lists start at an
     // estimate (>= 4 particles per active tile) and grow between chunks
     S.act_cap = batch ? std::max(1, std::min(ntiles, Np / 4 + 256)) : std::max(1, std::min(ntiles, Np));
+    const bool new_parts = S.Np_alloc < Np, new_lists = S.act_alloc < S.act_cap, new_tiles = !S.blk_of;
     for (int b = 0; b < 2; ++b) {
-        S.cell[b] = dalloc<int32_t>(Np);
-        S.f[b] = dalloc<float2>(Np);
-        S.v[b] = dalloc<float2>(Np);
-        S.h[b] = dalloc<float>(Np);
-        S.m[b] = dalloc<float>(Np);
-        S.id[b] = dalloc<int32_t>(Np);
-        S.vz[b] = dalloc<float>(Np);
-        S.z[b] = dalloc<float>(Np);
-        S.grp[b] = dalloc<int32_t>((size_t)ntiles * GRP_STRIDE);
-        S.act_list[b] = dalloc<int32_t>(S.act_cap);
+        if (new_parts) {
+            S.cell[b] = dalloc<int32_t>(Np);
+            S.f[b] = dalloc<float2>(Np);
+            S.v[b] = dalloc<float2>(Np);
+            S.h[b] = dalloc<float>(Np);
+            S.m[b] = dalloc<float>(Np);
+            S.id[b] = dalloc<int32_t>(Np);
+            S.vz[b] = dalloc<float>(Np);
+            S.z[b] = dalloc<float>(Np);
+        }
+        if (new_tiles) S.grp[b] = dalloc<int32_t>((size_t)ntiles * GRP_STRIDE);
+        if (new_lists) S.act_list[b] = dalloc<int32_t>(S.act_cap);
     }
-    S.act_stamp = dalloc<int32_t>(ntiles);
-    S.slot_of = dalloc<int32_t>(ntiles);
-    S.nxt_off = dalloc<int32_t>(ntiles);
-    S.gt_stamp = dalloc<int32_t>(ntiles);
-    S.blk_of = dalloc<int32_t>(ntiles);
+    if (new_parts) S.Np_alloc = Np;
+    if (new_lists) S.act_alloc = S.act_cap;
+    else S.act_cap = S.act_alloc;  // a reused list keeps its full length
+    if (new_tiles) {
+        S.act_stamp = dalloc<int32_t>(ntiles);
+        S.slot_of = dalloc<int32_t>(ntiles);
+        S.nxt_off = dalloc<int32_t>(ntiles);
+        S.gt_stamp = dalloc<int32_t>(ntiles);
+        S.blk_of = dalloc<int32_t>(ntiles);
+    }
     S.cnt = d_cnt.get() + sid;
     ensure_work_cap(work_cap_total + S.act_cap);
     work_cap_total += S.act_cap;
@@ -462,21 +500,25 @@ void Engine32::launch_t0() {
     launch_p2g(sh);
     k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
     SLAB_CUDA(cudaGetLastError());
-    nlaunch += 4;
+    nlaunch += acc_mode == k32::ACC_MIXED ? 5 : 4;
     pending_blocks = 0;  // later reads of the pool count see these blocks
 }
 
 void Engine32::launch_p2g(const Shared& sh) {
-    if (acc_mode == k32::ACC_WARP)
+    if (acc_mode == k32::ACC_MIXED) {  // dense tiles, then sparse tiles
+        k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, 0);
+        k32::k_p2g<k32::ACC_HILO><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, 1);
+    } else if (acc_mode == k32::ACC_WARP) {
         k32::k_p2g_warp<<<grid_p2g, k32::P2W_THREADS, k32::P2W_WARPS * sizeof(k32::P2WWarp), st>>>(sh);
-    else if (acc_mode == k32::ACC_CELL)
-        k32::k_p2g_cell<<<grid_p2g, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh);
-    else if (acc_mode == k32::ACC_I32)
-        k32::k_p2g<k32::ACC_I32><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
-    else if (acc_mode == k32::ACC_I64)
-        k32::k_p2g<k32::ACC_I64><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
-    else
-        k32::k_p2g<k32::ACC_HILO><<<grid_p2g, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh);
+    } else if (acc_mode == k32::ACC_CELL) {
+        k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, -1);
+    } else if (acc_mode == k32::ACC_I32) {
+        k32::k_p2g<k32::ACC_I32><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, -1);
+    } else if (acc_mode == k32::ACC_I64) {
+        k32::k_p2g<k32::ACC_I64><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, -1);
+    } else {
+        k32::k_p2g<k32::ACC_HILO><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, -1);
+    }
 }
 
 void Engine32::launch_kernel(int k, const Shared& sh) {
@@ -512,7 +554,7 @@ void Engine32::enqueue_steps(int chunk) {
     } else {
         graphs.launch(chunk, st, [&] { launch_step(); });
     }
-    nlaunch += 5 * (int64_t)chunk;
+    nlaunch += (acc_mode == k32::ACC_MIXED ? 6 : 5) * (int64_t)chunk;
 }
 
 SCnt Engine32::counters(int sid) {
@@ -543,6 +585,7 @@ bool Engine32::check_capacity() {
             }
             work_cap_total += cap - S.act_cap;
             S.act_cap = cap;
+            S.act_alloc = cap;
             host_scn[s].act_cap = cap;
             h2d(d_scn.get() + s, &host_scn[s], 1, st);
             grew = true;
@@ -628,14 +671,19 @@ std::vector<float> Engine32::gather_nodes(int sid, int stepid, int i0, int j0, i
     const int nout = (int)fields.size() + (with_v ? 2 : 0);
     std::vector<float> host((size_t)nout * total);
     if (total == 0) return host;
-    dptr<float> buf = dalloc<float>((size_t)nout * total);
-    dptr<const float*> fp = dalloc<const float*>(std::max<size_t>(1, fields.size()));
-    h2d(fp.get(), fields.data(), fields.size(), st);
+    // scratch kept between calls (downloads at every retirement must not allocate)
+    if ((size_t)nout * total > gather_cap) {
+        d_gather = dalloc<float>((size_t)nout * total);
+        gather_cap = (size_t)nout * total;
+    }
+    if (!d_gather_fp) d_gather_fp = dalloc<const float*>(8);
+    if (fields.size() > 8) throw Error{SLAB_E_ARG, "too many fields"};
+    h2d(d_gather_fp.get(), fields.data(), fields.size(), st);
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
-    k32::k_gather_nodes<<<blocks, 256, 0, st>>>(S.blk_of.get(), d_blk_stamp.get(), stepid, TY, i0, j0, nI, nJ, (int)fields.size(), fp.get(),
-                                                with_v ? d_nv.get() : nullptr, buf.get());
+    k32::k_gather_nodes<<<blocks, 256, 0, st>>>(S.blk_of.get(), d_blk_stamp.get(), stepid, TY, i0, j0, nI, nJ, (int)fields.size(),
+                                                d_gather_fp.get(), with_v ? d_nv.get() : nullptr, d_gather.get());
     SLAB_CUDA(cudaGetLastError());
-    d2h(host.data(), buf.get(), host.size(), st);
+    d2h(host.data(), d_gather.get(), host.size(), st);
     SLAB_CUDA(cudaStreamSynchronize(st));
     return host;
 }

@@ -127,6 +127,10 @@ struct Shared {
     int32_t nscn;
     const Scn* scn;
     int32_t* work_pref;   // [nscn+1] prefix of active tiles (P2G / G2P work)
+    int32_t* wlist;       // [2][work_cap] work items of the two P2G kernels: dense tiles, then sparse ones
+    int32_t* wcount;      // [2] their counts
+    int32_t split_min;    // tiles with more particles go to the dense kernel; < 0: one P2G kernel for all
+    int32_t pad3_;
     int32_t* gflat;       // [gcap][2] grid tiles of the running step: (scenario, grid tile)
     int32_t* gcount;      // entries in gflat
     int32_t gcap;

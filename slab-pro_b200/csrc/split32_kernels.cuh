@@ -158,6 +158,8 @@ __device__ void begin_scenarios(const Shared& sh, int t0_pass) {
         sh.work_pref[sh.nscn] = min(total, sh.work_cap);
         if (total > sh.work_cap) atomicOr(&sh.scn[0].ctl->err, ERR_CAPACITY);
         *sh.gcount = 0;
+        sh.wcount[0] = 0;
+        sh.wcount[1] = 0;
     }
 }
 
@@ -177,6 +179,27 @@ __global__ void k_arm_begin(Shared sh, int64_t steps_left, int stop_at_frame) {
     begin_scenarios(sh, 0);
 }
 
+
+// The work items of one CTA: a contiguous range of the flat work list, so
+// that consecutive items mostly belong to the same scenario.
+__device__ __forceinline__ void work_range(int nwork, int& w0, int& w1) {
+    const int per = (nwork + (int)gridDim.x - 1) / (int)gridDim.x;
+    w0 = min((int)blockIdx.x * per, nwork);
+    w1 = min(w0 + per, nwork);
+}
+
+// Scenario of the last work item looked up, with the step fields that do not
+// change during a launch (so a new item of the same scenario costs no loads).
+struct WorkCache {
+    int sid = -1, lo = 0, hi = 0, seq = 0, stepid = 0;
+};
+
+// Work items of a P2G kernel: class 0 (dense tiles), 1 (sparse tiles), or
+// -1 (every active tile, when the step runs one P2G kernel).
+__device__ __forceinline__ int p2g_count(const Shared& sh, int cls) {
+    return cls < 0 ? sh.work_pref[sh.nscn] : min(sh.wcount[cls], sh.work_cap);
+}
+__device__ __forceinline__ int p2g_item(const Shared& sh, int cls, int i) { return cls < 0 ? i : sh.wlist[cls * sh.work_cap + i]; }
 
 // K1 (bookkeeping half): one thread per active tile t. Its particles are
 // the stayers of its own segment in the current buffer plus the movers of
@@ -232,6 +255,11 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
         D.rpref[9] = acc;
         D.total = cnt;
         D.nxt_off = warp_atomic_add(&n->cursor, cnt, vmask);
+        if (sh.split_min >= 0) {  // dense tiles to the cell-sorted P2G, sparse ones to the fixed-point P2G
+            const int cls = cnt > sh.split_min ? 0 : 1;
+            const int at = warp_atomic_add(sh.wcount + cls, 1, vmask);
+            if (at < sh.work_cap) sh.wlist[cls * sh.work_cap + at] = w;
+        }
         D.pad_ = 0;
         S.slot_of[t] = w;
         const int stamp = n->stepid;
@@ -261,7 +289,8 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
 
 // ------------------------------------------------------------------- P2G
 
-constexpr int P2G_THREADS = 256;
+constexpr int P2G_THREADS = NCELL;  // one thread per cell slot; the CTA strides over its tile's particles
+constexpr int P2G_MIN_BLOCKS = NCELL == 64 ? 16 : 4;
 
 // Fixed-point accumulation schemes of k_p2g:
 //  ACC_I32   one int32 per sum, 2^-30 of the tile's bound
@@ -271,7 +300,10 @@ constexpr int P2G_THREADS = 256;
 //  ACC_I64   one int64 per sum at 2^-52 of the bound
 //  ACC_CELL  no fixed point: k_p2g_cell, FP32 sums over cell-sorted particles
 //  ACC_WARP  k_p2g_warp: ACC_HILO sums with one warp per tile
-enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2, ACC_CELL = 3, ACC_WARP = 4 };
+//  ACC_MIXED dense tiles (more than split_min particles) by k_p2g_cell, the
+//            others by k_p2g<ACC_HILO>: each tile's scheme depends only on its
+//            particle count, so results are still reproducible
+enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2, ACC_CELL = 3, ACC_WARP = 4, ACC_MIXED = 5 };
 
 struct P2GSmem {
     long long node[NQ * TN * TN];  // fixed-point sums of the (TILE+2)^2 window (int32 pairs / int64)
@@ -324,12 +356,14 @@ __device__ __forceinline__ PQ load_pq(const PBuf& B, int src, int li, int lj, co
 // than FP32 relative to the largest contribution. Pass B adds the
 // contributions; the window is converted back and written as the partials.
 template <int ACC>
-__global__ void __launch_bounds__(P2G_THREADS, 4) k_p2g(Shared sh) {
+__global__ void __launch_bounds__(P2G_THREADS, P2G_MIN_BLOCKS) k_p2g(Shared sh, int cls) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31;
-    const int nwork = sh.work_pref[sh.nscn];
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    int i0, i1;
+    work_range(p2g_count(sh, cls), i0, i1);
+    for (int i = i0; i < i1; ++i) {
+        const int w = p2g_item(sh, cls, i);
         load_desc(sh.desc + w, &sm.d);
         for (int k = tid; k < NQ * TN * TN; k += P2G_THREADS) sm.node[k] = 0;
         int* node32 = reinterpret_cast<int*>(sm.node);  // ACC_I32: [q][node]; ACC_HILO: hi at [q][node], lo at NQ*TN*TN + [q][node]
@@ -667,20 +701,6 @@ __device__ unsigned long long g_phase_clk[16];
 #define SLAB_PHASE_TILE()
 #endif
 
-// The work items of one CTA: a contiguous range of the flat work list, so
-// that consecutive items mostly belong to the same scenario.
-__device__ __forceinline__ void work_range(int nwork, int& w0, int& w1) {
-    const int per = (nwork + (int)gridDim.x - 1) / (int)gridDim.x;
-    w0 = min((int)blockIdx.x * per, nwork);
-    w1 = min(w0 + per, nwork);
-}
-
-// Scenario of the last work item looked up, with the step fields that do not
-// change during a launch (so a new item of the same scenario costs no loads).
-struct WorkCache {
-    int sid = -1, lo = 0, hi = 0, seq = 0, stepid = 0;
-};
-
 // index of work item w in its scenario's list (pref: the prefix over scenarios)
 __device__ __forceinline__ int cached_work(const Shared& sh, const int32_t* pref, int w, WorkCache& c) {
     if (w < c.lo || w >= c.hi) {
@@ -807,16 +827,17 @@ __device__ __forceinline__ void cell_sums(float (&acc)[NQ][NSLOT], bool staged, 
 // reproducible and the same alone or inside a batch. A tile costs two
 // dependent rounds of global loads (descriptor, candidates); each CTA takes
 // a contiguous run of work items.
-__global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared sh) {
+__global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared sh, int cls) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P2CSmem& sm = *reinterpret_cast<P2CSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const int li = tid / TILE, lj = tid % TILE;
-    int w0, w1;
-    work_range(sh.work_pref[sh.nscn], w0, w1);
+    int i0, i1;
+    work_range(p2g_count(sh, cls), i0, i1);
     SLAB_PHASE_BEGIN;
-    for (int w = w0; w < w1; ++w) {
+    for (int i = i0; i < i1; ++i) {
+        const int w = p2g_item(sh, cls, i);
         load_desc(sh.desc + w, &sm.d);
         for (int k = tid; k < P2C_WARPS * NCELL; k += P2C_THREADS) (&sm.wcur[0][0])[k] = 0;
         __syncthreads();
