@@ -77,6 +77,7 @@ struct TileDesc {
     int32_t t, total, nxt_off, sid;
     int32_t rstart[9];
     int32_t rpref[10];
+    int32_t blk4[4];  // node blocks of the tile's node window (own, +y, +x, +xy grid tile), written by k_grid
     int32_t pad_;
 };
 

@@ -261,6 +261,8 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
             if (at < sh.work_cap) sh.wlist[cls * sh.work_cap + at] = w;
         }
         D.pad_ = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) D.blk4[k] = -1;  // grid tiles off the terrain keep -1
         S.slot_of[t] = w;
         const int stamp = n->stepid;
         int gl[4], ng = 0;
@@ -1056,6 +1058,8 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
         }
         __syncthreads();
         const int blk = s_blk;
+        // the block of this grid tile is entry k of contributor k's window (for G2P)
+        if (tid < 4 && s_slot[tid] >= 0) sh.desc[s_slot[tid]].blk4[tid] = blk;
         double mloc = 0.0;
         if (blk >= 0) {
             float q[NQ];
@@ -1149,7 +1153,10 @@ __device__ __forceinline__ int dir_of(int ib, int jb, int ti, int tj) {
     return (di + 1) * 3 + (dj + 1);
 }
 
-constexpr int G2P_MIN_BLOCKS = NCELL == 64 ? 12 : 3;
+#ifndef SLAB_G2P_MIN_BLOCKS
+#define SLAB_G2P_MIN_BLOCKS (NCELL == 64 ? 16 : 3)
+#endif
+constexpr int G2P_MIN_BLOCKS = SLAB_G2P_MIN_BLOCKS;  // resident G2P CTAs per SM the register budget is cut for
 
 struct G2PSmem {
     float4 nv[TN * TN];
@@ -1157,10 +1164,41 @@ struct G2PSmem {
     int front, back;
     int wst[2][NCELL / 32], wmv[2][NCELL / 32];  // per-warp stayer / mover counts of a chunk (double buffered)
     int dcnt[9];
-    int blk4[4];
     TileDesc d;
     double red[5][NCELL / 32];
 };
+
+// one candidate of a tile in G2P: its index, data, and whether it is in the tile
+struct G2PCand {
+    int src;
+    int32_t cell, pid;
+    float2 f, v;
+    float h, m;
+    bool valid;
+};
+
+__device__ __forceinline__ G2PCand load_g2p_cand(const TileDesc& D, const PBuf& B, int k, int ncand, int t, int TY) {
+    G2PCand q;
+    q.valid = k < ncand;
+    q.src = 0;
+    q.cell = 0;
+    q.pid = 0;
+    q.f = make_float2(1.f, 1.f);
+    q.v = make_float2(0.f, 0.f);
+    q.h = q.m = 0.f;
+    if (q.valid) {
+        int r;
+        q.src = cand_to_index(k, D, r);
+        q.cell = B.cell[q.src];  // the other loads go out with it; the filter is applied on use
+        q.f = B.f[q.src];
+        q.v = B.v[q.src];
+        q.h = B.h[q.src];
+        q.m = B.m[q.src];
+        q.pid = B.id[q.src];
+        q.valid = tile_of_cell(q.cell, TY) == t;
+    }
+    return q;
+}
 
 // K4: G2P (src/simulation.cpp:877-940) of one tile: FLIP/PIC blend,
 // advection, depth update, and the write of the particle into the tile's
@@ -1177,10 +1215,6 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
     for (int w = w0; w < w1; ++w) {
         load_desc(sh.desc + w, &sm.d);
         if (tid < 9) sm.dcnt[tid] = 0;
-        if (tid == 32) {
-            sm.front = 0;
-            sm.back = 0;
-        }
         __syncthreads();
         const int sid = sm.d.sid;
         const Scn& S = sh.scn[sid];
@@ -1191,17 +1225,16 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         const int ti = t / sh.TY, tj = t % sh.TY;
         const bool outs = n->outs != 0;
         const bool need_vz = outs || n->vz_next;
-        if (tid < 4) {
-            const int gi = ti + (tid >> 1), gj = tj + (tid & 1);
-            sm.blk4[tid] = (gi < sh.TX && gj < sh.TY) ? S.blk_of[gi * sh.TY + gj] : -1;
-        }
-        __syncthreads();
+        const int ncand = sm.d.rpref[9];
+        const PBuf B = S.buf[cur];
+        // the first chunk's particles are requested before the node window, so both loads are in flight together
+        G2PCand pre = load_g2p_cand(sm.d, B, tid, ncand, t, sh.TY);
         for (int k = tid; k < TN * TN; k += NCELL) {
             const int a = k / TN, b = k % TN;
             const int i = ti * TILE + a, j = tj * TILE + b;
             float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
             if (i < sh.Nx && j < sh.Ny) {
-                const int blk = sm.blk4[(a >= TILE ? 2 : 0) + (b >= TILE ? 1 : 0)];
+                const int blk = sm.d.blk4[(a >= TILE ? 2 : 0) + (b >= TILE ? 1 : 0)];
                 if (blk >= 0) val = sh.nv[(size_t)blk * NCELL + (a % TILE) * TILE + (b % TILE)];
             }
             sm.nv[k] = val;
@@ -1213,10 +1246,8 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
             }
         }
         __syncthreads();
-        const int ncand = sm.d.rpref[9];
         const int total = sm.d.total;
         const int base = sm.d.nxt_off;
-        const PBuf B = S.buf[cur];
         const PBuf O = S.buf[nxt];
         const float dt = (float)c->dt;
         const float dt_ood = dt * S.ood;
@@ -1224,26 +1255,20 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         double mnx = INFINITY, mxx = 0.0, mny = INFINITY, mxy = 0.0, vv = 0.0;
         int front = 0, back = 0;  // stayers / movers placed so far (same in every thread)
         for (int k0 = 0; k0 < ncand; k0 += NCELL) {
-            const int k = k0 + tid;
-            bool valid = k < ncand;
-            int d = 4, ib = 0, jb = 0, src = 0;
-            int32_t cell = 0;
-            if (valid) {
-                int r;
-                src = cand_to_index(k, sm.d, r);
-                cell = B.cell[src];
-                valid = tile_of_cell(cell, sh.TY) == t;
-            }
+            const G2PCand q = k0 == 0 ? pre : load_g2p_cand(sm.d, B, k0 + tid, ncand, t, sh.TY);
+            const bool valid = q.valid;
+            const int32_t cell = q.cell;
+            int d = 4, ib = 0, jb = 0;
             float2 fn = make_float2(1.f, 1.f), vn = make_float2(0.f, 0.f);
             float hn = 0.f, m = 0.f, vzp = 0.f;
             double zp = 0.0;
             int32_t pid = 0;
             if (valid) {
-                const float2 f = B.f[src];
-                const float2 v = B.v[src];
-                const float h = B.h[src];
-                m = B.m[src];
-                pid = B.id[src];
+                const float2 f = q.f;
+                const float2 v = q.v;
+                const float h = q.h;
+                m = q.m;
+                pid = q.pid;
                 const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
                 float wx[3], wy[3], dwx[3], dwy[3];
                 bspline3(f.x, wx, dwx);
