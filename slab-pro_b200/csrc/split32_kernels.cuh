@@ -1071,16 +1071,20 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
 #pragma unroll
                 for (int k = 0; k < NQ; ++k) q[k] += P[k * TN * TN];
             };
+            const int i = gi * TILE + li, j = gj * TILE + lj;
+            const size_t bn = (size_t)blk * NCELL + tid;
+            const bool inside = i < sh.Nx && j < sh.Ny;
+            // terrain and maxima are requested with the partials (one round of loads, not three)
+            const float4 dm = inside ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
+            const float hmax0 = sh.hmax[bn], vmax0 = sh.vmax2[bn];
             add(s_slot[0], li, lj);
             if (li < 2) add(s_slot[2], li + TILE, lj);
             if (lj < 2) add(s_slot[1], li, lj + TILE);
             if (li < 2 && lj < 2) add(s_slot[3], li + TILE, lj + TILE);
-            const int i = gi * TILE + li, j = gj * TILE + lj;
-            const size_t bn = (size_t)blk * NCELL + tid;
             float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
             float hn = 0.f, vzn = 0.f;
             const float mi = q[0];
-            if (mi > 1e-6f && i < sh.Nx && j < sh.Ny) {
+            if (mi > 1e-6f && inside) {
                 const float vox = q[1] / mi, voy = q[2] / mi;
                 vzn = q[6] / mi;
                 hn = q[3] / mi;
@@ -1089,7 +1093,6 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
                 const float vsq = vtx * vtx + vty * vty;
                 float nvx = 0.f, nvy = 0.f;
                 if (vsq > 1e-16f) {
-                    const float4 dm = sh.dem[(int64_t)i * sh.Ny + j];
                     const float ct = dm.z;
                     const float vz = vtx * dm.x + vty * dm.y;
                     const float v3sq = vsq + vz * vz;
@@ -1112,8 +1115,8 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
                     }
                 }
                 out = make_float4(nvx, nvy, nvx - vox, nvy - voy);
-                sh.hmax[bn] = fmaxf(sh.hmax[bn], hn);
-                sh.vmax2[bn] = fmaxf(sh.vmax2[bn], nvx * nvx + nvy * nvy);
+                sh.hmax[bn] = fmaxf(hmax0, hn);
+                sh.vmax2[bn] = fmaxf(vmax0, nvx * nvx + nvy * nvy);
                 mloc = (double)mi;
             }
             sh.nv[bn] = out;
