@@ -265,6 +265,7 @@ def ours(args, rank, world):
         ms, wall, work, launches, _ = timed(s32, args.steps)
     assert work[0] == Np * args.steps, work
     ms_prof, _, work_prof, _, phases = timed(s32, args.steps, profile=True)
+    shapes, tunes = s32.launch_shapes()
     state = s32.particles()
     t32 = s32.state()[0]
     if args.only == "fp32":
@@ -373,6 +374,7 @@ def ours(args, rank, world):
         "fp64_plain": {"value": round(Np * args.steps / (ms64 * 1e-3), 1), "ms_per_step": round(ms64 / args.steps, 5),
                        "fp32_speedup": round(ms64 / ms, 2)},
         "gpu_launches": int(launches),
+        "launch_shapes": {"ctas": dict(zip(("prep", "p2g_dense", "p2g_sparse", "grid", "g2p"), shapes)), "tuning_passes": tunes},
         "clocks": clocks,
         "wall_s_timed": round(wall, 4),
         "sim_time_s": round(t32, 4),

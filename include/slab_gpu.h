@@ -185,6 +185,10 @@ slab_status slab_get_phase_times(slab_ctx* ctx, double out[5]);
  * grid updates). These are the units of the roofline accounting. */
 slab_status slab_work_counters(slab_ctx* ctx, int64_t out[2]);
 
+/* FP32_SPLIT: CTA counts of the step's five work kernels now in use and the
+ * tuning passes completed (as slab_batch_launch_shapes); zeros for FP64. */
+slab_status slab_launch_shapes(slab_ctx* ctx, int32_t out[6]);
+
 /* Number of kernels this context has launched since creation. */
 int64_t slab_kernel_launches(const slab_ctx* ctx);
 
@@ -235,6 +239,17 @@ int64_t slab_batch_kernel_launches(const slab_batch* b);
  * slab_get_phase_times (adds event records per step while on). */
 slab_status slab_batch_set_profiling(slab_batch* b, int32_t on);
 slab_status slab_batch_phase_times(slab_batch* b, double out[5]);
+/* Launch shapes (CTA counts) of the step's five work kernels: k_prep, P2G of
+ * the dense tiles, P2G of the sparse tiles, grid update, G2P. Any shape gives
+ * bitwise the same results. A tuner times five candidates per kernel (1/4,
+ * 1/2, 1, 2 and 4 times the occupancy grid) on live, interleaved steps and keeps
+ * the fastest; it runs on the first steps, after 4x as many steps as at its
+ * last pick, and when the active tile count halves or doubles.
+ * out[0..4] = the grids in use, out[5] = tuning passes completed. */
+slab_status slab_batch_launch_shapes(slab_batch* b, int32_t out[6]);
+/* grids[k] > 0 fixes kernel k's CTA count, 0 leaves it to the tuner (grids
+ * NULL: none fixed); tune = 0 stops the tuner (shapes stay as they are). */
+slab_status slab_batch_set_launch_shapes(slab_batch* b, const int32_t grids[5], int32_t tune);
 const char* slab_batch_last_error(const slab_batch* b);
 void slab_batch_destroy(slab_batch* b);
 

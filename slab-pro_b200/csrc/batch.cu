@@ -280,6 +280,24 @@ slab_status slab_batch_phase_times(slab_batch* b, double out[5]) {
     });
 }
 
+slab_status slab_batch_launch_shapes(slab_batch* b, int32_t out[6]) {
+    if (!b || !out) return SLAB_E_ARG;
+    return bguard(b, [&] {
+        int g[5];
+        b->E->launch_shapes(g);
+        for (int k = 0; k < 5; ++k) out[k] = g[k];
+        out[5] = b->E->tune.tunes;
+    });
+}
+
+slab_status slab_batch_set_launch_shapes(slab_batch* b, const int32_t grids[5], int32_t tune) {
+    if (!b) return SLAB_E_ARG;
+    if (grids)
+        for (int k = 0; k < 5; ++k)
+            if (grids[k] < 0) return SLAB_E_ARG;
+    return bguard(b, [&] { b->E->fix_shapes(grids, tune != 0); });
+}
+
 const char* slab_batch_last_error(const slab_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 void slab_batch_destroy(slab_batch* b) {

@@ -384,6 +384,14 @@ slab_status slab_work_counters(slab_ctx* c, int64_t out[2]) {
     });
 }
 
+slab_status slab_launch_shapes(slab_ctx* c, int32_t out[6]) {
+    if (!c || !out) return SLAB_E_ARG;
+    return guard(c, [&] {
+        need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
+        c->path->launch_shapes(out);
+    });
+}
+
 int64_t slab_kernel_launches(const slab_ctx* c) {
     if (!c) return 0;
     return c->extra_launches + (c->path ? c->path->launches() : 0);

@@ -158,6 +158,8 @@ struct Path {
     virtual int64_t launches() const = 0;
     virtual void phase_times(double out[5]) { for (int k = 0; k < 5; ++k) out[k] = 0; }
     virtual void set_profiling(bool) {}
+    // CTA counts of the work kernels and tuning passes (the FP32 path's tuner)
+    virtual void launch_shapes(int32_t out[6]) { for (int k = 0; k < 6; ++k) out[k] = 0; }
 };
 
 std::unique_ptr<Path> make_plain64(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d_ctl, Ctl* h_ctl);

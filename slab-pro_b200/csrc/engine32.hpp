@@ -70,6 +70,44 @@ class Engine32 {
     int blk_cap = 0;
     int64_t pending_blocks = 0;  // node blocks of scenarios added since the last t=0 pass (an estimate)
     int grid_p2g = 0, grid_p2g_cell = 0, grid_p2g_hilo = 0, grid_g2p = 0, grid_grid = 0, grid_prep = 0;
+
+    // Launch-shape tuner of the step's five work kernels (k_prep, k_p2g_cell,
+    // k_p2g<HILO>, k_grid, k_g2p). Each CTA of these kernels takes a
+    // contiguous slice of a device-built work list and every work item is
+    // computed by one CTA alone, so the grid size changes which CTA computes a
+    // tile, never a value: all candidates give bitwise the same results. The
+    // tuner times the candidates on live steps, interleaved (schedule step s
+    // runs candidate s mod NC, so a workload that changes during the schedule
+    // weighs on all candidates alike), and keeps per kernel the fastest. It
+    // tunes on the first steps, again after 4x as many steps as at the last
+    // pick, and when the active tile count has halved or doubled.
+    struct Tuner {
+        static constexpr int NK = 5, NC = 5, ROUNDS = 3, NSTEP = NC * ROUNDS;
+        static constexpr int FACTOR4[NC] = {1, 2, 4, 8, 16};  // grid = occupancy grid * FACTOR4[c] / 4
+        bool enabled = true;
+        int state = 0;         // 0: shapes fixed, 1: measuring, 2: measured, events not read yet
+        int done = 0;          // schedule steps launched
+        int64_t steps = 0;     // steps enqueued
+        int64_t next = 0;      // step count at which the next schedule starts
+        int64_t active = 0;    // active tiles seen by the last capacity check
+        int64_t active_at = 0; // active tiles when the last schedule started
+        int base[NK] = {};     // occupancy-derived grids
+        int pick[NK] = {2, 2, 2, 2, 2};
+        int fixed[NK] = {};    // > 0: grid set by the caller, not tuned
+        int tunes = 0;
+        std::vector<cudaEvent_t> ev;  // NK + 2 per schedule step
+        ~Tuner() {
+            for (auto e : ev) cudaEventDestroy(e);
+        }
+    } tune;
+    int tuned_grid(int k, int c) const;
+    void apply_shapes(const int* c);
+    void tune_pick();
+    void launch_step_timed(const Shared& sh, cudaEvent_t* e);
+    // the five work kernels' grid sizes now in use
+    void launch_shapes(int out[5]) const;
+    // grids[k] > 0 fixes kernel k's grid (NULL: none fixed); tune_on: the tuner runs
+    void fix_shapes(const int32_t* grids, bool tune_on);
     int work_cap = 0;
     int64_t work_cap_total = 0;
     void ensure_work_cap(int64_t need);

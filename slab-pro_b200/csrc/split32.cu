@@ -103,6 +103,9 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     int occ_d = 0;
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k32::k_prep, 256, 0));
     grid_prep = sms * std::max(occ_d, 1);  // one resident wave, one thread per active tile
+    const int base[Tuner::NK] = {grid_prep, grid_p2g_cell, grid_p2g_hilo, grid_grid, grid_g2p};
+    std::copy(base, base + Tuner::NK, tune.base);
+    if (const char* e = std::getenv("SLAB_TUNE")) tune.enabled = std::atoi(e) != 0;
     timer.nk = 5;  // k_prep, P2G, grid update, G2P, k_end
     const int phase_map[5] = {1, 2, 3, 4, 0};
     for (int k = 0; k < 5; ++k) timer.phase_of[k] = phase_map[k];
@@ -542,18 +545,120 @@ void Engine32::launch_step() {
     for (int k = 0; k < 5; ++k) launch_kernel(k, sh);
 }
 
+constexpr int Engine32::Tuner::FACTOR4[];
+
+int Engine32::tuned_grid(int k, int c) const {
+    if (tune.fixed[k] > 0) return tune.fixed[k];
+    return std::max(1, tune.base[k] * Tuner::FACTOR4[c] / 4);
+}
+
+void Engine32::apply_shapes(const int* c) {
+    int* g[Tuner::NK] = {&grid_prep, &grid_p2g_cell, &grid_p2g_hilo, &grid_grid, &grid_g2p};
+    for (int k = 0; k < Tuner::NK; ++k) *g[k] = tuned_grid(k, c[k]);
+}
+
+void Engine32::launch_shapes(int out[5]) const {
+    const int g[Tuner::NK] = {grid_prep, grid_p2g_cell, grid_p2g_hilo, grid_grid, grid_g2p};
+    for (int k = 0; k < Tuner::NK; ++k) out[k] = g[k];
+}
+
+void Engine32::fix_shapes(const int32_t* grids, bool tune_on) {
+    for (int k = 0; k < Tuner::NK; ++k) tune.fixed[k] = grids ? std::max<int32_t>(grids[k], 0) : 0;
+    tune.enabled = tune_on;
+    if (tune.state == 1) tune.state = 0;  // a schedule in flight is dropped (its events are not read)
+    apply_shapes(tune.pick);
+    graphs.clear();
+}
+
+// One MIXED step with an event before each kernel and after the last.
+void Engine32::launch_step_timed(const Shared& sh, cudaEvent_t* e) {
+    SLAB_CUDA(cudaEventRecord(e[0], st));
+    k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
+    SLAB_CUDA(cudaEventRecord(e[1], st));
+    k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, 0);
+    SLAB_CUDA(cudaEventRecord(e[2], st));
+    k32::k_p2g<k32::ACC_HILO><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, 1);
+    SLAB_CUDA(cudaEventRecord(e[3], st));
+    k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
+    SLAB_CUDA(cudaEventRecord(e[4], st));
+    k32::k_g2p<<<grid_g2p, NCELL, 0, st>>>(sh, T.z.get());
+    SLAB_CUDA(cudaEventRecord(e[5], st));
+    k32::k_end<<<1, 1024, 0, st>>>(sh);
+    SLAB_CUDA(cudaEventRecord(e[6], st));
+}
+
+// Reads the schedule's events and keeps, per kernel, the candidate with the
+// least summed time; the occupancy grid (candidate 2) stays unless another is
+// faster by more than 3 %, so timing noise does not flip the shapes.
+void Engine32::tune_pick() {
+    constexpr int W = Tuner::NK + 2;
+    SLAB_CUDA(cudaEventSynchronize(tune.ev[Tuner::NSTEP * W - 1]));
+    double ms[Tuner::NK][Tuner::NC] = {};
+    for (int s = 0; s < Tuner::NSTEP; ++s) {
+        const int c = s % Tuner::NC;
+        for (int k = 0; k < Tuner::NK; ++k) {
+            float t = 0;
+            SLAB_CUDA(cudaEventElapsedTime(&t, tune.ev[s * W + k], tune.ev[s * W + k + 1]));
+            ms[k][c] += t;
+        }
+    }
+    for (int k = 0; k < Tuner::NK; ++k) {
+        int best = 2;
+        for (int c = 0; c < Tuner::NC; ++c)
+            if (ms[k][c] < 0.97 * ms[k][2] && ms[k][c] < ms[k][best]) best = c;
+        tune.pick[k] = best;
+    }
+    apply_shapes(tune.pick);
+    graphs.clear();  // the step graphs carry the grid sizes
+    tune.state = 0;
+    tune.tunes += 1;
+    tune.next = std::max<int64_t>(4 * tune.steps, tune.steps + 256);
+}
+
 void Engine32::enqueue_steps(int chunk) {
     if (graph_nscn != nscn) {
         graphs.clear();
         graph_nscn = nscn;
     }
-    if (timer.on) {
-        const Shared sh = shared();
-        for (int k = 0; k < chunk; ++k) timer.profiled_step(st, [&](int kk) { launch_kernel(kk, sh); });
-        SLAB_CUDA(cudaGetLastError());
-    } else {
-        graphs.launch(chunk, st, [&] { launch_step(); });
+    int k = 0;
+    if (tune.enabled && acc_mode == k32::ACC_MIXED && !timer.on) {
+        if (tune.state == 2) tune_pick();
+        const bool moved = tune.active > 0 && tune.active_at > 0 && (tune.active > 2 * tune.active_at || 2 * tune.active < tune.active_at);
+        if (tune.state == 0 && nscn > 0 && (tune.steps >= tune.next || moved)) {
+            constexpr int W = Tuner::NK + 2;
+            while ((int)tune.ev.size() < Tuner::NSTEP * W) {
+                cudaEvent_t e;
+                SLAB_CUDA(cudaEventCreate(&e));
+                tune.ev.push_back(e);
+            }
+            tune.state = 1;
+            tune.done = 0;
+            tune.active_at = std::max<int64_t>(tune.active, 1);
+        }
+        if (tune.state == 1) {
+            const Shared sh = shared();
+            for (; k < chunk && tune.done < Tuner::NSTEP; ++k, ++tune.done) {
+                int c[Tuner::NK];
+                for (int q = 0; q < Tuner::NK; ++q) c[q] = tune.done % Tuner::NC;
+                apply_shapes(c);
+                launch_step_timed(sh, tune.ev.data() + (size_t)tune.done * (Tuner::NK + 2));
+            }
+            apply_shapes(tune.pick);
+            for (; k < chunk; ++k) launch_step();
+            SLAB_CUDA(cudaGetLastError());
+            if (tune.done == Tuner::NSTEP) tune.state = 2;
+        }
     }
+    if (k < chunk) {
+        if (timer.on) {
+            const Shared sh = shared();
+            for (; k < chunk; ++k) timer.profiled_step(st, [&](int kk) { launch_kernel(kk, sh); });
+            SLAB_CUDA(cudaGetLastError());
+        } else {
+            graphs.launch(chunk, st, [&] { launch_step(); });
+        }
+    }
+    tune.steps += chunk;
     nlaunch += (acc_mode == k32::ACC_MIXED ? 6 : 5) * (int64_t)chunk;
 }
 
@@ -571,9 +676,11 @@ bool Engine32::check_capacity() {
     d2h(&used_blocks, d_misc.get(), 1, st);
     SLAB_CUDA(cudaStreamSynchronize(st));
     bool grew = false;
+    int64_t active = 0;
     for (int s = 0; s < nscn; ++s) {
         if (!slots[s]) continue;
         const int need = std::max(h_cnt[s].act_count[0], h_cnt[s].act_count[1]);
+        active += need;
         Store& S = (*slots[s]);
         if (2 * need > S.act_cap && S.act_cap < ntiles) {
             const int cap = std::min(ntiles, std::max(2 * S.act_cap, 4 * need));
@@ -591,6 +698,7 @@ bool Engine32::check_capacity() {
             grew = true;
         }
     }
+    tune.active = active;
     if (grew) ensure_work_cap(work_cap_total);
     if (2 * (int64_t)used_blocks > blk_cap) {
         grow_blocks((int)std::min<int64_t>((int64_t)blk_cap * 2, INT32_MAX / NCELL));
@@ -776,6 +884,12 @@ struct Split32 final : Path {
     void phase_times(double out[5]) override {
         E.timer.collect();
         for (int k = 0; k < 5; ++k) out[k] = E.timer.acc[k];
+    }
+    void launch_shapes(int32_t out[6]) override {
+        int g[5];
+        E.launch_shapes(g);
+        for (int k = 0; k < 5; ++k) out[k] = g[k];
+        out[5] = E.tune.tunes;
     }
 };
 

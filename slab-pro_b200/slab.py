@@ -83,6 +83,7 @@ def lib():
         L.slab_poisson_disk.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int32, C.c_uint64, dp, C.c_int64,
                                         C.POINTER(C.c_int64)]
         L.slab_kernel_launches.argtypes = [vp]
+        L.slab_launch_shapes.argtypes = [vp, C.POINTER(C.c_int32)]
         L.slab_kernel_launches.restype = C.c_int64
         L.slab_last_error.argtypes = [vp]
         L.slab_last_error.restype = C.c_char_p
@@ -242,6 +243,12 @@ class Slab:
         self._check(self.L.slab_get_phase_times(self.h, _dp(out)))
         return out
 
+    def launch_shapes(self):
+        """FP32: (CTA counts of k_prep, dense P2G, sparse P2G, grid update, G2P; tuning passes done)."""
+        out = (C.c_int32 * 6)()
+        self._check(self.L.slab_launch_shapes(self.h, out))
+        return [int(v) for v in out[:5]], int(out[5])
+
 
 class Batch:
     """Many scenarios on one shared terrain, advanced together (FP32 split)."""
@@ -263,6 +270,8 @@ class Batch:
         L.slab_batch_kernel_launches.argtypes = [vp]
         L.slab_batch_set_profiling.argtypes = [vp, C.c_int32]
         L.slab_batch_phase_times.argtypes = [vp, dp]
+        L.slab_batch_launch_shapes.argtypes = [vp, C.POINTER(C.c_int32)]
+        L.slab_batch_set_launch_shapes.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32]
         L.slab_batch_kernel_launches.restype = C.c_int64
         L.slab_batch_last_error.argtypes = [vp]
         L.slab_batch_last_error.restype = C.c_char_p
@@ -356,6 +365,17 @@ class Batch:
         out = np.zeros(5)
         self._check(self.L.slab_batch_phase_times(self.h, _dp(out)))
         return out.tolist()
+
+    def launch_shapes(self):
+        """(CTA counts of k_prep, dense P2G, sparse P2G, grid update, G2P; tuning passes done)."""
+        out = (C.c_int32 * 6)()
+        self._check(self.L.slab_batch_launch_shapes(self.h, out))
+        return [int(v) for v in out[:5]], int(out[5])
+
+    def set_launch_shapes(self, grids=None, tune: bool = True):
+        """Fix CTA counts (grids[k] > 0; 0 or None: tuned); tune=False stops the tuner."""
+        g = None if grids is None else (C.c_int32 * 5)(*[int(v) for v in grids])
+        self._check(self.L.slab_batch_set_launch_shapes(self.h, g, 1 if tune else 0))
 
 
 class ServerConfig(C.Structure):
