@@ -719,21 +719,20 @@ __device__ __forceinline__ int cached_work(const Shared& sh, const int32_t* pref
 
 
 constexpr int P2C_THREADS = NCELL;  // one thread per cell of the tile
-constexpr int P2C_MIN_BLOCKS = NCELL == 64 ? 8 : 2;  // resident CTAs per SM the register budget is cut for
+constexpr int P2C_MIN_BLOCKS = NCELL == 64 ? 12 : 3;  // resident CTAs per SM the register budget is cut for
 constexpr int P2C_WARPS = P2C_THREADS / 32;
 constexpr int NSLOT = 9;            // nodes a cell's particles reach (3 x 3)
 constexpr int P2C_CAP = 6 * NCELL;  // candidates of a tile staged in shared memory (more go through global memory)
 
 struct P2CStage {
     float4 sa[P2C_CAP];  // staged candidates, by candidate index: f.x, f.y, m, h
-    float4 sb[P2C_CAP];  //                                        v.x, v.y, vz, -
+    float2 sv[P2C_CAP];  //                                        v
+    float svz[P2C_CAP];  //                                        vz
 };
 
 struct P2CSmem {
-    union {
-        P2CStage st;                    // while the sums are taken
-        float part[NQ * NSLOT][NCELL];  // then the per-cell sums: [q * 9 + a * 3 + b][cell]
-    } u;
+    P2CStage st;
+    float nsum[NQ * TN * TN];  // node sums of the tile's window, [q][node]
     int16_t lc[P2C_CAP];   // local cell of each staged candidate (-1: not in the tile)
     int16_t idx[P2C_CAP];  // sorted position -> candidate index
     float4 dem[(TILE + 1) * (TILE + 1)];
@@ -743,17 +742,17 @@ struct P2CSmem {
 };
 
 // P2G quantities of a staged particle (as load_pq)
-__device__ __forceinline__ PQ staged_pq(float4 a, float4 b, int li, int lj, const float4* dem, float g, float hod) {
+__device__ __forceinline__ PQ staged_pq(float4 a, float2 v, float vz, int li, int lj, const float4* dem, float g, float hod) {
     PQ p;
     const float4 dm = dem[(li + (a.x >= 1.f ? 1 : 0)) * (TILE + 1) + (lj + (a.y >= 1.f ? 1 : 0))];
     const float K = a.z * g * dm.z * dm.z;
     p.fx = a.x;
     p.fy = a.y;
     p.m = a.z;
-    p.mvx = a.z * b.x;
-    p.mvy = a.z * b.y;
+    p.mvx = a.z * v.x;
+    p.mvy = a.z * v.y;
     p.mh = a.z * a.w;
-    p.mvz = a.z * b.z;
+    p.mvz = a.z * vz;
     p.Kgx = K * dm.x;
     p.Kgy = K * dm.y;
     p.Khh = K * a.w * hod;
@@ -762,42 +761,42 @@ __device__ __forceinline__ PQ staged_pq(float4 a, float4 b, int li, int lj, cons
     return p;
 }
 
-// Sums of one particle over the 9 nodes of its cell's stencil
+// Sums of one particle over the 3 nodes of stencil row A of its cell
 // (src/simulation.cpp:758-795); OUTS adds m vz.
-template <bool OUTS>
-__device__ __forceinline__ void add_particle(float (&acc)[NQ][NSLOT], const PQ& p) {
+template <bool OUTS, int A>
+__device__ __forceinline__ void add_particle_row(float (&acc)[NQ][3], const PQ& p) {
     float wx[3], wy[3], dwx[3], dwy[3];
     bspline3(p.fx, wx, dwx);
     bspline3(p.fy, wy, dwy);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const int s = a * 3 + b;
-            const float wgt = wx[a] * wy[b];
-            if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
-                acc[0][s] += p.m * wgt;
-                acc[1][s] += p.mvx * wgt;
-                acc[2][s] += p.mvy * wgt;
-                acc[3][s] += p.mh * wgt;
-                acc[4][s] += p.Khh * (dwx[a] * wy[b]) - p.Kgx * wgt;
-                acc[5][s] += p.Khh * (dwy[b] * wx[a]) - p.Kgy * wgt;
-                if (OUTS) acc[6][s] += p.mvz * wgt;
-            }
+    for (int b = 0; b < 3; ++b) {
+        const float wgt = wx[A] * wy[b];
+        if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
+            acc[0][b] += p.m * wgt;
+            acc[1][b] += p.mvx * wgt;
+            acc[2][b] += p.mvy * wgt;
+            acc[3][b] += p.mh * wgt;
+            acc[4][b] += p.Khh * (dwx[A] * wy[b]) - p.Kgx * wgt;
+            acc[5][b] += p.Khh * (dwy[b] * wx[A]) - p.Kgy * wgt;
+            if (OUTS) acc[6][b] += p.mvz * wgt;
         }
     }
 }
 
-// Sums of one cell's particles in sorted order: staged in shared memory, or
-// (tiles over P2C_CAP candidates) read through the sorted index list in
-// global memory.
-template <bool OUTS>
-__device__ __forceinline__ void cell_sums(float (&acc)[NQ][NSLOT], bool staged, const P2CSmem& sm, const int32_t* __restrict__ order,
-                                          int c0, int nn, const PBuf& B, int li, int lj, float g, float hod) {
+// Row-A sums of one cell's particles in sorted order: staged in shared
+// memory, or (tiles over P2C_CAP candidates) read through the sorted index
+// list in global memory.
+template <bool OUTS, int A>
+__device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, const P2CSmem& sm, const int32_t* __restrict__ order,
+                                              int c0, int nn, const PBuf& B, int li, int lj, float g, float hod) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) acc[q][b] = 0.f;
     if (staged) {
         for (int r = c0; r < c0 + nn; ++r) {
             const int k = sm.idx[r];
-            add_particle<OUTS>(acc, staged_pq(sm.u.st.sa[k], sm.u.st.sb[k], li, lj, sm.dem, g, hod));
+            add_particle_row<OUTS, A>(acc, staged_pq(sm.st.sa[k], sm.st.sv[k], sm.st.svz[k], li, lj, sm.dem, g, hod));
         }
         return;
     }
@@ -805,8 +804,33 @@ __device__ __forceinline__ void cell_sums(float (&acc)[NQ][NSLOT], bool staged, 
     for (int r = 0; r < nn; ++r) {
         const int src = nsrc;
         if (r + 1 < nn) nsrc = order[c0 + r + 1];
-        add_particle<OUTS>(acc, load_pq(B, src, li, lj, sm.dem, g, hod, OUTS));
+        add_particle_row<OUTS, A>(acc, load_pq(B, src, li, lj, sm.dem, g, hod, OUTS));
     }
+}
+
+// Stencil row A of every cell into the node sums: in round (A, b) each node
+// receives the row sum of exactly one cell, so the rounds need no atomics and
+// every node adds its <= 9 cells in (a, b) order.
+template <bool OUTS, int A>
+__device__ __forceinline__ void p2c_row(P2CSmem& sm, bool staged, const int32_t* __restrict__ order, int c0, int nn, const PBuf& B,
+                                        int li, int lj, float g, float hod) {
+    float acc[NQ][3];
+    cell_row_sums<OUTS, A>(acc, staged, sm, order, c0, nn, B, li, lj, g, hod);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        __syncthreads();
+        const int nd = (li + A) * TN + (lj + b);
+#pragma unroll
+        for (int q = 0; q < (OUTS ? NQ : NQ - 1); ++q) sm.nsum[q * TN * TN + nd] += acc[q][b];
+    }
+}
+
+template <bool OUTS>
+__device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const int32_t* __restrict__ order, int c0, int nn, const PBuf& B,
+                                         int li, int lj, float g, float hod) {
+    p2c_row<OUTS, 0>(sm, staged, order, c0, nn, B, li, lj, g, hod);
+    p2c_row<OUTS, 1>(sm, staged, order, c0, nn, B, li, lj, g, hod);
+    p2c_row<OUTS, 2>(sm, staged, order, c0, nn, B, li, lj, g, hod);
 }
 
 // K2: P2G of one tile (src/simulation.cpp:726-798) as a segmented reduction
@@ -822,8 +846,10 @@ __device__ __forceinline__ void cell_sums(float (&acc)[NQ][NSLOT], bool staged, 
 //     tiles: an index into the tile's segment of the next particle buffer,
 //     unused until G2P);
 //  4. thread = cell: FP32 sums of the cell's particles, in sorted order, for
-//     the 9 nodes of its stencil;
-//  5. thread = node: the node's sums over its <= 9 cells, in a fixed order.
+//     the 3 nodes of one stencil row at a time (21 accumulators, so 12 tiles
+//     fit on an SM), each row added into shared node sums in three rounds:
+//     every node adds its <= 9 cells in (a, b) order;
+//  5. the node sums are the tile's partial window.
 // The candidates of a tile come in an order fixed by the previous step's G2P
 // (ordered placement), so every sum has a fixed order: results are bitwise
 // reproducible and the same alone or inside a batch. A tile costs two
@@ -842,6 +868,7 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
         const int w = p2g_item(sh, cls, i);
         load_desc(sh.desc + w, &sm.d);
         for (int k = tid; k < P2C_WARPS * NCELL; k += P2C_THREADS) (&sm.wcur[0][0])[k] = 0;
+        for (int k = tid; k < NQ * TN * TN; k += P2C_THREADS) sm.nsum[k] = 0.f;
         __syncthreads();
         SLAB_PHASE_MARK(0);
         const Scn& S = sh.scn[sm.d.sid];
@@ -883,8 +910,9 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
                 if (staged) {
                     sm.lc[k] = (int16_t)lc;
                     if (lc >= 0) {
-                        sm.u.st.sa[k] = make_float4(f.x, f.y, m, h);
-                        sm.u.st.sb[k] = make_float4(v.x, v.y, vz, 0.f);
+                        sm.st.sa[k] = make_float4(f.x, f.y, m, h);
+                        sm.st.sv[k] = v;
+                        sm.st.svz[k] = vz;
                     }
                 }
             }
@@ -942,47 +970,18 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
         }
         __syncthreads();
         SLAB_PHASE_MARK(3);
-        // 4. per-cell sums (the staged data is then overwritten by them)
+        // 4. per-cell row sums into the node sums
         {
-            float acc[NQ][NSLOT];
-#pragma unroll
-            for (int q = 0; q < NQ; ++q)
-#pragma unroll
-                for (int s = 0; s < NSLOT; ++s) acc[q][s] = 0.f;
             const int nn = max(0, min(n_c, total - c0));
             const float g = S.g, hod = 0.5f * S.ood;
-            if (outs) cell_sums<true>(acc, staged, sm, order, c0, nn, B, li, lj, g, hod);
-            else cell_sums<false>(acc, staged, sm, order, c0, nn, B, li, lj, g, hod);
-            __syncthreads();
-#pragma unroll
-            for (int q = 0; q < NQ; ++q)
-#pragma unroll
-                for (int s = 0; s < NSLOT; ++s) sm.u.part[q * NSLOT + s][tid] = acc[q][s];
+            if (outs) p2c_rows<true>(sm, staged, order, c0, nn, B, li, lj, g, hod);
+            else p2c_rows<false>(sm, staged, order, c0, nn, B, li, lj, g, hod);
         }
         __syncthreads();
         SLAB_PHASE_MARK(4);
-        // 5. node sums over the cells that reach the node, (a, b) ascending
+        // 5. the tile's partial window
         float* P = sh.part + (size_t)w * PART_STRIDE;
-        for (int k = tid; k < TN * TN; k += P2C_THREADS) {
-            const int A = k / TN, Bn = k % TN;
-            float v[NQ];
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) v[q] = 0.f;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const int ci = A - a;
-                if ((unsigned)ci >= TILE) continue;
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    const int cj = Bn - b;
-                    if ((unsigned)cj >= TILE) continue;
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) v[q] += sm.u.part[q * NSLOT + a * 3 + b][ci * TILE + cj];
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) P[q * TN * TN + k] = v[q];
-        }
+        for (int k = tid; k < PART_STRIDE; k += P2C_THREADS) P[k] = sm.nsum[k];
         __syncthreads();
         SLAB_PHASE_MARK(5);
         SLAB_PHASE_TILE();
