@@ -69,10 +69,10 @@ class Engine32 {
     int TX = 0, TY = 0, ntiles = 0;
     int blk_cap = 0;
     int64_t pending_blocks = 0;  // node blocks of scenarios added since the last t=0 pass (an estimate)
-    int grid_p2g = 0, grid_p2g_cell = 0, grid_p2g_hilo = 0, grid_g2p = 0, grid_grid = 0, grid_prep = 0;
+    int grid_p2g = 0, grid_p2g_cell = 0, grid_p2g_hilo = 0, grid_p2g_sparse = 0, grid_g2p = 0, grid_grid = 0, grid_prep = 0;
 
     // Launch-shape tuner of the step's five work kernels (k_prep, k_p2g_cell,
-    // k_p2g<HILO>, k_grid, k_g2p). Each CTA of these kernels takes a
+    // k_p2g_sparse, k_grid, k_g2p). Each CTA of these kernels takes a
     // contiguous slice of a device-built work list and every work item is
     // computed by one CTA alone, so the grid size changes which CTA computes a
     // tile, never a value: all candidates give bitwise the same results. The

@@ -85,6 +85,7 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
                                    (int)(k32::P2W_WARPS * sizeof(k32::P2WWarp))));
     if (const char* e = std::getenv("SLAB_P2G_ACC")) acc_mode = std::atoi(e);
     if (const char* e = std::getenv("SLAB_P2G_SPLIT")) split_min = std::atoi(e);
+    split_min = std::min(split_min, k32::P2S_CAP);
     int dev = 0, sms = 0, occ_p = 0, occ_g = 0, occ_u = 0;
     SLAB_CUDA(cudaGetDevice(&dev));
     SLAB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -98,12 +99,15 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     grid_p2g = sms * std::max(occ_p, 1);
     grid_p2g_cell = sms * std::max(occ_c, 1);
     grid_p2g_hilo = sms * std::max(occ_h, 1);
+    int occ_s = 0;
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k32::k_p2g_sparse, k32::P2S_THREADS, sizeof(k32::P2SSmem)));
+    grid_p2g_sparse = sms * std::max(occ_s, 1);
     grid_g2p = sms * std::max(occ_g, 1);
     grid_grid = sms * std::max(occ_u, 1);
     int occ_d = 0;
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k32::k_prep, 256, 0));
     grid_prep = sms * std::max(occ_d, 1);  // one resident wave, one thread per active tile
-    const int base[Tuner::NK] = {grid_prep, grid_p2g_cell, grid_p2g_hilo, grid_grid, grid_g2p};
+    const int base[Tuner::NK] = {grid_prep, grid_p2g_cell, grid_p2g_sparse, grid_grid, grid_g2p};
     std::copy(base, base + Tuner::NK, tune.base);
     if (const char* e = std::getenv("SLAB_TUNE")) tune.enabled = std::atoi(e) != 0;
     timer.nk = 5;  // k_prep, P2G, grid update, G2P, k_end
@@ -510,9 +514,9 @@ void Engine32::launch_t0() {
 void Engine32::launch_p2g(const Shared& sh) {
     if (acc_mode == k32::ACC_MIXED) {  // dense tiles, then sparse tiles
         k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, 0);
-        k32::k_p2g<k32::ACC_HILO><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, 1);
+        k32::k_p2g_sparse<<<grid_p2g_sparse, k32::P2S_THREADS, sizeof(k32::P2SSmem), st>>>(sh, 1);
     } else if (acc_mode == k32::ACC_WARP) {
-        k32::k_p2g_warp<<<grid_p2g, k32::P2W_THREADS, k32::P2W_WARPS * sizeof(k32::P2WWarp), st>>>(sh);
+        k32::k_p2g_warp<<<grid_p2g, k32::P2W_THREADS, k32::P2W_WARPS * sizeof(k32::P2WWarp), st>>>(sh, -1);
     } else if (acc_mode == k32::ACC_CELL) {
         k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, -1);
     } else if (acc_mode == k32::ACC_I32) {
@@ -553,12 +557,12 @@ int Engine32::tuned_grid(int k, int c) const {
 }
 
 void Engine32::apply_shapes(const int* c) {
-    int* g[Tuner::NK] = {&grid_prep, &grid_p2g_cell, &grid_p2g_hilo, &grid_grid, &grid_g2p};
+    int* g[Tuner::NK] = {&grid_prep, &grid_p2g_cell, &grid_p2g_sparse, &grid_grid, &grid_g2p};
     for (int k = 0; k < Tuner::NK; ++k) *g[k] = tuned_grid(k, c[k]);
 }
 
 void Engine32::launch_shapes(int out[5]) const {
-    const int g[Tuner::NK] = {grid_prep, grid_p2g_cell, grid_p2g_hilo, grid_grid, grid_g2p};
+    const int g[Tuner::NK] = {grid_prep, grid_p2g_cell, grid_p2g_sparse, grid_grid, grid_g2p};
     for (int k = 0; k < Tuner::NK; ++k) out[k] = g[k];
 }
 
@@ -577,7 +581,7 @@ void Engine32::launch_step_timed(const Shared& sh, cudaEvent_t* e) {
     SLAB_CUDA(cudaEventRecord(e[1], st));
     k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, 0);
     SLAB_CUDA(cudaEventRecord(e[2], st));
-    k32::k_p2g<k32::ACC_HILO><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, 1);
+    k32::k_p2g_sparse<<<grid_p2g_sparse, k32::P2S_THREADS, sizeof(k32::P2SSmem), st>>>(sh, 1);
     SLAB_CUDA(cudaEventRecord(e[3], st));
     k32::k_grid<<<grid_grid, NCELL, 0, st>>>(sh);
     SLAB_CUDA(cudaEventRecord(e[4], st));

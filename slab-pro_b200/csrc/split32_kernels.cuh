@@ -303,8 +303,9 @@ constexpr int P2G_MIN_BLOCKS = NCELL == 64 ? 16 : 4;
 //  ACC_CELL  no fixed point: k_p2g_cell, FP32 sums over cell-sorted particles
 //  ACC_WARP  k_p2g_warp: ACC_HILO sums with one warp per tile
 //  ACC_MIXED dense tiles (more than split_min particles) by k_p2g_cell, the
-//            others by k_p2g<ACC_HILO>: each tile's scheme depends only on its
-//            particle count, so results are still reproducible
+//            others by k_p2g_sparse (64-bit fixed point): each tile's scheme
+//            depends only on its particle count, so results are still
+//            reproducible
 enum { ACC_I32 = 0, ACC_HILO = 1, ACC_I64 = 2, ACC_CELL = 3, ACC_WARP = 4, ACC_MIXED = 5 };
 
 struct P2GSmem {
@@ -550,17 +551,18 @@ __device__ __forceinline__ PQ warp_pq(const Shared& sh, const PBuf& B, const Til
 // particles of one cell (mcc); a node's sum stays below 9 * mcc * 0.75 * b,
 // and the scale is the largest power of two that keeps that below 2^30; the
 // hi word is the rounded contribution, the lo word the rest at 2^-20.
-__global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh) {
+__global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh, int cls) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     P2WWarp& sw = reinterpret_cast<P2WWarp*>(smem_raw)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * P2W_WARPS + (threadIdx.x >> 5), nw = gridDim.x * P2W_WARPS;
-    const int nwork = sh.work_pref[sh.nscn];
+    const int nwork = p2g_count(sh, cls);
     const int per = (nwork + nw - 1) / nw;
-    const int w0 = min(gw * per, nwork), w1 = min(w0 + per, nwork);
+    const int i0 = min(gw * per, nwork), i1 = min(i0 + per, nwork);
     int* hi = sw.node;
     int* lo = sw.node + NQ * TN * TN;
-    for (int w = w0; w < w1; ++w) {
+    for (int i = i0; i < i1; ++i) {
+        const int w = p2g_item(sh, cls, i);
         if (lane < (int)(sizeof(TileDesc) / 4)) reinterpret_cast<int*>(&sw.d)[lane] = reinterpret_cast<const int*>(sh.desc + w)[lane];
         for (int k = lane; k < 2 * NQ * TN * TN; k += 32) sw.node[k] = 0;
         for (int k = lane; k < NCELL; k += 32) sw.ccnt[k] = 0;
@@ -987,6 +989,233 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
         SLAB_PHASE_TILE();
     }
     SLAB_PHASE_MARK(6);
+}
+
+// ----------------------------------------------------- P2G of sparse tiles
+
+// K2 for tiles with at most split_min particles (src/simulation.cpp:726-798).
+// Such a tile's time is load latency, not arithmetic, so the kernel:
+//  - keeps the scenario's buffer pointers across consecutive tiles of one
+//    scenario, and requests the next tile's descriptor while this one runs;
+//  - requests the terrain window and the first candidate of every thread in
+//    one round;
+//  - pass A: per particle quantities into shared memory, cell counts and the
+//    per-quantity bounds of one contribution (as k_p2g);
+//  - pass B: one (particle, stencil row) item per thread, three nodes each,
+//    added as the hi/lo 32-bit fixed-point pairs of k_p2g<ACC_HILO> with
+//    native shared-memory integer atomics. The integer sums are exact, so
+//    the result does not depend on arrival order, and it is bitwise the
+//    result of k_p2g<ACC_HILO> for the same tile.
+constexpr int P2S_THREADS = NCELL;
+constexpr int P2S_MIN_BLOCKS = NCELL == 64 ? 16 : 4;
+constexpr int P2S_CAP = NCELL;  // particles of a sparse tile (split_min is capped to it)
+constexpr int P2S_DEMW = (TILE + 1) * (TILE + 1);
+constexpr int P2S_DEM_PER = (P2S_DEMW + P2S_THREADS - 1) / P2S_THREADS;
+constexpr int DESC_WORDS = (int)(sizeof(TileDesc) / 4);
+static_assert(DESC_WORDS <= P2S_THREADS, "one descriptor word per thread");
+
+struct P2SSmem {
+    int hi[NQ * TN * TN];  // fixed-point sums of the (TILE+2)^2 window, [q][node]: rounded part
+    int lo[NQ * TN * TN];  //                                                      2^-20 finer rest
+    float4 dem[P2S_DEMW];
+    PQ pq[P2S_CAP];
+    int ccnt[NCELL];
+    unsigned bmax[NQ];
+    int mcc, nv;
+    float scale[NQ], iscale[NQ];
+    TileDesc d;
+};
+
+__device__ __forceinline__ PQ make_pq(float2 f, float2 v, float m, float h, float vz, int li, int lj, const float4* dem, float g, float hod) {
+    PQ p;
+    const float4 dm = dem[(li + (f.x >= 1.f ? 1 : 0)) * (TILE + 1) + (lj + (f.y >= 1.f ? 1 : 0))];
+    const float K = m * g * dm.z * dm.z;
+    p.fx = f.x;
+    p.fy = f.y;
+    p.m = m;
+    p.mvx = m * v.x;
+    p.mvy = m * v.y;
+    p.mh = m * h;
+    p.mvz = m * vz;
+    p.Kgx = K * dm.x;
+    p.Kgy = K * dm.y;
+    p.Khh = K * h * hod;
+    p.li = li;
+    p.lj = lj;
+    return p;
+}
+
+__global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shared sh, int cls) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P2SSmem& sm = *reinterpret_cast<P2SSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31;
+    int i0, i1;
+    work_range(p2g_count(sh, cls), i0, i1);
+    int w_cur = i0 < i1 ? p2g_item(sh, cls, i0) : 0;
+    int w_nxt = i0 + 1 < i1 ? p2g_item(sh, cls, i0 + 1) : 0;
+    if (i0 < i1) load_desc(sh.desc + w_cur, &sm.d);
+    int csid = -1;
+    PBuf B{};
+    Ctl* ctl = nullptr;
+    bool outs = false;
+    float g = 0.f, hod = 0.f;
+    for (int i = i0; i < i1; ++i) {
+        const int w = w_cur;
+        for (int k = tid; k < NQ * TN * TN; k += P2S_THREADS) {
+            sm.hi[k] = 0;
+            sm.lo[k] = 0;
+        }
+        for (int k = tid; k < NCELL; k += P2S_THREADS) sm.ccnt[k] = 0;
+        if (tid < NQ) sm.bmax[tid] = 0u;
+        if (tid == 0) {
+            sm.mcc = 0;
+            sm.nv = 0;
+        }
+        __syncthreads();
+        // the next tile's descriptor and the item after it, stored at the end
+        int dn = 0, w_nn = 0;
+        if (i + 1 < i1 && tid < DESC_WORDS) dn = reinterpret_cast<const int*>(sh.desc + w_nxt)[tid];
+        if (i + 2 < i1) w_nn = p2g_item(sh, cls, i + 2);
+        if (sm.d.sid != csid) {  // uniform: a new scenario in this CTA's run
+            csid = sm.d.sid;
+            const Scn& S = sh.scn[csid];
+            const SCnt* n = S.cnt;
+            B = S.buf[n->seq & 1];
+            outs = n->outs != 0;
+            g = S.g;
+            hod = 0.5f * S.ood;
+            ctl = S.ctl;
+        }
+        const int t = sm.d.t;
+        const int ti = t / sh.TY, tj = t % sh.TY;
+        const int ncand = sm.d.rpref[9];
+        // one round: the terrain window and each thread's first candidate
+        float4 dmr[P2S_DEM_PER];
+#pragma unroll
+        for (int r = 0; r < P2S_DEM_PER; ++r) {
+            const int k = tid + r * P2S_THREADS;
+            const int ii = ti * TILE + k / (TILE + 1), jj = tj * TILE + k % (TILE + 1);
+            dmr[r] = (k < P2S_DEMW && ii < sh.Nx && jj < sh.Ny) ? sh.dem[(int64_t)ii * sh.Ny + jj] : make_float4(0.f, 0.f, 1.f, 0.f);
+        }
+        int d0 = 0;
+        int32_t cell0 = 0;
+        float2 f0 = make_float2(0.f, 0.f), v0 = make_float2(0.f, 0.f);
+        float m0 = 0.f, h0 = 0.f, vz0 = 0.f;
+        if (tid < ncand) {
+            const int src = cand_to_index(tid, sm.d, d0);
+            cell0 = B.cell[src];
+            f0 = B.f[src];
+            v0 = B.v[src];
+            m0 = B.m[src];
+            h0 = B.h[src];
+            if (outs) vz0 = B.vz[src];
+        }
+#pragma unroll
+        for (int r = 0; r < P2S_DEM_PER; ++r) {
+            const int k = tid + r * P2S_THREADS;
+            if (k < P2S_DEMW) sm.dem[k] = dmr[r];
+        }
+        __syncthreads();
+        // pass A: particle quantities, cell counts, bounds
+        float bm = 0.f, bvx = 0.f, bvy = 0.f, bh = 0.f, bvz = 0.f, bF = 0.f;
+        for (int k = tid; k < ncand; k += P2S_THREADS) {
+            int d = d0;
+            int32_t cell = cell0;
+            float2 f = f0, v = v0;
+            float m = m0, h = h0, vz = vz0;
+            if (k != tid) {
+                const int src = cand_to_index(k, sm.d, d);
+                cell = B.cell[src];
+                f = B.f[src];
+                v = B.v[src];
+                m = B.m[src];
+                h = B.h[src];
+                vz = outs ? B.vz[src] : 0.f;
+            }
+            const int li = cell_i(cell) - ti * TILE, lj = cell_j(cell) - tj * TILE;
+            if ((unsigned)li >= TILE || (unsigned)lj >= TILE) {
+                if (d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
+                continue;
+            }
+            const PQ p = make_pq(f, v, m, h, vz, li, lj, sm.dem, g, hod);
+            const int slot = atomicAdd(&sm.nv, 1);
+            if (slot < P2S_CAP) sm.pq[slot] = p;
+            else atomicOr(&ctl->err, ERR_CAPACITY);
+            const int c = atomicAdd(&sm.ccnt[li * TILE + lj], 1) + 1;
+            atomicMax(&sm.mcc, c);
+            bm = fmaxf(bm, p.m);
+            bvx = fmaxf(bvx, fabsf(p.mvx));
+            bvy = fmaxf(bvy, fabsf(p.mvy));
+            bh = fmaxf(bh, p.mh);
+            bvz = fmaxf(bvz, fabsf(p.mvz));
+            bF = fmaxf(bF, p.Khh + fmaxf(fabsf(p.Kgx), fabsf(p.Kgy)));
+        }
+        bm = warp_max(bm);
+        bvx = warp_max(bvx);
+        bvy = warp_max(bvy);
+        bh = warp_max(bh);
+        bvz = warp_max(bvz);
+        bF = warp_max(bF);
+        if (lane == 0) {
+            atomicMax(&sm.bmax[0], __float_as_uint(bm));
+            atomicMax(&sm.bmax[1], __float_as_uint(bvx));
+            atomicMax(&sm.bmax[2], __float_as_uint(bvy));
+            atomicMax(&sm.bmax[3], __float_as_uint(bh));
+            atomicMax(&sm.bmax[4], __float_as_uint(bF));
+            atomicMax(&sm.bmax[5], __float_as_uint(bF));
+            atomicMax(&sm.bmax[6], __float_as_uint(bvz));
+        }
+        __syncthreads();
+        if (tid < NQ) {
+            const float bound = 9.f * (float)sm.mcc * 0.75f * __uint_as_float(sm.bmax[tid]);
+            int e = 0;
+            if (bound > 0.f) {
+                int E;
+                frexpf(bound, &E);  // bound < 2^E
+                e = min(max(30 - E, -120), 120);
+            }
+            sm.scale[tid] = ldexpf(1.f, e);
+            sm.iscale[tid] = ldexpf(1.f, -e);
+        }
+        __syncthreads();
+        // pass B: (particle, stencil row) items
+        const int nv = min(sm.nv, P2S_CAP);
+        for (int it = tid; it < 3 * nv; it += P2S_THREADS) {
+            const int pi = it / 3, a = it - 3 * pi;
+            const PQ p = sm.pq[pi];
+            float wx[3], wy[3], dwx[3], dwy[3];
+            bspline3(p.fx, wx, dwx);
+            bspline3(p.fy, wy, dwy);
+            const float wxa = a == 0 ? wx[0] : (a == 1 ? wx[1] : wx[2]);
+            const float dwxa = a == 0 ? dwx[0] : (a == 1 ? dwx[1] : dwx[2]);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const float wgt = wxa * wy[b];
+                if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
+                    const int nd = (p.li + a) * TN + (p.lj + b);
+                    const float cq[NQ] = {p.m * wgt, p.mvx * wgt, p.mvy * wgt, p.mh * wgt, p.Khh * (dwxa * wy[b]) - p.Kgx * wgt,
+                                          p.Khh * (dwy[b] * wxa) - p.Kgy * wgt, p.mvz * wgt};
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) {
+                        if (q == 6 && !outs) continue;
+                        const float x = cq[q] * sm.scale[q];
+                        const int h_ = __float2int_rn(x);
+                        atomicAdd(sm.hi + q * TN * TN + nd, h_);
+                        const int l_ = __float2int_rn((x - (float)h_) * 1048576.f);
+                        if (l_) atomicAdd(sm.lo + q * TN * TN + nd, l_);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        float* P = sh.part + (size_t)w * PART_STRIDE;
+        for (int k = tid; k < PART_STRIDE; k += P2S_THREADS)
+            P[k] = (float)(((double)sm.hi[k] + (double)sm.lo[k] * (1.0 / 1048576.0)) * (double)sm.iscale[k / (TN * TN)]);
+        __syncthreads();
+        if (i + 1 < i1 && tid < DESC_WORDS) reinterpret_cast<int*>(&sm.d)[tid] = dn;
+        w_cur = w_nxt;
+        w_nxt = w_nn;
+    }
 }
 
 // ------------------------------------------------------------ grid update
