@@ -1220,36 +1220,75 @@ __global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shar
 
 // ------------------------------------------------------------ grid update
 
+// Values of one scenario that the grid update reads for every grid tile.
+struct GridScn {
+    SCnt* n;
+    Ctl* c;
+    int32_t* act_stamp;
+    int32_t* slot_of;
+    int32_t* blk_of;
+    float dt, g, mu_c, mu_v, xi, mu1, mu2, I0, d, phi;
+    int sid, seq, stepid, outs, fric;
+};
+
+__device__ __forceinline__ void load_grid_scn(const Shared& sh, int sid, GridScn& z) {
+    const Scn& S = sh.scn[sid];
+    SCnt* n = S.cnt;
+    z.n = n;
+    z.c = S.ctl;
+    z.act_stamp = S.act_stamp;
+    z.slot_of = S.slot_of;
+    z.blk_of = S.blk_of;
+    z.dt = (float)S.ctl->dt;
+    z.g = S.g;
+    z.mu_c = S.mu_c;
+    z.mu_v = S.mu_v;
+    z.xi = S.xi;
+    z.mu1 = S.mu1;
+    z.mu2 = S.mu2;
+    z.I0 = S.I0;
+    z.d = S.d;
+    z.phi = S.phi;
+    z.fric = S.fric;
+    z.sid = sid;
+    z.seq = n->seq;
+    z.stepid = n->stepid;
+    z.outs = n->outs;
+}
+
 // K3 + K6: computeGridVelocity (src/simulation.cpp:800-875) for the TILE^2
 // nodes owned by one grid tile. A node's P2G sum is the partials of the
 // tiles whose window covers it, added in a fixed order (own, -x, -y, -xy).
 // h_max / v_max2 are updated in the node block; the FP64 grid mass sum is
 // the conservation diagnostic.
+// Latency: the scenario's values stay in shared memory across a run of its
+// grid tiles, and thread 0 reads the grid-tile list two entries ahead.
 __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
-    __shared__ int s_sid, s_gt, s_seq, s_blk;
+    __shared__ int s_gt, s_blk;
     __shared__ int s_slot[4];
     __shared__ double s_red[NCELL / 32];
     __shared__ unsigned s_act[NCELL / 32];
+    __shared__ GridScn Z;
     const int tid = threadIdx.x;
     const int li = tid / TILE, lj = tid % TILE;
     int w0, w1;
     work_range(min(*sh.gcount, sh.gcap), w0, w1);
-    int csid = -1, cseq = 0;  // scenario of the last item and its step (thread 0)
+    // thread 0: the current and the next entry of the flat grid-tile list
+    int2 e_cur = make_int2(-1, 0), e_nxt = make_int2(-1, 0);
+    if (tid == 0) {
+        Z.sid = -1;
+        if (w0 < w1) e_cur = reinterpret_cast<const int2*>(sh.gflat)[w0];
+        if (w0 + 1 < w1) e_nxt = reinterpret_cast<const int2*>(sh.gflat)[w0 + 1];
+    }
     for (int w = w0; w < w1; ++w) {
         if (tid == 0) {
-            const int2 e = reinterpret_cast<const int2*>(sh.gflat)[w];
-            if (e.x != csid) {
-                csid = e.x;
-                cseq = sh.scn[csid].cnt->seq;
-            }
-            s_sid = e.x;
-            s_seq = cseq;
-            s_gt = e.y;
+            if (e_cur.x != Z.sid) load_grid_scn(sh, e_cur.x, Z);  // a new scenario in this CTA's run
+            s_gt = e_cur.y;
+            e_cur = e_nxt;
+            if (w + 2 < w1) e_nxt = reinterpret_cast<const int2*>(sh.gflat)[w + 2];
         }
         __syncthreads();
-        const Scn& S = sh.scn[s_sid];
-        SCnt* n = S.cnt;
-        Ctl* c = S.ctl;
+        Ctl* c = Z.c;
         const int gt = s_gt;
         const int gi = gt / sh.TY, gj = gt % sh.TY;
         if (tid < 4) {
@@ -1258,12 +1297,12 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
             int slot = -1;
             if (ti_ >= 0 && tj_ >= 0) {
                 const int tt = ti_ * sh.TY + tj_;
-                const int st_ = S.act_stamp[tt], sl = S.slot_of[tt];  // both loads in flight together
-                if (st_ == s_seq) slot = sl;
+                const int st_ = Z.act_stamp[tt], sl = Z.slot_of[tt];  // both loads in flight together
+                if (st_ == Z.seq) slot = sl;
             }
             s_slot[tid] = slot;
         } else if (tid == 32) {
-            int blk = S.blk_of[gt];
+            int blk = Z.blk_of[gt];
             if (blk < 0) {
                 // a block released by a retired scenario, else a fresh one
                 const int f = atomicSub(sh.free_count, 1);
@@ -1277,11 +1316,11 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
                     atomicOr(&c->err, ERR_CAPACITY);
                     blk = -1;
                 } else {
-                    S.blk_of[gt] = blk;
-                    sh.blk_owner[blk] = s_sid;
+                    Z.blk_of[gt] = blk;
+                    sh.blk_owner[blk] = Z.sid;
                 }
             }
-            if (blk >= 0) sh.blk_stamp[blk] = n->stepid;
+            if (blk >= 0) sh.blk_stamp[blk] = Z.stepid;
             s_blk = blk;
         }
         __syncthreads();
@@ -1302,7 +1341,7 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
             const int i = gi * TILE + li, j = gj * TILE + lj;
             const size_t bn = (size_t)blk * NCELL + tid;
             const bool inside = i < sh.Nx && j < sh.Ny;
-            // terrain and maxima are requested with the partials (one round of loads, not three)
+            // terrain and maxima are requested with the partials (one round of loads)
             const float4 dm = inside ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
             const float hmax0 = sh.hmax[bn], vmax0 = sh.vmax2[bn];
             add(s_slot[0], li, lj);
@@ -1316,7 +1355,7 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
                 const float vox = q[1] / mi, voy = q[2] / mi;
                 vzn = q[6] / mi;
                 hn = q[3] / mi;
-                const float dt = (float)c->dt;
+                const float dt = Z.dt;
                 const float vtx = vox + dt * (q[4] / mi), vty = voy + dt * (q[5] / mi);
                 const float vsq = vtx * vtx + vty * vty;
                 float nvx = 0.f, nvy = 0.f;
@@ -1325,15 +1364,16 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
                     const float vz = vtx * dm.x + vty * dm.y;
                     const float v3sq = vsq + vz * vz;
                     const float v3 = sqrtf(v3sq);
+                    const float g = Z.g;
                     float af;
-                    if (S.fric == SLAB_COULOMB) {
-                        af = S.mu_c * S.g * ct;
-                    } else if (S.fric == SLAB_VOELLMY) {
-                        af = S.mu_v * S.g * ct + S.g * v3sq / (S.xi * hn * ct);
+                    if (Z.fric == SLAB_COULOMB) {
+                        af = Z.mu_c * g * ct;
+                    } else if (Z.fric == SLAB_VOELLMY) {
+                        af = Z.mu_v * g * ct + g * v3sq / (Z.xi * hn * ct);
                     } else {
-                        const float I = 5.f * S.d * v3 / (2.f * hn * ct * ct * sqrtf(S.g * hn * S.phi));
-                        const float muI = S.mu1 + (S.mu2 - S.mu1) / (1.f + S.I0 / I);
-                        af = muI * S.g * ct;
+                        const float I = 5.f * Z.d * v3 / (2.f * hn * ct * ct * sqrtf(g * hn * Z.phi));
+                        const float muI = Z.mu1 + (Z.mu2 - Z.mu1) / (1.f + Z.I0 / I);
+                        af = muI * g * ct;
                     }
                     const float dv = dt * af;
                     if (dv < v3) {
@@ -1348,7 +1388,7 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
                 mloc = (double)mi;
             }
             sh.nv[bn] = out;
-            if (n->outs) {
+            if (Z.outs) {
                 sh.oh[bn] = hn;
                 sh.om[bn] = (i < sh.Nx && j < sh.Ny) ? mi : 0.f;
                 sh.ovz[bn] = vzn;
@@ -1369,7 +1409,7 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
                 sum += s_red[k];
                 na += s_act[k];
             }
-            if (sum != 0.0) atomicAdd(&n->grid_mass, sum);
+            if (sum != 0.0) atomicAdd(&Z.n->grid_mass, sum);
             if (na) atomicAdd(&c->node_steps, (unsigned long long)na);
         }
         __syncthreads();
@@ -1389,6 +1429,55 @@ __device__ __forceinline__ int dir_of(int ib, int jb, int ti, int tj) {
 #endif
 constexpr int G2P_MIN_BLOCKS = SLAB_G2P_MIN_BLOCKS;  // resident G2P CTAs per SM the register budget is cut for
 
+// Values of one scenario that a G2P launch reads for every tile: loaded
+// once per run of consecutive tiles of that scenario.
+struct G2PScn {
+    SCnt* n;
+    Ctl* c;
+    PBuf B, O;                 // current and next particle buffers
+    int32_t* grp_nxt;          // segment records of the next step
+    int32_t* act_stamp;
+    int32_t* act_list_nxt;
+    int32_t* act_count_nxt;
+    double dx;
+    float dt, dt_ood, ood, fr;
+    int sid, seq, act_cap, outs, need_vz;
+};
+
+__device__ __forceinline__ void load_g2p_scn(const Shared& sh, int sid, G2PScn& z) {
+    const Scn& S = sh.scn[sid];
+    SCnt* n = S.cnt;
+    Ctl* c = S.ctl;
+    const int seq = n->seq, cur = seq & 1, nxt = cur ^ 1;
+    z.n = n;
+    z.c = c;
+    z.B = S.buf[cur];
+    z.O = S.buf[nxt];
+    z.grp_nxt = S.grp[nxt];
+    z.act_stamp = S.act_stamp;
+    z.act_list_nxt = S.act_list[nxt];
+    z.act_count_nxt = &n->act_count[nxt];
+    z.dx = c->dx;
+    z.dt = (float)c->dt;
+    z.ood = S.ood;
+    z.dt_ood = z.dt * S.ood;
+    z.fr = S.fr;
+    z.sid = sid;
+    z.seq = seq;
+    z.act_cap = S.act_cap;
+    z.outs = n->outs != 0;
+    z.need_vz = z.outs || n->vz_next;
+}
+
+// puts tile tt on the next step's active list, once
+__device__ __forceinline__ void g2p_activate(const G2PScn& z, int tt) {
+    if (atomicMax(&z.act_stamp[tt], z.seq + 1) < z.seq + 1) {
+        const int kk = atomicAdd(z.act_count_nxt, 1);
+        if (kk < z.act_cap) z.act_list_nxt[kk] = tt;
+        else atomicOr(&z.c->err, ERR_CAPACITY);
+    }
+}
+
 struct G2PSmem {
     float4 nv[TN * TN];
     float4 dem[(TILE + 1) * (TILE + 1)];
@@ -1396,6 +1485,7 @@ struct G2PSmem {
     int wst[2][NCELL / 32], wmv[2][NCELL / 32];  // per-warp stayer / mover counts of a chunk (double buffered)
     int dcnt[9];
     TileDesc d;
+    G2PScn z;
     double red[5][NCELL / 32];
 };
 
@@ -1436,30 +1526,40 @@ __device__ __forceinline__ G2PCand load_g2p_cand(const TileDesc& D, const PBuf& 
 // segment of the next buffer -- stayers from the front, particles that moved
 // to a neighbour tile from the back, with per-direction counts. The block
 // max of |v|^2 and the particle bounding box feed the next step's dt and
-// remesh box (K5).
+// remesh box (K5). Latency: the scenario's values stay in shared memory
+// across a run of its tiles, the next tile's descriptor is requested while
+// this one runs, and a tile's neighbour activations (two dependent atomics)
+// are issued while the next tile's loads are in flight.
 __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const double* __restrict__ z64) {
     __shared__ G2PSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwork = sh.work_pref[sh.nscn];
     int w0, w1;
     work_range(nwork, w0, w1);
+    if (w0 < w1) load_desc(sh.desc + w0, &sm.d);
+    if (tid == 0) sm.z.sid = -1;
+    int pend_tt = -1;  // threads 0..8: neighbour tile the previous tile activates
     for (int w = w0; w < w1; ++w) {
-        load_desc(sh.desc + w, &sm.d);
         if (tid < 9) sm.dcnt[tid] = 0;
         __syncthreads();
-        const int sid = sm.d.sid;
-        const Scn& S = sh.scn[sid];
-        SCnt* n = S.cnt;
-        Ctl* c = S.ctl;
-        const int seq = n->seq, cur = seq & 1, nxt = cur ^ 1;
+        int dn = 0;
+        if (w + 1 < w1 && tid < DESC_WORDS) dn = reinterpret_cast<const int*>(sh.desc + w + 1)[tid];
+        if (sm.d.sid != sm.z.sid) {  // uniform: a new scenario in this CTA's run
+            if (pend_tt >= 0) g2p_activate(sm.z, pend_tt);
+            pend_tt = -1;
+            __syncthreads();
+            if (tid == 0) load_g2p_scn(sh, sm.d.sid, sm.z);
+            __syncthreads();
+        }
+        const G2PScn& Z = sm.z;
+        Ctl* c = Z.c;
         const int t = sm.d.t;
         const int ti = t / sh.TY, tj = t % sh.TY;
-        const bool outs = n->outs != 0;
-        const bool need_vz = outs || n->vz_next;
+        const bool outs = Z.outs != 0;
+        const bool need_vz = Z.need_vz != 0;
         const int ncand = sm.d.rpref[9];
-        const PBuf B = S.buf[cur];
-        // the first chunk's particles are requested before the node window, so both loads are in flight together
-        G2PCand pre = load_g2p_cand(sm.d, B, tid, ncand, t, sh.TY);
+        // the first chunk's particles, the node window and the terrain are requested together
+        G2PCand pre = load_g2p_cand(sm.d, Z.B, tid, ncand, t, sh.TY);
         for (int k = tid; k < TN * TN; k += NCELL) {
             const int a = k / TN, b = k % TN;
             const int i = ti * TILE + a, j = tj * TILE + b;
@@ -1476,13 +1576,16 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
                 sm.dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
             }
         }
+        if (pend_tt >= 0) g2p_activate(Z, pend_tt);  // the previous tile's, while the loads above are in flight
+        pend_tt = -1;
         __syncthreads();
         const int total = sm.d.total;
         const int base = sm.d.nxt_off;
-        const PBuf O = S.buf[nxt];
-        const float dt = (float)c->dt;
-        const float dt_ood = dt * S.ood;
-        const double dx = c->dx;
+        const PBuf& B = Z.B;
+        const PBuf O = Z.O;
+        const float dt = Z.dt;
+        const float dt_ood = Z.dt_ood;
+        const double dx = Z.dx;
         double mnx = INFINITY, mxx = 0.0, mny = INFINITY, mxy = 0.0, vv = 0.0;
         int front = 0, back = 0;  // stayers / movers placed so far (same in every thread)
         for (int k0 = 0; k0 < ncand; k0 += NCELL) {
@@ -1517,8 +1620,8 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
                         fly += nv.w * wgt;
                         div += (dwx[a] * wy[b]) * nv.x + (dwy[b] * wx[a]) * nv.y;
                     }
-                div *= S.ood;
-                const float fr = S.fr;
+                div *= Z.ood;
+                const float fr = Z.fr;
                 vn = make_float2(fr * (v.x + flx) + (1.f - fr) * picx, fr * (v.y + fly) + (1.f - fr) * picy);
                 hn = h / (1.f + dt * div);
                 if (need_vz) {
@@ -1606,24 +1709,17 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         }
         __syncthreads();
         if (tid < 9) {
-            int32_t* G = S.grp[nxt] + (size_t)t * GRP_STRIDE;
+            int32_t* G = Z.grp_nxt + (size_t)t * GRP_STRIDE;
             const int cnt = tid == 4 ? sm.front : sm.dcnt[tid];
             G[3 + tid] = cnt;
             if (tid == 0) {
                 G[0] = base;
                 G[1] = base + sm.front;
                 G[2] = base + sm.front + sm.back;
-                G[GRP_STAMP] = seq + 1;
+                G[GRP_STAMP] = Z.seq + 1;
                 if (sm.front + sm.back != total) atomicOr(&c->err, ERR_CAPACITY);
             }
-            if (cnt) {
-                const int tt = (ti + dir_i(tid)) * sh.TY + (tj + dir_j(tid));
-                if (atomicMax(&S.act_stamp[tt], seq + 1) < seq + 1) {
-                    const int kk = atomicAdd(&n->act_count[nxt], 1);
-                    if (kk < S.act_cap) S.act_list[nxt][kk] = tt;
-                    else atomicOr(&c->err, ERR_CAPACITY);
-                }
-            }
+            if (cnt) pend_tt = (ti + dir_i(tid)) * sh.TY + (tj + dir_j(tid));
         }
         // per-tile reductions into the scenario's control block
         mnx = warp_min(mnx);
@@ -1654,7 +1750,9 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
             atomicMax(reinterpret_cast<unsigned long long*>(&c->vmax2_acc), (unsigned long long)__double_as_longlong(vv));
         }
         __syncthreads();
+        if (w + 1 < w1 && tid < DESC_WORDS) reinterpret_cast<int*>(&sm.d)[tid] = dn;
     }
+    if (pend_tt >= 0) g2p_activate(sm.z, pend_tt);  // the last tile's
 }
 
 // K5: end of the step for every running scenario (the per-step reductions
