@@ -136,6 +136,7 @@ Shared Engine32::shared() const {
     sh.blk_cap = blk_cap;
     sh.nscn = nscn;
     sh.scn = d_scn.get();
+    sh.cnt = d_cnt.get();
     sh.work_pref = d_work_pref.get();
     sh.wlist = d_wlist.get();
     sh.wcount = d_misc.get() + 2;

@@ -127,6 +127,7 @@ struct Shared {
     int32_t blk_cap;
     int32_t nscn;
     const Scn* scn;
+    SCnt* cnt;            // [nscn] step counters (scn[s].cnt == cnt + s)
     int32_t* work_pref;   // [nscn+1] prefix of active tiles (P2G / G2P work)
     int32_t* wlist;       // [2][work_cap] work items of the two P2G kernels: dense tiles, then sparse ones
     int32_t* wcount;      // [2] their counts

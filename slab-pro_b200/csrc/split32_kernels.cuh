@@ -91,6 +91,32 @@ __device__ int warp_atomic_add(int* addr, int val, unsigned mask) {
     return base + prefix;
 }
 
+// warp_atomic_add in two halves, so that several atomics are in flight
+// before the first result is used: issue (the leader's atomic), then finish
+// (the broadcast of its result)
+struct WarpAdd {
+    unsigned peers;
+    int leader, prefix, base;
+};
+__device__ __forceinline__ WarpAdd warp_add_issue(int* addr, int val, unsigned mask) {
+    WarpAdd a;
+    a.peers = __match_any_sync(mask, (unsigned long long)addr);
+    const int lane = threadIdx.x & 31;
+    a.leader = __ffs(a.peers) - 1;
+    a.prefix = 0;
+    int total = 0;
+    for (unsigned m = a.peers; m; m &= m - 1) {
+        const int l = __ffs(m) - 1;
+        const int v = __shfl_sync(a.peers, val, l);
+        if (l < lane) a.prefix += v;
+        total += v;
+    }
+    a.base = 0;
+    if (lane == a.leader) a.base = atomicAdd(addr, total);
+    return a;
+}
+__device__ __forceinline__ int warp_add_finish(const WarpAdd& a) { return __shfl_sync(a.peers, a.base, a.leader) + a.prefix; }
+
 // candidate index -> particle index in the current buffer (range d)
 __device__ __forceinline__ int cand_to_index(int q, const TileDesc& D, int& d) {
     d = 0;
@@ -218,8 +244,9 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
         int sid, loc;
         find_work(sh.work_pref, sh.nscn, w, sid, loc);
         const Scn& S = sh.scn[sid];
-        SCnt* n = S.cnt;
+        SCnt* n = sh.cnt + sid;  // no load of S.cnt in the chain
         const int seq = n->seq, cur = seq & 1;
+        const int stamp = n->stepid;
         const int t = S.act_list[cur][loc];
         const int ti = t / sh.TY, tj = t % sh.TY;
         TileDesc D;
@@ -254,24 +281,28 @@ __global__ void __launch_bounds__(256) k_prep(Shared sh) {
         }
         D.rpref[9] = acc;
         D.total = cnt;
-        D.nxt_off = warp_atomic_add(&n->cursor, cnt, vmask);
-        if (sh.split_min >= 0) {  // dense tiles to the cell-sorted P2G, sparse ones to the fixed-point P2G
-            const int cls = cnt > sh.split_min ? 0 : 1;
-            const int at = warp_atomic_add(sh.wcount + cls, 1, vmask);
-            if (at < sh.work_cap) sh.wlist[cls * sh.work_cap + at] = w;
-        }
-        D.pad_ = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) D.blk4[k] = -1;  // grid tiles off the terrain keep -1
-        S.slot_of[t] = w;
-        const int stamp = n->stepid;
-        int gl[4], ng = 0;
+        // every atomic of the tile is issued before the first result is used
+        // (grid-tile stamps, segment cursor, class list), so they share one round
         int old[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int gi = ti + (k >> 1), gj = tj + (k & 1);
             old[k] = (gi < sh.TX && gj < sh.TY) ? atomicMax(&S.gt_stamp[gi * sh.TY + gj], stamp) : stamp;
         }
+        const WarpAdd a_cur = warp_add_issue(&n->cursor, cnt, vmask);
+        const int cls = cnt > sh.split_min ? 0 : 1;
+        WarpAdd a_cls{};
+        if (sh.split_min >= 0) a_cls = warp_add_issue(sh.wcount + cls, 1, vmask);
+        D.nxt_off = warp_add_finish(a_cur);
+        if (sh.split_min >= 0) {  // dense tiles to the cell-sorted P2G, sparse ones to the fixed-point P2G
+            const int at = warp_add_finish(a_cls);
+            if (at < sh.work_cap) sh.wlist[cls * sh.work_cap + at] = w;
+        }
+        D.pad_ = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) D.blk4[k] = -1;  // grid tiles off the terrain keep -1
+        S.slot_of[t] = w;
+        int gl[4], ng = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (old[k] < stamp) gl[ng++] = (ti + (k >> 1)) * sh.TY + (tj + (k & 1));
