@@ -1035,8 +1035,7 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
 //  - pass B: one (particle, stencil row) item per thread, three nodes each,
 //    added as the hi/lo 32-bit fixed-point pairs of k_p2g<ACC_HILO> with
 //    native shared-memory integer atomics. The integer sums are exact, so
-//    the result does not depend on arrival order, and it is bitwise the
-//    result of k_p2g<ACC_HILO> for the same tile.
+//    the result does not depend on arrival order.
 constexpr int P2S_THREADS = NCELL;
 constexpr int P2S_MIN_BLOCKS = NCELL == 64 ? 16 : 4;
 constexpr int P2S_CAP = NCELL;  // particles of a sparse tile (split_min is capped to it)
