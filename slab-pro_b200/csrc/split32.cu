@@ -6,6 +6,8 @@
 #include <cstdlib>
 #include <type_traits>
 #include <cstring>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "engine.hpp"
@@ -20,6 +22,31 @@ template <typename T> void h2d(T* d, const T* h, size_t n, cudaStream_t s) {
 }
 template <typename T> void d2h(T* h, const T* d, size_t n, cudaStream_t s) {
     if (n) SLAB_CUDA(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+}
+
+// Zeroes n doubles with up to 8 host threads: the maxima maps of a large
+// terrain are hundreds of MB, mostly pages of the caller's arrays that were
+// never touched, and one thread takes tens of milliseconds to fault them in.
+void zero_fill(double* p, size_t n) {
+    if (!p || n == 0) return;
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    if (n < ((size_t)1 << 20) || hw == 1) {
+        std::memset(p, 0, n * sizeof(double));
+        return;
+    }
+    const size_t per = (n + hw - 1) / hw;
+    std::vector<std::thread> th;
+    size_t done = 0;  // the prefix handed to threads
+    try {
+        for (unsigned k = 0; k < hw && done < n; ++k) {
+            const size_t a = done, b = std::min(n, a + per);
+            th.emplace_back([p, a, b] { std::memset(p + a, 0, (b - a) * sizeof(double)); });
+            done = b;
+        }
+    } catch (const std::system_error&) {  // no thread to be had: the rest on this one
+    }
+    if (done < n) std::memset(p + done, 0, (n - done) * sizeof(double));
+    for (auto& t : th) t.join();
 }
 }  // namespace
 
@@ -827,11 +854,23 @@ void Engine32::download_grid(int sid, slab_grid_view* gv) {
 }
 
 void Engine32::download_max(int sid, double* hmax, double* vmax2) {
-    const std::vector<float> f = gather_nodes(sid, -1, 0, 0, T.Nx, T.Ny, {d_hmax.get(), d_vmax2.get()}, false);
+    // nodes outside the box of the scenario's node blocks were never updated:
+    // zero; only the box is gathered on the device and copied back
+    int box[4];
+    box_of_blocks(sid, box);
     const size_t nn = (size_t)T.Nx * T.Ny;
-    for (size_t k = 0; k < nn; ++k) {
-        if (hmax) hmax[k] = f[k];
-        if (vmax2) vmax2[k] = f[nn + k];
+    zero_fill(hmax, nn);
+    zero_fill(vmax2, nn);
+    const int nI = box[1] - box[0] + 1, nJ = box[3] - box[2] + 1;
+    if (nI <= 0 || nJ <= 0) return;
+    const std::vector<float> f = gather_nodes(sid, -1, box[0], box[2], nI, nJ, {d_hmax.get(), d_vmax2.get()}, false);
+    const size_t n = (size_t)nI * nJ;
+    for (int i = 0; i < nI; ++i) {
+        const size_t row = (size_t)(box[0] + i) * T.Ny + box[2], src = (size_t)i * nJ;
+        for (int j = 0; j < nJ; ++j) {
+            if (hmax) hmax[row + j] = f[src + j];
+            if (vmax2) vmax2[row + j] = f[n + src + j];
+        }
     }
 }
 
