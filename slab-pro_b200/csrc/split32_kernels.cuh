@@ -3,7 +3,10 @@
 //   k_prep   (grid)    one thread per active tile: its 9 candidate ranges,
 //                      its segment in the next buffer, its grid tiles on the
 //                      flat grid-tile list
-//   k_p2g_*  (grid)    one CTA (or warp) per active tile: P2G partial sums
+//   k_p2g_cell, k_p2g_sparse (grid)
+//                      one CTA per active tile: P2G partial sums, tiles of
+//                      more than split_min particles by the cell-sorted
+//                      kernel, the others by the sparse-tile kernel
 //   k_grid   (grid)    one CTA per grid tile: grid update + friction
 //   k_g2p    (grid)    one CTA per active tile: G2P, advection, regrouping
 //   k_end    (1 CTA)   per scenario: end of the step, then the next step's
@@ -13,10 +16,10 @@
 // scenarios, so one launch advances every running scenario by one step, each
 // with its own dt and friction law.
 //
-// Every result is independent of the timing of the threads: the default P2G
-// sorts a tile's particles by cell in a stable, data-determined order and
-// sums in that order (the fixed-point variants add integers, exact and
-// associative); the grid update adds the partials of a node's tiles in a
+// Every result is independent of the timing of the threads: the cell-sorted
+// P2G sorts a tile's particles by cell in a stable, data-determined order and
+// sums in that order; the sparse-tile P2G and the other fixed-point variants
+// add integers, exact and associative; the grid update adds the partials of a node's tiles in a
 // fixed order; G2P places particles by block prefix sums in candidate order;
 // everything else is per particle or a max/min. So a step is bitwise
 // reproducible, alone or inside a batch.
