@@ -139,7 +139,7 @@ def write_ref_inputs(c, P, d):
     return dem, parts
 
 
-def ref_json(c, d, nsteps_time):
+def ref_json(c, d, nsteps_time, output_dt=None):
     cfg = c["cfg"]
     fr = cfg["friction"]
     fj = {"type": fr}
@@ -151,7 +151,7 @@ def ref_json(c, d, nsteps_time):
         fj["mu_I"] = {"mu_1": cfg["mui_mu1"], "mu_2": cfg["mui_mu2"], "I0": cfg["mui_I0"], "d": cfg["mui_d"], "phi": cfg["mui_phi"]}
     j = {"project_dir": os.path.join(d, "out"), "sim_name": "bench",
          "physical_params": {"gravity": cfg["gravity"], "rho": cfg["rho"]},
-         "time_params": {"output_dt": nsteps_time, "total_time": nsteps_time},
+         "time_params": {"output_dt": output_dt or nsteps_time, "total_time": nsteps_time},
          "numerical_params": {"C_cfl": cfg["C_cfl"], "dt_max": cfg["dt_max"], "flip_ratio": cfg["flip_ratio"], "sampling_method": "UNIFORM"},
          "friction": fj,
          "terrain": {"type": "ANALYTICAL", "analytical": {"Lx": 8.0, "Ly": 8.0, "dx": c["dx"]}},
@@ -162,21 +162,29 @@ def ref_json(c, d, nsteps_time):
     return path
 
 
-def run_reference(c, P, nsteps, replicas):
-    """Run the reference binary `replicas` times concurrently for about
-    `nsteps` steps from state P; returns (particle-steps/s aggregate, steps,
-    seconds of the slowest replica)."""
+def run_reference(c, P, nsteps, replicas, warmup=0):
+    """Run the reference binary `replicas` times concurrently from state P:
+    `warmup` untimed steps, then about `nsteps` timed ones. Output frames are
+    placed every `warmup` steps (or once, at the end); at each frame the
+    binary prints the sum of the reference's own per-phase timers so far
+    (SLAB_REF_FRAME_TIMERS, oracle/ref_hooks.cpp) and the step count, and the
+    timed part is what lies between the first frame after the warm-up (t=0
+    without one) and the last frame. Returns (particle-steps/s aggregate,
+    timed steps of one replica, seconds of the slowest replica)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not os.path.exists(O.REF_BIN):
         raise RuntimeError("oracle/_ref/slab_ref not built")
+    dt_max = c["cfg"]["dt_max"]
+    if warmup > 0:
+        nsteps = -(-nsteps // warmup) * warmup  # whole frames after the warm-up
+    T = (warmup + nsteps) * dt_max
     with tempfile.TemporaryDirectory() as d:
         dem, parts = write_ref_inputs(c, P, d)
-        T = nsteps * c["cfg"]["dt_max"]
         procs = []
         for r in range(replicas):
-            cfg = ref_json(c, d, T)
-            env = dict(os.environ, SLAB_REF_NO_DUMP="1")
+            cfg = ref_json(c, d, T, output_dt=warmup * dt_max if warmup > 0 else None)
+            env = dict(os.environ, SLAB_REF_NO_DUMP="1", SLAB_REF_FRAME_TIMERS="1")
             procs.append(subprocess.Popen([O.REF_BIN, cfg, "--dem-bin", dem, "--particles", parts], stdout=subprocess.PIPE,
                                           stderr=subprocess.PIPE, text=True, env=env))
         secs, steps = [], []
@@ -184,18 +192,23 @@ def run_reference(c, P, nsteps, replicas):
             out, err = p.communicate()
             if p.returncode != 0:
                 raise RuntimeError(f"slab_ref failed: {err.strip()[-300:]}")
-            phase = 0.0
-            last = 0
+            marks, pending = [], None  # (step count, phase seconds so far) per output frame
             for ln in out.splitlines():
-                if ln.startswith("Time step:"):
-                    last = int(ln.split()[2])
-                for key in ("updateDt took", "sort took", "remesh took", "P2G took", "computeGridVelocity took", "G2P took"):
-                    if ln.startswith(key):
-                        phase += float(ln.split()[-2])
-            secs.append(phase)
-            steps.append(last)
+                if ln.startswith("Phase seconds so far:"):
+                    pending = float(ln.split()[-1])
+                elif ln.startswith("Time step:") and pending is not None:
+                    marks.append((int(ln.split()[2]), pending))
+                    pending = None
+            first = 1 if warmup > 0 else 0
+            if len(marks) < first + 2:
+                raise RuntimeError(f"slab_ref printed {len(marks)} frames")
+            (n0, s0), (n1, s1) = marks[first], marks[-1]
+            steps.append(n1 - n0)
+            secs.append(s1 - s0)
     Np = len(P["h"])
     tmax = max(secs)
+    if min(steps) <= 0 or tmax <= 0:
+        raise RuntimeError("no timed reference steps")
     return sum(steps) * Np / tmax, steps[0], tmax
 
 
@@ -618,16 +631,18 @@ def reference_arm(args, rank, world):
     Np = len(P["h"])
     replicas = max(1, min(os.cpu_count() or 1, args.ref_procs))
     k = max(2, min(args.steps, int(args.cpu_seconds * 8e6 / Np)))
+    w = max(0, args.warmup)
     t0 = time.perf_counter()
-    v, st, sec = run_reference(c, P, k, replicas)
+    v, st, sec = run_reference(c, P, k, replicas, warmup=w)
     wall = time.perf_counter() - t0
     return {"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": METRIC, "n_gpus": world, "steps": st,
-            "warmup": 0, "ms_per_step": round(sec / max(st, 1) * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "warmup": w, "ms_per_step": round(sec / max(st, 1) * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": c["name"], "particles": Np, "dem": list(c["z"].shape), "dx": c["dx"],
                        "friction": c["cfg"]["friction"], "parallelism": f"{replicas} concurrent single-threaded processes"},
             "cpu_baseline": {"value": round(v, 1), "unit": METRIC, "cores": replicas, "kind": "reference",
-                             "sample": f"{st} steps from t=0 per process, {replicas} processes, per-phase timers "
+                             "sample": f"{w} untimed and {st} timed steps from t=0 per process, {replicas} processes, "
+                                       f"the reference's per-phase timers "
                                        f"(slowest {sec:.1f} s, wall {wall:.1f} s)"},
             "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 

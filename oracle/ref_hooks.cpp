@@ -15,6 +15,9 @@
 //                            then h, mass, v[2], vz, flip[2] on the remeshed grid
 //   max_values.bin           i64 Nx, Ny, then h_max, v_max2 over the terrain
 //
+// With SLAB_REF_FRAME_TIMERS=1, saveParticleData also prints the sum of the
+// reference's per-phase timers at every frame (the benchmark's reference arm).
+//
 // saveTerrain() is never called by the reference itself; here it is a
 // phase-level driver: it runs the t=0 pass and SLAB_REF_STEPS steps of the
 // reference's own private step functions and writes every step's state to
@@ -75,7 +78,21 @@ static bool no_dump() {
     return e && e[0] == '1';
 }
 
+// SLAB_REF_FRAME_TIMERS=1: at every output frame, print the sum of the
+// reference's own per-phase timers so far. simulate() prints the frame's step
+// count right after this hook, so a benchmark can time the steps between two
+// frames (for instance, after untimed warm-up steps that end at frame 1).
+static bool frame_timers() {
+    const char* e = std::getenv("SLAB_REF_FRAME_TIMERS");
+    return e && e[0] == '1';
+}
+
 template <typename T_, typename TV2_> void Simulation<T_, TV2_>::saveParticleData() const {
+    if (frame_timers()) {
+        std::printf("Phase seconds so far: %.9f\n",
+                    (double)(runtime_updateDt + runtime_sort + runtime_remesh + runtime_P2G + runtime_computeGridVelocity + runtime_G2P));
+        std::fflush(stdout);
+    }
     if (no_dump()) return;
     Out o(particle_path / frame_name("particles_frame_", padding, frame, ".bin"));
     o.i64(Np);

@@ -1,7 +1,9 @@
 """The bench's reference arm (`bench.py --impl reference`): the reference's own
 step loop (oracle/_ref/slab_ref, built from the reference's sources) timed on
 the host cores, printed as one JSON line with the fields of the product arm's
-line. Runs on the small 35-degree slope workload so it takes about a second."""
+line. The W warm-up steps are untimed: the run puts an output frame after
+them and times the steps between that frame and the last one. Runs on the
+small 35-degree slope workload so it takes about a second."""
 import json
 import os
 import subprocess
@@ -24,7 +26,8 @@ def test_reference_arm_prints_one_json_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference"
     assert d["metric"] == "particle-steps/s" and d["unit"] == d["metric"] and d["higher_is_better"] is True
-    assert d["value"] > 0 and d["steps"] >= 2
+    assert d["value"] > 0 and d["steps"] >= 3  # at least one frame of 3 steps after the warm-up
+    assert d["warmup"] == 3
     assert d["config"]["workload"] == "slope35_arc_401x101_dx5" and d["config"]["particles"] == 1600
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"]
