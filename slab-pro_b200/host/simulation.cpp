@@ -448,14 +448,16 @@ void Simulation::initializeParticles() {
         particles.h[p] = h_init[p];
         particles.A[p] = A_init;
         particles.mass[p] = rho * particles.h[p] * particles.A[p];
-        particles.theta[p] = particleSlopeAngle(p);
+        // the 4x4 node window of the z interpolation holds the particle's cell
+        // (the slope angle's node) too: check it before either is read
         const Vec2& xp = particles.x[p];
         const int ib = static_cast<int>((xp(0) - terrain.x[0]) * one_over_dx) - 1;
         const int jb = static_cast<int>((xp(1) - terrain.y[0]) * one_over_dx) - 1;
+        if (ib < 0 || jb < 0 || ib + 3 >= terrain.Nx || jb + 3 >= terrain.Ny)
+            throw std::runtime_error("release reaches the terrain edge (particle " + std::to_string(p) + ")");
+        particles.theta[p] = particleSlopeAngle(p);
         for (int i = ib; i < ib + 4; ++i)
             for (int j = jb; j < jb + 4; ++j) {
-                if (i < 0 || j < 0 || i >= terrain.Nx || j >= terrain.Ny)
-                    throw std::runtime_error("release reaches the terrain edge (particle " + std::to_string(p) + ")");
                 const T w = wip(xp(0), xp(1), terrain.x[i], terrain.y[j], one_over_dx);
                 particles.z[p] += terrain.z[ind(i, j, terrain.Ny)] * w;
             }

@@ -77,6 +77,45 @@ def test_malformed_json_and_unknown_names(tmp_path):
     assert r.returncode == 1 and "Unknown friction type" in r.stderr
 
 
+def _write_asc(d, text):
+    p = os.path.join(str(d), "bad.asc")
+    with open(p, "w") as f:
+        f.write(text)
+    return p
+
+
+BAD_INPUTS = {
+    "terrain type": (lambda j, d: j["terrain"].__setitem__("type", "MOON"), "Unknown terrain type: MOON"),
+    "release type": (lambda j, d: j["release"].__setitem__("type", "TRIANGLE"), "Unknown release shape type: TRIANGLE"),
+    "sampling": (lambda j, d: j["numerical_params"].__setitem__("sampling_method", "HEXAGONAL"), "Unknown sampling method"),
+    "polygon": (lambda j, d: j["release"].update({"type": "POLYGON", "polygon": {"filepath": os.path.join(str(d), "x.shp")}}),
+                "POLYGON releases need a shapefile reader"),
+    "missing dem": (lambda j, d: j["terrain"]["dem"].__setitem__("filepath", os.path.join(str(d), "none.asc")), "Failed to open ASC file"),
+    "bad header": (lambda j, d: j["terrain"]["dem"].__setitem__("filepath", _write_asc(d, "hello world\n")), "Bad ASC header"),
+    "short dem": (lambda j, d: j["terrain"]["dem"].__setitem__(
+        "filepath", _write_asc(d, "ncols 4\nnrows 3\nxllcorner 0\nyllcorner 0\ncellsize 5\nNODATA_value -9999\n1 2 3 4\n5 6\n")),
+        "ASC file ended early"),
+    # releases past each side of the 2000 x 500 m terrain: a clear error, not a read outside it
+    "edge low": (lambda j, d: j["release"]["rectangle"].__setitem__("center", [5.0, 5.0]), "release reaches the terrain edge"),
+    "edge x": (lambda j, d: j["release"]["rectangle"].__setitem__("center", [1990.0, 250.0]), "release reaches the terrain edge"),
+    "edge y": (lambda j, d: j["release"]["rectangle"].__setitem__("center", [150.0, 498.0]), "release reaches the terrain edge"),
+}
+
+
+@pytest.mark.parametrize("case", list(BAD_INPUTS))
+def test_bad_inputs_are_reported(case, tmp_path):
+    """Each bad input stops initialisation with exit code 1 and a message, as
+    the reference's main() reports a std::runtime_error."""
+    mutate, msg = BAD_INPUTS[case]
+    c = cases.case_slope35()
+    cfg = MG.write_inputs(c, str(tmp_path))
+    j = json.load(open(cfg))
+    mutate(j, tmp_path)
+    json.dump(j, open(cfg, "w"))
+    r = subprocess.run([CLI, cfg, "--init-only", str(tmp_path / "p.bin")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and msg in r.stderr, (r.returncode, r.stderr[-300:])
+
+
 def _writers():
     L = ctypes.CDLL(SIMLIB)
     L.slab_write_geotiff.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_char_p,
