@@ -370,7 +370,8 @@ def ours(args, rank, world):
     d2h = sum(out[k].nbytes for k in out) + 2 * hmx.nbytes
     e2e = {"value": round(Np * K_e2e / min(e2e_times), 1), "unit": METRIC,
            "h2d_bytes_per_step": int(h2d / K_e2e), "d2h_bytes_per_step": int(d2h / K_e2e),
-           "window": f"upload + t=0 pass + {K_e2e} steps + particle and max-map download, host FP64 arrays, best of 2"}
+           "window": f"upload + t=0 pass + {K_e2e} steps + particle and max-map download, host FP64 arrays, best of 2; "
+                     f"d2h counts the host arrays returned (the library copies only the node box the flow touched of the max maps)"}
     e.close()
 
     clocks = clk.summary()
