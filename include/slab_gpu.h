@@ -192,6 +192,8 @@ slab_status slab_launch_shapes(slab_ctx* ctx, int32_t out[6]);
 /* Number of kernels this context has launched since creation. */
 int64_t slab_kernel_launches(const slab_ctx* ctx);
 
+/* The message of the context's last failed call. With ctx NULL: the message
+ * of the calling thread's last failed slab_create, which leaves no context. */
 const char* slab_last_error(const slab_ctx* ctx);
 void slab_destroy(slab_ctx* ctx);
 

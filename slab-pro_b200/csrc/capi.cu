@@ -186,7 +186,10 @@ const char* slab_status_name(slab_status s) {
 }
 
 slab_status slab_create(const slab_terrain_desc* td, const double* z, slab_ctx** out) {
-    if (!td || !z || !out) return SLAB_E_ARG;
+    if (!td || !z || !out) {
+        set_thread_error("slab_create: terrain, z and out must not be NULL");
+        return SLAB_E_ARG;
+    }
     *out = nullptr;
     slab_ctx* c = new slab_ctx();
     slab_status s = guard(c, [&] {
@@ -215,6 +218,7 @@ slab_status slab_create(const slab_terrain_desc* td, const double* z, slab_ctx**
         SLAB_CUDA(cudaStreamSynchronize(c->stream));
     });
     if (s != SLAB_OK) {
+        set_thread_error(c->err);  // the context goes: slab_last_error(NULL) keeps the message
         slab_destroy(c);
         return s;
     }

@@ -52,5 +52,6 @@ def test_version_and_status_names_without_gpu():
 def test_null_arguments_are_rejected_without_gpu():
     L = slab.lib()
     assert L.slab_create(None, None, None) == 1
+    assert b"NULL" in L.slab_last_error(None)  # a failed create leaves its message for slab_last_error(NULL)
     assert L.slab_set_params(None, None) == 1
     assert L.slab_advance_steps(None, 1, None) == 1
