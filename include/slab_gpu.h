@@ -6,7 +6,7 @@
  * whose simulate() (src/simulation.cpp:484-522) runs the step loop on the
  * host. This header is the interface that loop is replaced by. Each entry
  * point below names the reference code it stands in for. The C++ class in
- * slab-pro_b200/csrc/simulation.hpp keeps the reference's public Simulation
+ * slab-pro_b200/host/simulation.hpp keeps the reference's public Simulation
  * API and calls these functions from its simulate().
  *
  * Conventions
@@ -53,7 +53,7 @@ typedef enum slab_friction_type { SLAB_COULOMB = 0, SLAB_VOELLMY = 1, SLAB_MU_I 
  *              reference loop and the comparison baseline.
  *  FP32_SPLIT: positions as int32 cell index + FP32 in-cell offset, FP32
  *              particle/grid state, deterministic atomic-free P2G over
- *              cell-sorted particles in sparse 16x16-cell tiles. FP64 only for
+ *              cell-sorted particles in sparse 8x8-cell tiles. FP64 only for
  *              terrain metric terms, conservation sums, time and dt. */
 typedef enum slab_precision { SLAB_FP64_PLAIN = 0, SLAB_FP32_SPLIT = 1 } slab_precision;
 
@@ -87,16 +87,22 @@ typedef struct slab_terrain_desc {
 } slab_terrain_desc;
 
 /* The remeshed grid the reference writes at every frame
- * (src/simulation.cpp:584-642, src/save_function.cpp:96-226). The caller sets
- * the pointers (capacity given in cap_nodes); the call fills Nx, Ny, i_off,
- * j_off and the arrays (flattened i*Ny + j over the Nx x Ny box). */
+ * (src/simulation.cpp:584-642, src/save_function.cpp:96-226), with the
+ * members of class Grid (src/data_arrays.hpp:71-84) as computeGridVelocity
+ * leaves them (src/simulation.cpp:800-875). The caller sets the pointers
+ * (capacity given in cap_nodes; any pointer may be NULL); the call fills Nx,
+ * Ny, i_off, j_off and the arrays (flattened i*Ny + j over the Nx x Ny box).
+ * Every 2-vector field is interleaved (x, y). */
 typedef struct slab_grid_view {
     int32_t Nx, Ny, i_off, j_off;
     int64_t cap_nodes;
-    double* h;
-    double* mass;
-    double* v;  /* interleaved vx,vy */
-    double* vz;
+    double* h;     /* Grid::h, normalised by the node mass */
+    double* mass;  /* Grid::mass */
+    double* v;     /* Grid::v after friction */
+    double* vz;    /* Grid::vz */
+    double* flip;  /* Grid::flip = v - v_old (zero where mass <= 1e-6) */
+    double* F;     /* Grid::F, the P2G force sum */
+    double* a;     /* Grid::a = F / mass (zero where mass <= 1e-6) */
 } slab_grid_view;
 
 typedef struct slab_ctx slab_ctx;
@@ -169,6 +175,14 @@ slab_status slab_download_max(slab_ctx* ctx, double* h_max, double* v_max2);
  * mass of the last step, out[2..3] = particle momentum (x, y). */
 slab_status slab_conservation(slab_ctx* ctx, double out[4]);
 
+/* Particle moments after the last step, all FP64 and summed on the device in
+ * a fixed order: out[0] = total mass, out[1..2] = centre of mass (x, y),
+ * out[3..4] = momentum (x, y), out[5] = kinetic energy sum m |v|^2 / 2. The
+ * centre of mass frame by frame is the trajectory an FP32 run is compared
+ * with an FP64 run on; the reference prints only the total volume
+ * (src/simulation.cpp:473-475). */
+slab_status slab_moments(slab_ctx* ctx, double out[6]);
+
 /* time, dt, frame and steps so far (Simulation members time, dt, frame). */
 slab_status slab_get_state(slab_ctx* ctx, double* time, double* dt, int32_t* frame, int64_t* steps);
 
@@ -208,7 +222,7 @@ void slab_destroy(slab_ctx* ctx);
  * (src/main.cpp:29-57). */
 typedef struct slab_batch slab_batch;
 
-/* capacity_hint: node blocks (16x16 nodes, 9 KB each) to reserve up front,
+/* capacity_hint: node blocks (8x8 nodes, 2.8 KB each) to reserve up front,
  * 0 = automatic; the pool grows as scenarios spread. */
 slab_status slab_batch_create(const slab_terrain_desc* terrain, const double* z, int32_t max_scenarios, int64_t capacity_hint,
                               slab_batch** out);
@@ -228,6 +242,8 @@ slab_status slab_batch_scenario_status(slab_batch* b, int32_t scenario_id);
 slab_status slab_batch_download_particles(slab_batch* b, int32_t scenario_id, double* x_xy, double* v_xy, double* vz, double* h,
                                           double* A, double* mass, double* z);
 slab_status slab_batch_download_max(slab_batch* b, int32_t scenario_id, double* h_max, double* v_max2);
+/* The scenario's particle moments, as slab_moments. */
+slab_status slab_batch_moments(slab_batch* b, int32_t scenario_id, double out[6]);
 /* The node box {i0, i1, j0, j1} a scenario's flow has touched and, when the
  * map pointers are not NULL and the box has at most cap_nodes nodes, h_max
  * and v_max2 over that box ((i-i0)*(j1-j0+1) + (j-j0)); an empty box has
@@ -330,19 +346,28 @@ slab_status slab_poisson_disk(double Lx, double Ly, double r, int32_t k, uint64_
  * dt = 0) with the FP32 split arithmetic, from particle arrays the caller
  * already has on the device, into device arrays the caller provides. It
  * makes no allocation: its scratch is a fixed array compiled into the
- * library (SLAB_STATIC_MAX_NODES nodes, about 3.9 MB per GPU, held by every
- * GPU that loads the library until the process exits).
+ * library (SLAB_STATIC_MAX_NODES nodes, about 3.9 MB per GPU). The array is
+ * reserved on a device when the library's code is first loaded there: under
+ * CUDA's default lazy module loading that is this entry point's first call
+ * on the device (its first launch or symbol lookup), which can then fail
+ * with SLAB_E_CUDA if the heap is already full. Make a first call (Np = 0
+ * will do) before reserving the heap, or set CUDA_MODULE_LOADING=EAGER so
+ * the array is reserved when the library loads. It stays reserved until
+ * the process exits.
  *  - d_z: terrain heights on the device, Nx*Ny, i*Ny + j.
  *  - d_x_xy, d_v_xy (interleaved), d_vz, d_h, d_mass: Np particles.
  *  - box = {i0, i1, j0, j1}: the inclusive node box of the outputs; every
- *    particle's 3x3 stencil must lie inside it, at most
- *    SLAB_STATIC_MAX_NODES nodes (larger boxes are rejected with SLAB_E_ARG).
+ *    particle's 3x3 stencil must lie inside it (else SLAB_E_DOMAIN), at
+ *    most SLAB_STATIC_MAX_NODES nodes (larger boxes are rejected with
+ *    SLAB_E_ARG).
  *  - outputs (device, box nodes, flattened (i-i0)*(j1-j0+1) + (j-j0)):
  *    normalised flow height, grid mass, velocity (interleaved), vz.
- *  - stream: a cudaStream_t or NULL. The call waits for the stream.
- * The first call on a device looks up the device address of the scratch
- * array; make that first call before any stream capture. All calls share
- * the scratch: calls that overlap on the GPU (other threads, other streams)
+ *  - stream: a cudaStream_t or NULL. The call ends by waiting for the
+ *    stream (it reads back an error flag), so it cannot be recorded into a
+ *    CUDA graph by stream capture.
+ * The first call on a device also looks up the device address of the
+ * scratch array. All calls share the scratch and each clears the part it
+ * uses first: calls that overlap on the GPU (other threads, other streams)
  * race and must be serialised by the caller. On error slab_last_error(NULL)
  * gives the message. */
 slab_status slab_initial_grid_static(const slab_terrain_desc* terrain, const double* d_z, const slab_params* params, int32_t Np,

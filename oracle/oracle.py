@@ -69,6 +69,7 @@ def lib():
         L.oracle_get_particles.argtypes = [C.c_void_p] + [dp] * 8
         L.oracle_get_grid_dims.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
         L.oracle_get_grid.argtypes = [C.c_void_p] + [dp] * 5
+        L.oracle_get_grid_force.argtypes = [C.c_void_p, dp, dp]
         L.oracle_get_max.argtypes = [C.c_void_p, dp, dp]
         L.oracle_get_terrain_metrics.argtypes = [C.c_void_p, dp, dp]
         L.oracle_get_ids.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
@@ -158,9 +159,12 @@ class Oracle:
         self.L.oracle_get_grid_dims(self.h, d)
         gNx, gNy, i0, j0 = list(d)
         n = gNx * gNy
-        out = {"h": np.zeros(n), "mass": np.zeros(n), "v": np.zeros(2 * n), "vz": np.zeros(n), "flip": np.zeros(2 * n)}
+        out = {"h": np.zeros(n), "mass": np.zeros(n), "v": np.zeros(2 * n), "vz": np.zeros(n), "flip": np.zeros(2 * n),
+               "F": np.zeros(2 * n), "a": np.zeros(2 * n)}
         self.L.oracle_get_grid(self.h, *[_dp(out[k]) for k in ("h", "mass", "v", "vz", "flip")])
-        g = {k: out[k].reshape(gNx, gNy, -1).squeeze(-1) if k not in ("v", "flip") else out[k].reshape(gNx, gNy, 2) for k in out}
+        self.L.oracle_get_grid_force(self.h, _dp(out["F"]), _dp(out["a"]))
+        vec = ("v", "flip", "F", "a")
+        g = {k: out[k].reshape(gNx, gNy, -1).squeeze(-1) if k not in vec else out[k].reshape(gNx, gNy, 2) for k in out}
         g.update(Nx=gNx, Ny=gNy, i_off=i0, j_off=j0)
         return g
 

@@ -489,6 +489,24 @@ void oracle_get_grid_dims(const oracle_sim* s, int32_t* d) {
     d[3] = s->gj0;
 }
 
+/* Grid::F as P2G leaves it (simulation.cpp:792-793) and Grid::a = F / m_i
+ * where m_i > 1e-6 (simulation.cpp:807-814), zero elsewhere as remesh fills
+ * it (simulation.cpp:626-627). */
+void oracle_get_grid_force(const oracle_sim* s, double* F, double* a) {
+    size_t n = (size_t)s->gNx * s->gNy;
+    for (size_t k = 0; k < n; ++k) {
+        const double m_i = s->gm[k];
+        if (F) {
+            F[2 * k] = s->gFx[k];
+            F[2 * k + 1] = s->gFy[k];
+        }
+        if (a) {
+            a[2 * k] = m_i > 1e-6 ? s->gFx[k] / m_i : 0.0;
+            a[2 * k + 1] = m_i > 1e-6 ? s->gFy[k] / m_i : 0.0;
+        }
+    }
+}
+
 void oracle_get_grid(const oracle_sim* s, double* h, double* mass, double* v, double* vz, double* flip) {
     size_t n = (size_t)s->gNx * s->gNy;
     for (size_t k = 0; k < n; ++k) {

@@ -60,6 +60,9 @@ void oracle_get_particles(const oracle_sim* s, double* x, double* z, double* v, 
 /* grid header: Nx, Ny, i_off, j_off (the remeshed bounding box) */
 void oracle_get_grid_dims(const oracle_sim* s, int32_t* dims4);
 void oracle_get_grid(const oracle_sim* s, double* h, double* mass, double* v, double* vz, double* flip);
+/* Grid::F (P2G force sums) and Grid::a = F / mass over the same box,
+ * interleaved (x, y) */
+void oracle_get_grid_force(const oracle_sim* s, double* F, double* a);
 void oracle_get_max(const oracle_sim* s, double* h_max, double* v_max2);
 /* upload index of each particle in the current (block-sorted) order */
 void oracle_get_ids(const oracle_sim* s, int32_t* ids);

@@ -217,6 +217,14 @@ slab_status slab_batch_download_particles(slab_batch* b, int32_t sid, double* x,
     });
 }
 
+slab_status slab_batch_moments(slab_batch* b, int32_t sid, double out[6]) {
+    if (!b || !out) return SLAB_E_ARG;
+    return bguard(b, [&] {
+        bneed(sid >= 0 && sid < b->E->nscn, SLAB_E_NOTFOUND, "unknown scenario");
+        b->E->moments(sid, out);
+    });
+}
+
 slab_status slab_batch_download_max(slab_batch* b, int32_t sid, double* h_max, double* v_max2) {
     if (!b) return SLAB_E_ARG;
     return bguard(b, [&] {

@@ -350,6 +350,14 @@ slab_status slab_conservation(slab_ctx* c, double out[4]) {
     });
 }
 
+slab_status slab_moments(slab_ctx* c, double out[6]) {
+    if (!c || !out) return SLAB_E_ARG;
+    return guard(c, [&] {
+        need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
+        c->path->moments(out);
+    });
+}
+
 slab_status slab_get_state(slab_ctx* c, double* time, double* dt, int32_t* frame, int64_t* steps) {
     if (!c) return SLAB_E_ARG;
     return guard(c, [&] {

@@ -74,6 +74,18 @@ template <typename R> __device__ __forceinline__ void bspline3(R f, R w[3], R dw
     dw[2] = c;
 }
 
+// Fixed-point P2G sums keep each contribution as an int32 pair: hi, the
+// contribution rounded to the quantum, and lo, the rest below the quantum in
+// units of 2^-L quanta (|lo| <= 2^(L-1)). With at most n contributions to a
+// node, L = min(20, 31 - ceil(log2 n)) keeps every lo sum below 2^30 for any
+// n, so no int32 sum can overflow however many particles share a cell.
+__host__ __device__ inline int lo_bits_for(int n) {
+    int c = 0;
+    while (c < 31 && (1 << c) < n) ++c;  // ceil(log2 n), 0 for n <= 1
+    const int L = 31 - c;
+    return L < 20 ? L : 20;
+}
+
 __device__ __forceinline__ void atomic_max_u64(uint64_t* a, uint64_t v) {
     atomicMax(reinterpret_cast<unsigned long long*>(a), static_cast<unsigned long long>(v));
 }

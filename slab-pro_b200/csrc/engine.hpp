@@ -47,6 +47,19 @@ struct DFree {
 template <typename T> using dptr = std::unique_ptr<T, DFree>;
 template <typename T> dptr<T> dalloc(size_t n) { return dptr<T>(dmalloc<T>(n)); }
 
+// A grid download with no field pointer set only reports the box.
+inline bool grid_view_wants_fields(const slab_grid_view& g) { return g.h || g.mass || g.v || g.vz || g.flip || g.F || g.a; }
+
+// Grid::a = F / m_i where m_i > 1e-6, zero elsewhere, as computeGridVelocity
+// leaves it (src/simulation.cpp:807-814; remesh zero-fills it, :626-627).
+inline void fill_grid_acceleration(double* a, const double* F, const double* m, size_t n) {
+    for (size_t k = 0; k < n; ++k) {
+        const bool moving = m[k] > 1e-6;
+        a[2 * k] = moving ? F[2 * k] / m[k] : 0.0;
+        a[2 * k + 1] = moving ? F[2 * k + 1] / m[k] : 0.0;
+    }
+}
+
 // Terrain metric terms shared by both paths, computed once on the device in
 // FP64 (Simulation::terrainGradients / terrainTheta,
 // src/complex_terrain.cpp:84-111).
@@ -155,6 +168,9 @@ struct Path {
     virtual void download_grid(slab_grid_view* view) = 0;
     virtual void download_max(double* h_max, double* v_max2) = 0;
     virtual void conservation(double out[4]) = 0;
+    // FP64 particle moments: mass, centre of mass (x, y), momentum (x, y),
+    // kinetic energy (moments.cuh)
+    virtual void moments(double out[6]) = 0;
     virtual int64_t launches() const = 0;
     virtual void phase_times(double out[5]) { for (int k = 0; k < 5; ++k) out[k] = 0; }
     virtual void set_profiling(bool) {}

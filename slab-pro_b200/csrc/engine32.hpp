@@ -59,6 +59,8 @@ class Engine32 {
     void download_grid(int sid, slab_grid_view* gv);
     void download_max(int sid, double* hmax, double* vmax2);
     void conservation(int sid, double out[4], double rho);
+    void moments(int sid, double out[6]);
+    dptr<double> d_mom;  // moment partials and result (moments.cuh)
     Shared shared() const;
 
     const Terrain& T;
@@ -128,7 +130,7 @@ class Engine32 {
     std::vector<float> gather_nodes(int sid, int stepid, int i0, int j0, int nI, int nJ, const std::vector<const float*>& fields,
                                     bool with_v);
     dptr<float4> d_nv;
-    dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz;
+    dptr<float> d_hmax, d_vmax2, d_oh, d_om, d_ovz, d_oFx, d_oFy;
     dptr<int32_t> d_blk_stamp, d_blk_owner, d_misc, d_work_pref, d_gflat, d_wlist, d_free_blocks;
     dptr<Scn> d_scn;
     dptr<SCnt> d_cnt;

@@ -127,6 +127,12 @@ __global__ void k_bounds(int* s, PartIn P, int Np, const double* z, int Nx, int 
     }
 }
 
+// bits below one quantum kept by a lo word: a node adds at most 9 * s[7]
+// contributions (9 cells, s[7] particles in the fullest), each lo part at
+// most 2^(L-1) in magnitude, so L = 31 - ceil(log2(9 s[7])) (at most 20)
+// keeps every lo sum below 2^30
+__device__ __forceinline__ int lo_bits(const int* s) { return lo_bits_for(9 * s[7]); }
+
 __device__ __forceinline__ float scale_of(const int* s, int q, float* inv) {
     const float bound = 9.f * (float)s[7] * 0.75f * __uint_as_float((unsigned)s[q]);
     int e = 0;
@@ -144,6 +150,7 @@ __device__ __forceinline__ float scale_of(const int* s, int q, float* inv) {
 __global__ void k_p2g(int* s, PartIn P, int Np, const double* z, int Nx, int Ny, double dx, float g, Box b) {
     float sc[SQ], inv;
     for (int q = 0; q < SQ; ++q) sc[q] = scale_of(s, q, &inv);
+    const float lo_mul = ldexpf(1.f, lo_bits(s));
     int* hi = s + HDR + MAXN;
     int* lo = hi + (size_t)SQ * MAXN;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < Np; p += gridDim.x * blockDim.x) {
@@ -165,7 +172,7 @@ __global__ void k_p2g(int* s, PartIn P, int Np, const double* z, int Nx, int Ny,
                     const float xs = v[q] * sc[q];
                     const int h_ = __float2int_rn(xs);
                     atomicAdd(&hi[(size_t)q * MAXN + nd], h_);
-                    const int l_ = __float2int_rn((xs - (float)h_) * 1048576.f);
+                    const int l_ = __float2int_rn((xs - (float)h_) * lo_mul);
                     if (l_) atomicAdd(&lo[(size_t)q * MAXN + nd], l_);
                 }
             }
@@ -177,13 +184,14 @@ __global__ void k_p2g(int* s, PartIn P, int Np, const double* z, int Nx, int Ny,
 __global__ void k_grid(const int* s, Box b, double* out_h, double* out_m, double* out_v, double* out_vz) {
     float inv[SQ];
     for (int q = 0; q < SQ; ++q) scale_of(s, q, &inv[q]);
+    const double lo_div = ldexp(1.0, -lo_bits(s));
     const int* hi = s + HDR + MAXN;
     const int* lo = hi + (size_t)SQ * MAXN;
     const int n = b.nI * b.nJ;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         float q[SQ];
         for (int r = 0; r < SQ; ++r)
-            q[r] = (float)(((double)hi[(size_t)r * MAXN + k] + (double)lo[(size_t)r * MAXN + k] * (1.0 / 1048576.0)) * (double)inv[r]);
+            q[r] = (float)(((double)hi[(size_t)r * MAXN + k] + (double)lo[(size_t)r * MAXN + k] * lo_div) * (double)inv[r]);
         const float mi = q[0];
         float hn = 0.f, vzn = 0.f, vx = 0.f, vy = 0.f;
         if (mi > 1e-6f) {
@@ -223,12 +231,16 @@ extern "C" slab_status slab_initial_grid_static(const slab_terrain_desc* terrain
         !d_vz_out)
         return fail(SLAB_E_ARG, "slab_initial_grid_static: null argument");
     if (Np < 0) return fail(SLAB_E_ARG, "slab_initial_grid_static: Np < 0");
-    const int nI = box[1] - box[0] + 1, nJ = box[3] - box[2] + 1;
-    if (box[0] < 0 || box[2] < 0 || box[1] > terrain->Nx - 1 || box[3] > terrain->Ny - 1 || nI < 3 || nJ < 3)
+    if (terrain->Nx < 3 || terrain->Ny < 3 || !(terrain->dx > 0.0))
+        return fail(SLAB_E_ARG, "slab_initial_grid_static: terrain smaller than 3x3 nodes or dx <= 0");
+    // extents in 64 bits: box values straight from the caller cannot overflow
+    const int64_t nI64 = (int64_t)box[1] - box[0] + 1, nJ64 = (int64_t)box[3] - box[2] + 1;
+    if (box[0] < 0 || box[2] < 0 || box[1] > terrain->Nx - 1 || box[3] > terrain->Ny - 1 || nI64 < 3 || nJ64 < 3)
         return fail(SLAB_E_ARG, "slab_initial_grid_static: box outside the terrain or smaller than 3x3 nodes");
-    if ((int64_t)nI * nJ > SLAB_STATIC_MAX_NODES)
-        return fail(SLAB_E_ARG, "slab_initial_grid_static: box has " + std::to_string((int64_t)nI * nJ) + " nodes, the maximum is " +
+    if (nI64 * nJ64 > SLAB_STATIC_MAX_NODES)
+        return fail(SLAB_E_ARG, "slab_initial_grid_static: box has " + std::to_string(nI64 * nJ64) + " nodes, the maximum is " +
                                     std::to_string(SLAB_STATIC_MAX_NODES));
+    const int nI = (int)nI64, nJ = (int)nJ64;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64) return fail(SLAB_E_CUDA, "slab_initial_grid_static: no usable CUDA device");

@@ -12,6 +12,7 @@
 #include <cstring>
 
 #include "engine.hpp"
+#include "moments.cuh"
 
 namespace slab {
 namespace {
@@ -25,7 +26,23 @@ struct N64 {
     double *m, *px, *py, *pvz, *hm, *Fx, *Fy;  // P2G accumulators (zero between steps)
     double2 *v, *flip;                          // grid velocity and FLIP increment of the last step
     double *out_h, *out_m, *out_vz;             // normalised grid fields for output frames
+    double *out_Fx, *out_Fy;                    // the P2G force sums of output frames (Grid::F)
     double *h_max, *v_max2;                     // Grid::h_max / Grid::v_max2 of the terrain
+};
+
+// position, velocity and mass of particle p, for the moments reduction
+struct PlainParticle {
+    const double2* x;
+    const double2* v;
+    const double* m;
+    __device__ void operator()(int p, double& px, double& py, double& vx, double& vy, double& mass) const {
+        const double2 a = x[p], b = v[p];
+        px = a.x;
+        py = a.y;
+        vx = b.x;
+        vy = b.y;
+        mass = m[p];
+    }
 };
 
 struct Phys {
@@ -162,6 +179,8 @@ __global__ void __launch_bounds__(256) k64_grid(Ctl* c, N64 n, const double2* __
             n.out_h[k] = hn;
             n.out_m[k] = mi;
             n.out_vz[k] = vzn;
+            n.out_Fx[k] = n.Fx[k];
+            n.out_Fy[k] = n.Fy[k];
         }
         n.m[k] = 0.0;
         n.px[k] = 0.0;
@@ -302,7 +321,7 @@ struct Plain64 final : Path {
     dptr<double> vz, h, A, m, z;
     dptr<double> acc;  // 7 accumulators, each Nx*Ny
     dptr<double2> gv, gflip;
-    dptr<double> out3;  // out_h, out_m, out_vz
+    dptr<double> out5;  // out_h, out_m, out_vz, out_Fx, out_Fy
     dptr<double> maxes; // h_max, v_max2
     int64_t nlaunch = 0;
     StepGraphs graphs;
@@ -329,12 +348,12 @@ struct Plain64 final : Path {
         acc = dalloc<double>(7 * nn);
         gv = dalloc<double2>(nn);
         gflip = dalloc<double2>(nn);
-        out3 = dalloc<double>(3 * nn);
+        out5 = dalloc<double>(5 * nn);
         maxes = dalloc<double>(2 * nn);
         SLAB_CUDA(cudaMemsetAsync(acc.get(), 0, 7 * nn * sizeof(double), st));
         SLAB_CUDA(cudaMemsetAsync(gv.get(), 0, nn * sizeof(double2), st));
         SLAB_CUDA(cudaMemsetAsync(gflip.get(), 0, nn * sizeof(double2), st));
-        SLAB_CUDA(cudaMemsetAsync(out3.get(), 0, 3 * nn * sizeof(double), st));
+        SLAB_CUDA(cudaMemsetAsync(out5.get(), 0, 5 * nn * sizeof(double), st));
         SLAB_CUDA(cudaMemsetAsync(maxes.get(), 0, 2 * nn * sizeof(double), st));
     }
 
@@ -342,9 +361,9 @@ struct Plain64 final : Path {
     N64 nodes() {
         const size_t nn = (size_t)T.Nx * T.Ny;
         double* a = acc.get();
-        double* o = out3.get();
+        double* o = out5.get();
         return N64{a, a + nn, a + 2 * nn, a + 3 * nn, a + 4 * nn, a + 5 * nn, a + 6 * nn, gv.get(), gflip.get(),
-                   o, o + nn, o + 2 * nn, maxes.get(), maxes.get() + nn};
+                   o, o + nn, o + 2 * nn, o + 3 * nn, o + 4 * nn, maxes.get(), maxes.get() + nn};
     }
 
     void upload(int np, const double* hx, const double* hv, const double* hvz, const double* hh, const double* hA, const double* hm,
@@ -437,18 +456,44 @@ struct Plain64 final : Path {
         gv_->Ny = gNy;
         gv_->i_off = i0;
         gv_->j_off = j0;
-        if (!gv_->h && !gv_->mass && !gv_->v && !gv_->vz) return;  // box only
+        if (!grid_view_wants_fields(*gv_)) return;  // box only
         if ((int64_t)gNx * gNy > gv_->cap_nodes) throw Error{SLAB_E_ARG, "grid view capacity too small"};
         N64 n = nodes();
-        std::vector<double> row(2 * (size_t)gNy);
+        // Grid::a = F / mass needs both, whichever of them the caller asked for
+        std::vector<double> Fh, mh;
+        double* Fdst = gv_->F;
+        double* mdst = gv_->mass;
+        if (gv_->a && !Fdst) {
+            Fh.resize(2 * (size_t)gNx * gNy);
+            Fdst = Fh.data();
+        }
+        if (gv_->a && !mdst) {
+            mh.resize((size_t)gNx * gNy);
+            mdst = mh.data();
+        }
+        std::vector<double> fy;
+        if (Fdst) fy.resize((size_t)gNx * gNy);
         for (int i = 0; i < gNx; ++i) {
             const size_t src = (size_t)(i0 + i) * T.Ny + j0, dst = (size_t)i * gNy;
             if (gv_->h) SLAB_CUDA(cudaMemcpyAsync(gv_->h + dst, n.out_h + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
-            if (gv_->mass) SLAB_CUDA(cudaMemcpyAsync(gv_->mass + dst, n.out_m + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (mdst) SLAB_CUDA(cudaMemcpyAsync(mdst + dst, n.out_m + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
             if (gv_->vz) SLAB_CUDA(cudaMemcpyAsync(gv_->vz + dst, n.out_vz + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
             if (gv_->v) SLAB_CUDA(cudaMemcpyAsync(gv_->v + 2 * dst, n.v + src, gNy * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            if (gv_->flip) SLAB_CUDA(cudaMemcpyAsync(gv_->flip + 2 * dst, n.flip + src, gNy * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            if (Fdst) {  // x components into place, y components beside them, interleaved below
+                SLAB_CUDA(cudaMemcpyAsync(Fdst + dst, n.out_Fx + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
+                SLAB_CUDA(cudaMemcpyAsync(fy.data() + dst, n.out_Fy + src, gNy * sizeof(double), cudaMemcpyDeviceToHost, st));
+            }
         }
         SLAB_CUDA(cudaStreamSynchronize(st));
+        const size_t nn = (size_t)gNx * gNy;
+        if (Fdst) {
+            for (size_t k = nn; k-- > 0;) {
+                Fdst[2 * k] = Fdst[k];
+                Fdst[2 * k + 1] = fy[k];
+            }
+        }
+        if (gv_->a) fill_grid_acceleration(gv_->a, Fdst, mdst, nn);
     }
 
     void download_max(double* hmax, double* vmax2) override {
@@ -480,6 +525,17 @@ struct Plain64 final : Path {
         out[1] = G;
         out[2] = Px;
         out[3] = Py;
+    }
+
+    dptr<double> mom;
+    void moments(double out[6]) override {
+        if (!mom) mom = dalloc<double>((size_t)MOM_BLOCKS * MOM_N + MOM_N);
+        k_moments<<<MOM_BLOCKS, MOM_THREADS, 0, st>>>(Np, PlainParticle{x.get(), v.get(), m.get()}, mom.get());
+        k_moments_final<<<1, MOM_THREADS, 0, st>>>(mom.get(), mom.get() + (size_t)MOM_BLOCKS * MOM_N);
+        nlaunch += 2;
+        SLAB_CUDA(cudaGetLastError());
+        SLAB_CUDA(cudaMemcpyAsync(out, mom.get() + (size_t)MOM_BLOCKS * MOM_N, MOM_N * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SLAB_CUDA(cudaStreamSynchronize(st));
     }
 
     int64_t launches() const override { return nlaunch; }

@@ -13,6 +13,7 @@
 #include "engine.hpp"
 #include "engine32.hpp"
 #include "split32_kernels.cuh"
+#include "moments.cuh"
 
 namespace slab {
 
@@ -65,10 +66,12 @@ __global__ void k_gather_nodes(const int32_t* __restrict__ blk_of, const int32_t
         const bool ok = blk >= 0 && (stepid < 0 || blk_stamp[blk] == stepid);
         const size_t n = (size_t)blk * NCELL + (i % TILE) * TILE + (j % TILE);
         for (int q = 0; q < nf; ++q) out[q * total + k] = ok ? fields[q][n] : 0.f;
-        if (nv) {
+        if (nv) {  // velocity and FLIP increment
             const float4 v = ok ? nv[n] : make_float4(0.f, 0.f, 0.f, 0.f);
             out[nf * total + k] = v.x;
             out[(nf + 1) * total + k] = v.y;
+            out[(nf + 2) * total + k] = v.z;
+            out[(nf + 3) * total + k] = v.w;
         }
     }
 }
@@ -87,6 +90,8 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     d_oh = dalloc<float>((size_t)this->blk_cap * NCELL);
     d_om = dalloc<float>((size_t)this->blk_cap * NCELL);
     d_ovz = dalloc<float>((size_t)this->blk_cap * NCELL);
+    d_oFx = dalloc<float>((size_t)this->blk_cap * NCELL);
+    d_oFy = dalloc<float>((size_t)this->blk_cap * NCELL);
     d_blk_stamp = dalloc<int32_t>(this->blk_cap);
     d_blk_owner = dalloc<int32_t>(this->blk_cap);
     d_misc = dalloc<int32_t>(8);
@@ -157,6 +162,8 @@ Shared Engine32::shared() const {
     sh.oh = d_oh.get();
     sh.om = d_om.get();
     sh.ovz = d_ovz.get();
+    sh.oFx = d_oFx.get();
+    sh.oFy = d_oFy.get();
     sh.blk_stamp = d_blk_stamp.get();
     sh.blk_owner = d_blk_owner.get();
     sh.blk_count = d_misc.get();
@@ -755,6 +762,8 @@ void Engine32::grow_blocks(int cap) {
     grow(d_oh, NCELL, 0);
     grow(d_om, NCELL, 0);
     grow(d_ovz, NCELL, 0);
+    grow(d_oFx, NCELL, 0);
+    grow(d_oFy, NCELL, 0);
     grow(d_blk_stamp, 1, 0xff);
     grow(d_blk_owner, 1, 0xff);
     grow(d_free_blocks, 1, 0);
@@ -808,7 +817,7 @@ std::vector<float> Engine32::gather_nodes(int sid, int stepid, int i0, int j0, i
                                           bool with_v) {
     Store& S = (*slots[sid]);
     const int64_t total = (int64_t)nI * nJ;
-    const int nout = (int)fields.size() + (with_v ? 2 : 0);
+    const int nout = (int)fields.size() + (with_v ? 4 : 0);
     std::vector<float> host((size_t)nout * total);
     if (total == 0) return host;
     // scratch kept between calls (downloads at every retirement must not allocate)
@@ -838,17 +847,33 @@ void Engine32::download_grid(int sid, slab_grid_view* gv) {
     gv->Ny = gNy;
     gv->i_off = i0;
     gv->j_off = j0;
-    if (!gv->h && !gv->mass && !gv->v && !gv->vz) return;  // box only
+    if (!grid_view_wants_fields(*gv)) return;  // box only
     if ((int64_t)gNx * gNy > gv->cap_nodes) throw Error{SLAB_E_ARG, "grid view capacity too small"};
-    const std::vector<float> f = gather_nodes(sid, c.stepid, i0, j0, gNx, gNy, {d_oh.get(), d_om.get(), d_ovz.get()}, true);
+    const std::vector<float> f =
+        gather_nodes(sid, c.stepid, i0, j0, gNx, gNy, {d_oh.get(), d_om.get(), d_ovz.get(), d_oFx.get(), d_oFy.get()}, true);
     const size_t n = (size_t)gNx * gNy;
+    const float *fh = f.data(), *fm = fh + n, *fvz = fm + n, *fFx = fvz + n, *fFy = fFx + n, *fvx = fFy + n, *fvy = fvx + n,
+                *flx = fvy + n, *fly = flx + n;
     for (size_t k = 0; k < n; ++k) {
-        if (gv->h) gv->h[k] = f[k];
-        if (gv->mass) gv->mass[k] = f[n + k];
-        if (gv->vz) gv->vz[k] = f[2 * n + k];
+        if (gv->h) gv->h[k] = fh[k];
+        if (gv->mass) gv->mass[k] = fm[k];
+        if (gv->vz) gv->vz[k] = fvz[k];
         if (gv->v) {
-            gv->v[2 * k] = f[3 * n + k];
-            gv->v[2 * k + 1] = f[4 * n + k];
+            gv->v[2 * k] = fvx[k];
+            gv->v[2 * k + 1] = fvy[k];
+        }
+        if (gv->flip) {
+            gv->flip[2 * k] = flx[k];
+            gv->flip[2 * k + 1] = fly[k];
+        }
+        if (gv->F) {
+            gv->F[2 * k] = fFx[k];
+            gv->F[2 * k + 1] = fFy[k];
+        }
+        if (gv->a) {  // the FP32 quotient of the grid update, F / m (src/simulation.cpp:814)
+            const bool moving = fm[k] > 1e-6f;
+            gv->a[2 * k] = moving ? (double)(fFx[k] / fm[k]) : 0.0;
+            gv->a[2 * k + 1] = moving ? (double)(fFy[k] / fm[k]) : 0.0;
         }
     }
 }
@@ -892,6 +917,41 @@ void Engine32::conservation(int sid, double out[4], double rho) {
 }
 
 namespace {
+// position (from the split cell + offset), velocity and mass of particle p of
+// a buffer, for the moments reduction
+struct SplitParticle {
+    const int32_t* cell;
+    const float2* f;
+    const float2* v;
+    const float* m;
+    double dx;
+    __device__ void operator()(int p, double& x, double& y, double& vx, double& vy, double& mass) const {
+        const int32_t c = cell[p];
+        const float2 fp = f[p], vp = v[p];
+        x = ((double)cell_i(c) + (double)fp.x) * dx;
+        y = ((double)cell_j(c) + (double)fp.y) * dx;
+        vx = vp.x;
+        vy = vp.y;
+        mass = m[p];
+    }
+};
+}  // namespace
+
+void Engine32::moments(int sid, double out[6]) {
+    Store& S = (*slots[sid]);
+    const SCnt c = counters(sid);
+    const int b = c.seq & 1;  // the buffer the last G2P wrote
+    if (!d_mom) d_mom = dalloc<double>((size_t)MOM_BLOCKS * MOM_N + MOM_N);
+    const SplitParticle get{S.cell[b].get(), S.f[b].get(), S.v[b].get(), S.m[b].get(), T.dx};
+    k_moments<<<MOM_BLOCKS, MOM_THREADS, 0, st>>>(S.Np, get, d_mom.get());
+    k_moments_final<<<1, MOM_THREADS, 0, st>>>(d_mom.get(), d_mom.get() + (size_t)MOM_BLOCKS * MOM_N);
+    nlaunch += 2;
+    SLAB_CUDA(cudaGetLastError());
+    d2h(out, d_mom.get() + (size_t)MOM_BLOCKS * MOM_N, MOM_N, st);
+    SLAB_CUDA(cudaStreamSynchronize(st));
+}
+
+namespace {
 
 // The single-scenario FP32 path behind slab_ctx.
 struct Split32 final : Path {
@@ -919,6 +979,7 @@ struct Split32 final : Path {
     void download_grid(slab_grid_view* gv) override { E.download_grid(sid, gv); }
     void download_max(double* hm, double* vm) override { E.download_max(sid, hm, vm); }
     void conservation(double out[4]) override { E.conservation(sid, out, prm.rho); }
+    void moments(double out[6]) override { E.moments(sid, out); }
     int64_t launches() const override { return E.nlaunch; }
     void set_profiling(bool on) override {
         E.timer.collect();

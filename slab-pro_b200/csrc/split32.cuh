@@ -121,6 +121,8 @@ struct Shared {
     float* oh;         // output fields (frame steps)
     float* om;
     float* ovz;
+    float* oFx;        // P2G force sums (Grid::F) of frame steps
+    float* oFy;
     int32_t* blk_stamp;   // stepid of the last grid update of the block
     int32_t* blk_owner;   // scenario of the block
     int32_t* blk_count;

@@ -473,6 +473,9 @@ __global__ void __launch_bounds__(P2G_THREADS, P2G_MIN_BLOCKS) k_p2g(Shared sh, 
         __syncthreads();
         const float s0 = sm.scale[0], s1 = sm.scale[1], s2 = sm.scale[2], s3 = sm.scale[3], s4 = sm.scale[4], s5 = sm.scale[5],
                     s6 = sm.scale[6];
+        const int lob = lo_bits_for(9 * sm.mcc);  // lo sums of a node stay below 2^30
+        const float lo_mul = ldexpf(1.f, lob);
+        const double lo_div = ldexp(1.0, -lob);
         // pass B: fixed-point contributions
         for (int k = tid; k < ncand; k += P2G_THREADS) {
             int d;
@@ -505,7 +508,7 @@ __global__ void __launch_bounds__(P2G_THREADS, P2G_MIN_BLOCKS) k_p2g(Shared sh, 
                                 const int hi = __float2int_rn(x);
                                 atomicAdd(node32 + q * TN * TN + nd, hi);
                                 if (ACC == ACC_HILO) {
-                                    const int lo = __float2int_rn((x - (float)hi) * 1048576.f);
+                                    const int lo = __float2int_rn((x - (float)hi) * lo_mul);
                                     if (lo) atomicAdd(node32 + (NQ + q) * TN * TN + nd, lo);
                                 }
                             }
@@ -520,7 +523,7 @@ __global__ void __launch_bounds__(P2G_THREADS, P2G_MIN_BLOCKS) k_p2g(Shared sh, 
             const float is = sm.iscale[k / (TN * TN)];
             float v;
             if (ACC == ACC_I64) v = (float)((double)sm.node[k] * (double)is);
-            else if (ACC == ACC_HILO) v = (float)(((double)node32[k] + (double)node32[NQ * TN * TN + k] * (1.0 / 1048576.0)) * (double)is);
+            else if (ACC == ACC_HILO) v = (float)(((double)node32[k] + (double)node32[NQ * TN * TN + k] * lo_div) * (double)is);
             else v = (float)node32[k] * is;
             P[k] = v;
         }
@@ -658,6 +661,9 @@ __global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh, int cls)
             sc[q] = ldexpf(1.f, e);
             isc[q] = ldexpf(1.f, -e);
         }
+        const int lob = lo_bits_for(9 * mcc);  // lo sums of a node stay below 2^30
+        const float lo_mul = ldexpf(1.f, lob);
+        const double lo_div = ldexp(1.0, -lob);
         // pass B: fixed-point contributions
         for (int c = 0, k0 = 0; k0 < ncand; ++c, k0 += 32) {
             const int k = k0 + lane;
@@ -692,7 +698,7 @@ __global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh, int cls)
                             const float x = cq[q] * sc[q];
                             const int h_ = __float2int_rn(x);
                             atomicAdd(hi + q * TN * TN + nd, h_);
-                            const int l_ = __float2int_rn((x - (float)h_) * 1048576.f);
+                            const int l_ = __float2int_rn((x - (float)h_) * lo_mul);
                             if (l_) atomicAdd(lo + q * TN * TN + nd, l_);
                         }
                     }
@@ -707,7 +713,7 @@ __global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh, int cls)
 #pragma unroll
             for (int r = 1; r < NQ; ++r)
                 if (q == r) is = isc[r];
-            P[k] = (float)(((double)hi[k] + (double)lo[k] * (1.0 / 1048576.0)) * (double)is);
+            P[k] = (float)(((double)hi[k] + (double)lo[k] * lo_div) * (double)is);
         }
         __syncwarp();
     }
@@ -1213,6 +1219,9 @@ __global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shar
         __syncthreads();
         // pass B: (particle, stencil row) items
         const int nv = min(sm.nv, P2S_CAP);
+        const int lob = lo_bits_for(9 * sm.mcc);  // lo sums of a node stay below 2^30 (20 bits for <= 64 particles)
+        const float lo_mul = ldexpf(1.f, lob);
+        const double lo_div = ldexp(1.0, -lob);
         for (int it = tid; it < 3 * nv; it += P2S_THREADS) {
             const int pi = it / 3, a = it - 3 * pi;
             const PQ p = sm.pq[pi];
@@ -1234,7 +1243,7 @@ __global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shar
                         const float x = cq[q] * sm.scale[q];
                         const int h_ = __float2int_rn(x);
                         atomicAdd(sm.hi + q * TN * TN + nd, h_);
-                        const int l_ = __float2int_rn((x - (float)h_) * 1048576.f);
+                        const int l_ = __float2int_rn((x - (float)h_) * lo_mul);
                         if (l_) atomicAdd(sm.lo + q * TN * TN + nd, l_);
                     }
                 }
@@ -1243,7 +1252,7 @@ __global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shar
         __syncthreads();
         float* P = sh.part + (size_t)w * PART_STRIDE;
         for (int k = tid; k < PART_STRIDE; k += P2S_THREADS)
-            P[k] = (float)(((double)sm.hi[k] + (double)sm.lo[k] * (1.0 / 1048576.0)) * (double)sm.iscale[k / (TN * TN)]);
+            P[k] = (float)(((double)sm.hi[k] + (double)sm.lo[k] * lo_div) * (double)sm.iscale[k / (TN * TN)]);
         __syncthreads();
         if (i + 1 < i1 && tid < DESC_WORDS) reinterpret_cast<int*>(&sm.d)[tid] = dn;
         w_cur = w_nxt;
@@ -1423,8 +1432,10 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
             sh.nv[bn] = out;
             if (Z.outs) {
                 sh.oh[bn] = hn;
-                sh.om[bn] = (i < sh.Nx && j < sh.Ny) ? mi : 0.f;
+                sh.om[bn] = inside ? mi : 0.f;
                 sh.ovz[bn] = vzn;
+                sh.oFx[bn] = inside ? q[4] : 0.f;
+                sh.oFy[bn] = inside ? q[5] : 0.f;
             }
         }
         // FP64 grid mass and active-node count of this tile (fixed-order block reduction)

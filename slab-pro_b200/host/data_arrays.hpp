@@ -94,23 +94,29 @@ class Grid {
         y.assign(ny, 0.0);
         v.assign(n, Vec2());
         vz.assign(n, 0.0);
+        a.assign(n, Vec2());
         mass.assign(n, 0.0);
+        F.assign(n, Vec2());
         z.assign(n, 0.0);
         h.assign(n, 0.0);
         h_max.assign(n, 0.0);
         v_max2.assign(n, 0.0);
         gradients.assign(n, Vec2());
+        flip.assign(n, Vec2());
         theta.assign(n, 0.0);
     }
     std::vector<T> x, y;
     std::vector<Vec2> v;
     std::vector<T> vz;
+    std::vector<Vec2> a;  // F / mass, without friction
     std::vector<T> mass;
+    std::vector<Vec2> F;  // P2G force sum
     std::vector<T> z;
     std::vector<T> h;
     std::vector<T> h_max;
     std::vector<T> v_max2;
     std::vector<Vec2> gradients;
+    std::vector<Vec2> flip;  // v - v_old: the FLIP increment, friction included
     std::vector<T> theta;
     T xllcorner = 0.0, yllcorner = 0.0;
     int Nx = 0, Ny = 0;

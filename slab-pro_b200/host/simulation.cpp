@@ -483,6 +483,9 @@ void Simulation::pull_frame() {
     gv.mass = grid.mass.data();
     gv.v = gv.cap_nodes ? &grid.v[0](0) : nullptr;
     gv.vz = grid.vz.data();
+    gv.flip = gv.cap_nodes ? &grid.flip[0](0) : nullptr;
+    gv.F = gv.cap_nodes ? &grid.F[0](0) : nullptr;
+    gv.a = gv.cap_nodes ? &grid.a[0](0) : nullptr;
     if (gv.cap_nodes > 0) check(slab_download_grid(ctx, &gv), ctx, "slab_download_grid");
 }
 

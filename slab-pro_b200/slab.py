@@ -48,7 +48,8 @@ class TerrainDesc(C.Structure):
 class GridView(C.Structure):
     _fields_ = [("Nx", C.c_int32), ("Ny", C.c_int32), ("i_off", C.c_int32), ("j_off", C.c_int32), ("cap_nodes", C.c_int64),
                 ("h", C.POINTER(C.c_double)), ("mass", C.POINTER(C.c_double)), ("v", C.POINTER(C.c_double)),
-                ("vz", C.POINTER(C.c_double))]
+                ("vz", C.POINTER(C.c_double)), ("flip", C.POINTER(C.c_double)), ("F", C.POINTER(C.c_double)),
+                ("a", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -76,6 +77,8 @@ def lib():
         L.slab_download_grid.argtypes = [vp, C.POINTER(GridView)]
         L.slab_download_max.argtypes = [vp, dp, dp]
         L.slab_conservation.argtypes = [vp, dp]
+        L.slab_moments.argtypes = [vp, dp]
+        L.slab_batch_moments.argtypes = [vp, C.c_int32, dp]
         L.slab_get_state.argtypes = [vp, dp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
         L.slab_set_profiling.argtypes = [vp, C.c_int32]
         L.slab_get_phase_times.argtypes = [vp, dp]
@@ -200,13 +203,19 @@ class Slab:
         return out
 
     def grid(self) -> dict:
-        cap = self.Nx * self.Ny
-        bufs = {k: np.zeros(2 * cap if k == "v" else cap) for k in ("h", "mass", "v", "vz")}
-        gv = GridView(0, 0, 0, 0, cap, _dp(bufs["h"]), _dp(bufs["mass"]), _dp(bufs["v"]), _dp(bufs["vz"]))
+        """The last step's grid over the remeshed box: the members of the
+        reference's Grid (h, mass, vz; v, flip, F, a as [Nx, Ny, 2])."""
+        box = GridView()
+        self._check(self.L.slab_download_grid(self.h, C.byref(box)))
+        cap = max(1, box.Nx * box.Ny)
+        vec = ("v", "flip", "F", "a")
+        bufs = {k: np.zeros(2 * cap if k in vec else cap) for k in ("h", "mass", "v", "vz", "flip", "F", "a")}
+        gv = GridView(0, 0, 0, 0, cap, *[_dp(bufs[k]) for k in ("h", "mass", "v", "vz", "flip", "F", "a")])
         self._check(self.L.slab_download_grid(self.h, C.byref(gv)))
         n = gv.Nx * gv.Ny
         g = {k: bufs[k][:n].reshape(gv.Nx, gv.Ny) for k in ("h", "mass", "vz")}
-        g["v"] = bufs["v"][:2 * n].reshape(gv.Nx, gv.Ny, 2)
+        for k in vec:
+            g[k] = bufs[k][:2 * n].reshape(gv.Nx, gv.Ny, 2)
         g.update(Nx=gv.Nx, Ny=gv.Ny, i_off=gv.i_off, j_off=gv.j_off)
         return g
 
@@ -220,6 +229,13 @@ class Slab:
         out = np.zeros(4)
         self._check(self.L.slab_conservation(self.h, _dp(out)))
         return out
+
+    def moments(self) -> dict:
+        """FP64 particle moments summed on the device: mass, centre of mass,
+        momentum, kinetic energy."""
+        out = np.zeros(6)
+        self._check(self.L.slab_moments(self.h, _dp(out)))
+        return {"mass": out[0], "com": out[1:3].copy(), "momentum": out[3:5].copy(), "kinetic": out[5]}
 
     def state(self):
         t, dt, f, s = C.c_double(), C.c_double(), C.c_int32(), C.c_int64()
@@ -333,6 +349,11 @@ class Batch:
         out["x"] = out["x"].reshape(n, 2)
         out["v"] = out["v"].reshape(n, 2)
         return out
+
+    def moments(self, sid: int) -> dict:
+        out = np.zeros(6)
+        self._check(self.L.slab_batch_moments(self.h, sid, _dp(out)))
+        return {"mass": out[0], "com": out[1:3].copy(), "momentum": out[3:5].copy(), "kinetic": out[5]}
 
     def max_maps(self, sid: int):
         hm = np.zeros(self.Nx * self.Ny)

@@ -165,3 +165,34 @@ def test_ply_roundtrip(tmp_path):
     assert list(r) == ["x", "y", "vx", "vy", "vz", "z", "h", "A"]
     for k, a in (("x", x[:, 0]), ("y", x[:, 1]), ("vx", v[:, 0]), ("vy", v[:, 1]), ("vz", vz), ("z", z), ("h", h), ("A", A)):
         assert np.array_equal(r[k], a.astype(np.float32)), k
+
+
+def test_reference_style_caller_reads_grid_members(tmp_path):
+    """A caller written against the reference's Grid (src/data_arrays.hpp:71-84)
+    that reads grid.a, grid.F and grid.flip compiles and links against
+    libslab_sim.so; the members resize with the grid."""
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include "simulation.hpp"
+#include <cstdio>
+int main() {
+    slab::Grid g(3, 4);
+    g.flip[5](0) = 1.0;
+    g.F[5](1) = 2.0;
+    g.a[5] = g.F[5];
+    slab::Simulation sim;
+    const slab::Grid& cur = sim.getGrid();
+    std::printf("%zu %zu %zu %zu %g %g %g\n", g.a.size(), g.F.size(), g.flip.size(), cur.flip.size(), g.flip[5](0), g.F[5](1),
+                g.a[5](1));
+    return 0;
+}
+''')
+    exe = tmp_path / "caller"
+    inc = [f"-I{os.path.join(ROOT, 'include')}", f"-I{os.path.join(ROOT, 'slab-pro_b200', 'host')}"]
+    libdir = os.path.dirname(SIMLIB)
+    r = subprocess.run(["g++", "-std=c++17", *inc, str(src), "-o", str(exe), f"-L{libdir}", "-lslab_sim", "-lslab_gpu",
+                        f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.split() == ["12", "12", "12", "0", "1", "2", "2"]
