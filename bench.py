@@ -62,12 +62,13 @@ def log(*a):
 
 
 def load_workload(name: str):
-    import slab
+    """The named workload, generated with numpy only (no library of this
+    repository is loaded, so the reference arm maps none)."""
     import workloads as W
     if name == "c1":
         return W.config1()
     if name == "c2":
-        return W.config2(sampler=slab.poisson_disk)
+        return W.config2()
     if name == "c3":
         return W.config3()
     raise SystemExit(f"unknown workload {name}")
@@ -212,6 +213,62 @@ def run_reference(c, P, nsteps, replicas, warmup=0):
     return sum(steps) * Np / tmax, steps[0], tmax
 
 
+def record_run(z, dx, cfg, P, prec, stream, perturb=0.0, seed=0):
+    """One scenario from t=0 to total_time through a context, frame by frame:
+    the FP64 centre of mass at t=0 and at every output frame (slab_moments),
+    the h_max and max-speed maps over the wet box, the total particle mass at
+    the start and the end, steps and wall seconds. perturb > 0 moves every
+    starting position by a seeded uniform offset of up to perturb * dx in
+    each coordinate (the FP64 sensitivity envelope)."""
+    import slab
+    import accuracy as Acc
+    if perturb > 0.0:
+        rng = np.random.default_rng(seed)
+        P = dict(P, x=P["x"] + dx * perturb * rng.uniform(-1.0, 1.0, P["x"].shape))
+    s = slab.Slab(z, dx)
+    s.set_stream(stream.cuda_stream)
+    s.set_params(cfg, prec)
+    w0 = time.perf_counter()
+    s.upload(P)
+    s.initial_pass()
+    m0 = s.moments()
+    com, steps = [m0["com"]], 0
+    while True:
+        t, _, k = s.advance_to_frame()
+        steps += k
+        mo = s.moments()
+        com.append(mo["com"])
+        if t >= cfg["total_time"] or k == 0:
+            break
+    hm, vm = s.max_maps()
+    wall = time.perf_counter() - w0
+    s.close()
+    box = Acc.wet_box(hm)
+    crop = (lambda m: m[box[0]:box[1] + 1, box[2]:box[3] + 1].copy()) if box[1] >= box[0] else (lambda m: np.zeros((0, 0)))
+    return {"box": box, "h_max": crop(hm), "v_max": np.sqrt(crop(vm)), "com": np.array(com), "mass": m0["mass"],
+            "mass_end": mo["mass"], "steps": steps, "wall_s": wall}
+
+
+def accuracy_block(z, dx, cfg, P, stream, envelope=True):
+    """FP32_SPLIT against FP64_PLAIN over a whole run of one scenario, and
+    beside it the FP64 envelope: FP64_PLAIN against FP64_PLAIN started from
+    positions moved by up to 1e-7 dx (the resolution of the FP32 split
+    position)."""
+    import slab
+    import accuracy as Acc
+    r64 = record_run(z, dx, cfg, P, slab.FP64_PLAIN, stream)
+    r32 = record_run(z, dx, cfg, P, slab.FP32_SPLIT, stream)
+    out = {"fp32_vs_fp64": Acc.compare_runs(r32, r64, dx),
+           "steps": {"fp64": r64["steps"], "fp32": r32["steps"]},
+           "mass_drift_rel": {"fp64": abs(r64["mass_end"] - r64["mass"]) / r64["mass"],
+                              "fp32": abs(r32["mass_end"] - r32["mass"]) / r32["mass"]},
+           "wall_s": {"fp64": round(r64["wall_s"], 2), "fp32": round(r32["wall_s"], 2)}}
+    if envelope:
+        rp = record_run(z, dx, cfg, P, slab.FP64_PLAIN, stream, perturb=1e-7, seed=11)
+        out["fp64_envelope"] = Acc.compare_runs(rp, r64, dx)
+    return out
+
+
 def ours(args, rank, world):
     import torch
     import slab
@@ -238,7 +295,6 @@ def ours(args, rank, world):
         s.initial_pass()
         return s
 
-    spin = int(round(args.spinup / cfg["dt_max"]))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def timed(s, K, profile=False):
@@ -270,31 +326,44 @@ def ours(args, rank, world):
             s.set_profiling(False)
         return ms, wall, (w1[0] - w0[0], w1[1] - w0[1]), s.kernel_launches() - l0, phases
 
-    # ---- FP32 split path (the product)
+    def spin_to(s, t_target):
+        """advance until the simulated time reaches t_target (developed flow)"""
+        while s.state()[0] < t_target - 1e-9:
+            if s.advance_steps(max(1, int(round((t_target - s.state()[0]) / cfg["dt_max"])))) == 0:
+                break
+
+    # ---- FP32 split path (the product): W warm-up steps from the workload's
+    # initial state, then K timed steps -- the state the reference arm times
     s32 = make(slab.FP32_SPLIT)
-    s32.advance_steps(spin)
     s32.advance_steps(args.warmup)
     with ClockSampler(dev) as clk:
         ms, wall, work, launches, _ = timed(s32, args.steps)
     assert work[0] == Np * args.steps, work
     ms_prof, _, work_prof, _, phases = timed(s32, args.steps, profile=True)
     shapes, tunes = s32.launch_shapes()
-    state = s32.particles()
+    # the same after the flow has developed (spin-up to args.spinup simulated seconds)
+    spin_to(s32, args.spinup)
+    ms_dev, _, work_dev, _, phases_dev = timed(s32, args.steps, profile=True)
     t32 = s32.state()[0]
+    s32.close()
     if args.only == "fp32":
         if rank == 0:
             return {"metric": METRIC, "value": round(Np * args.steps / (ms * 1e-3), 1), "unit": METRIC, "n_gpus": world,
                     "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
                     "config": {"workload": c["name"], "particles": Np, "only": "fp32"},
-                    "phases_ms": [round(p / args.steps, 5) for p in phases], "gpu_launches": int(launches)}
+                    "phases_ms": [round(p / args.steps, 5) for p in phases],
+                    "developed": {"sim_time_s": round(t32, 3), "ms_per_step": round(ms_dev / args.steps, 5),
+                                  "phases_ms": [round(p / args.steps, 5) for p in phases_dev],
+                                  "active_nodes_per_step": work_dev[1] / args.steps},
+                    "active_nodes_per_step": work_prof[1] / args.steps, "gpu_launches": int(launches)}
         return None
 
     # ---- plain FP64 path on the same schedule
     s64 = make(slab.FP64_PLAIN)
-    s64.advance_steps(spin)
     s64.advance_steps(args.warmup)
     ms64, _, work64, _, _ = timed(s64, args.steps)
-    state64 = s64.particles()
+    spin_to(s64, args.spinup)
+    ms64_dev, _, _, _, _ = timed(s64, args.steps)
     s64.close()
 
     # ---- max over ranks
@@ -309,18 +378,23 @@ def ours(args, rank, world):
     if rank != 0:
         return None
 
-    # ---- roofline of the dominant kernel (profiled pass, same schedule)
+    # ---- roofline of the dominant kernel (profiled pass, same state)
     peak, peak_kind = measured_peak()
     names = {1: "prep", 2: "p2g", 3: "grid", 4: "g2p"}
-    nodes_per_step = work_prof[1] / args.steps
-    per_kernel = {}
-    for idx, nm in names.items():
-        t_ms = phases[idx] / args.steps
-        bp, bn = KERNEL_BYTES[nm]
-        bytes_launch = bp * Np + bn * nodes_per_step
-        per_kernel[nm] = {"ms": round(t_ms, 5), "algorithmic_bytes": int(bytes_launch),
-                          "gbs": round(bytes_launch / (t_ms * 1e-3) / 1e9, 1) if t_ms > 0 else None,
-                          "share": round(phases[idx] / max(sum(phases), 1e-12), 3)}
+
+    def per_kernel_of(ph, wk):
+        nodes = wk[1] / args.steps
+        out = {}
+        for idx, nm in names.items():
+            t_ms = ph[idx] / args.steps
+            bp, bn = KERNEL_BYTES[nm]
+            bytes_launch = bp * Np + bn * nodes
+            out[nm] = {"ms": round(t_ms, 5), "algorithmic_bytes": int(bytes_launch),
+                       "gbs": round(bytes_launch / (t_ms * 1e-3) / 1e9, 1) if t_ms > 0 else None,
+                       "share": round(ph[idx] / max(sum(ph), 1e-12), 3)}
+        return out, nodes
+
+    per_kernel, nodes_per_step = per_kernel_of(phases, work_prof)
     dom = max(("p2g", "grid", "g2p"), key=lambda k: per_kernel[k]["ms"])
     ach = per_kernel[dom]["gbs"]
     traffic = None
@@ -334,28 +408,27 @@ def ours(args, rank, world):
                 "whole_step": {"algorithmic_bytes": int(BYTES_P * Np + BYTES_N * nodes_per_step),
                                "gbs": round((BYTES_P * Np + BYTES_N * nodes_per_step) / (step_ms * 1e-3) / 1e9, 1)},
                 "per_kernel": per_kernel, "active_nodes_per_step": round(nodes_per_step, 1)}
+    pk_dev, nodes_dev = per_kernel_of(phases_dev, work_dev)
 
     # ---- CPU baseline: the reference's own step loop, 1 core, same state
     cpu = None
     if not args.no_cpu:
         try:
-            Pref = dict(state64)
-            Pref["theta"] = np.zeros(Np)
+            Pref = dict(P0)
             k_cpu = max(3, int(args.cpu_seconds * 8e6 / Np))
-            v_cpu, st_cpu, sec_cpu = run_reference(c, Pref, k_cpu, 1)
+            v_cpu, st_cpu, sec_cpu = run_reference(c, Pref, k_cpu, 1, warmup=args.warmup)
             cpu = {"value": round(v_cpu, 1), "unit": METRIC, "cores": 1, "kind": "reference",
-                   "sample": f"{st_cpu} steps of the same {Np}-particle scenario from the same developed state, "
-                             f"reference step-loop sources (oracle/_ref/slab_ref), per-phase timers, {sec_cpu:.1f} s"}
+                   "sample": f"{st_cpu} steps after {args.warmup} warm-up steps from the workload's initial state, "
+                             f"{Np} particles, reference step-loop sources (oracle/_ref/slab_ref), per-phase timers, {sec_cpu:.1f} s"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
     # ---- e2e through the public API with host buffers
     K_e2e = args.e2e_steps
-    hb = {k: np.ascontiguousarray(state[k]) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
+    hb = {k: np.ascontiguousarray(P0[k]) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
     e = slab.Slab(c["z"], c["dx"])
     e.set_stream(stream.cuda_stream)
     e.set_params(cfg, slab.FP32_SPLIT)
-    hm = np.zeros(c["z"].shape)
     e2e_times = []
     for it in range(2):
         torch.cuda.synchronize()
@@ -373,6 +446,7 @@ def ours(args, rank, world):
            "window": f"upload + t=0 pass + {K_e2e} steps + particle and max-map download, host FP64 arrays, best of 2; "
                      f"d2h counts the host arrays returned (the library copies only the node box the flow touched of the max maps)"}
     e.close()
+    del hmx, out
 
     clocks = clk.summary()
     line = {
@@ -380,19 +454,36 @@ def ours(args, rank, world):
         "ms_per_step": round(ms_all / args.steps, 5), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (f64 dt, time, metric terms, sums)", "data": "synthetic",
         "config": {"workload": c["name"], "particles": Np, "dem": list(c["z"].shape), "dx": c["dx"],
-                   "friction": c["cfg"]["friction"], "spinup_s": args.spinup, "l2": "flushed between timed steps (256 MiB write)",
+                   "friction": c["cfg"]["friction"], "state": f"{args.warmup} warm-up steps from the initial state",
+                   "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "fp64_plain": {"value": round(Np * args.steps / (ms64 * 1e-3), 1), "ms_per_step": round(ms64 / args.steps, 5),
                        "fp32_speedup": round(ms64 / ms, 2)},
+        "developed": {"sim_time_s": round(t32, 3), "value": round(Np * args.steps / (ms_dev * 1e-3), 1),
+                      "ms_per_step": round(ms_dev / args.steps, 5), "fp64_plain_ms_per_step": round(ms64_dev / args.steps, 5),
+                      "fp32_speedup": round(ms64_dev / ms_dev, 2), "active_nodes_per_step": round(nodes_dev, 1),
+                      "per_kernel": pk_dev},
         "gpu_launches": int(launches),
         "launch_shapes": {"ctas": dict(zip(("prep", "p2g_dense", "p2g_sparse", "grid", "g2p"), shapes)), "tuning_passes": tunes},
         "clocks": clocks,
         "wall_s_timed": round(wall, 4),
-        "sim_time_s": round(t32, 4),
     }
+    if world == 1 and not args.no_accuracy:
+        try:
+            acc = accuracy_block(c["z"], c["dx"], c["cfg"], P0, stream, envelope=not args.no_envelope)
+            line["accuracy"] = dict(acc, workload=c["name"])
+        except Exception as ex:
+            line["accuracy"] = {"error": f"{type(ex).__name__}: {ex}"}
+        if args.workload != "c2" and not args.no_c2_accuracy:
+            try:
+                c2 = load_workload("c2")
+                line["accuracy_c2"] = dict(accuracy_block(c2["z"], c2["dx"], c2["cfg"], c2["particles"], stream), workload=c2["name"],
+                                           particles=len(c2["particles"]["h"]))
+            except Exception as ex:
+                line["accuracy_c2"] = {"error": f"{type(ex).__name__}: {ex}"}
     if world == 1 and not args.no_ensemble and args.only != "serving":
         try:
             line["ensemble"] = ensemble(args, stream, dev)
@@ -537,7 +628,7 @@ def serving(args, stream, dev):
     import workloads as W
     g0 = time.perf_counter()
     dx = 0.5
-    z = W.fractal_slope_dem(8192, dx, seed=2027, rms=7.5)
+    z = W.config3_dem()
     reqs = W.config5_stream(z, dx, args.c5_window)
     gen_s = time.perf_counter() - g0
     n = len(reqs)
@@ -623,14 +714,45 @@ def serving(args, stream, dev):
     return out
 
 
+def ref_process_bytes(c) -> int:
+    """Host memory one reference process needs: its terrain Grid holds 17
+    doubles per DEM node (src/data_arrays.hpp:49-93), its particles 84 B each,
+    its remeshed grid about 4 nodes per particle at 136 B, plus input copies."""
+    nodes = c["z"].size
+    Np = len(c["particles"]["h"])
+    return int(1.2 * (144 * nodes + 84 * Np + 4 * 136 * Np + 8 * nodes + 100 * Np))
+
+
+def host_available_bytes() -> int:
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def repo_libraries_loaded() -> list:
+    """Shared libraries of this repository mapped into this process."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {ln.split()[-1] for ln in f if ln.rstrip().endswith(".so")}
+    except OSError:
+        return []
+    return sorted(os.path.relpath(p, ROOT) for p in paths if p.startswith(ROOT + os.sep))
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return None
-    import slab  # noqa: F401 (sampler for the workload)
     c = load_workload(args.workload)
     P = dict(c["particles"])
     Np = len(P["h"])
-    replicas = max(1, min(os.cpu_count() or 1, args.ref_procs))
+    avail = host_available_bytes()
+    by_mem = max(1, int(0.7 * avail // ref_process_bytes(c))) if avail else 1
+    replicas = max(1, min(os.cpu_count() or 1, args.ref_procs, by_mem))
     k = max(2, min(args.steps, int(args.cpu_seconds * 8e6 / Np)))
     w = max(0, args.warmup)
     t0 = time.perf_counter()
@@ -640,12 +762,14 @@ def reference_arm(args, rank, world):
             "warmup": w, "ms_per_step": round(sec / max(st, 1) * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": c["name"], "particles": Np, "dem": list(c["z"].shape), "dx": c["dx"],
-                       "friction": c["cfg"]["friction"], "parallelism": f"{replicas} concurrent single-threaded processes"},
+                       "friction": c["cfg"]["friction"], "state": f"{w} warm-up steps from the initial state",
+                       "parallelism": f"{replicas} concurrent single-threaded processes"},
             "cpu_baseline": {"value": round(v, 1), "unit": METRIC, "cores": replicas, "kind": "reference",
-                             "sample": f"{w} untimed and {st} timed steps from t=0 per process, {replicas} processes, "
-                                       f"the reference's per-phase timers "
-                                       f"(slowest {sec:.1f} s, wall {wall:.1f} s)"},
-            "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": f"{w} untimed and {st} timed steps from the workload's initial state per process, "
+                                       f"{replicas} processes (host cores {os.cpu_count()}, memory bound {by_mem}), "
+                                       f"the reference's per-phase timers (slowest {sec:.1f} s, wall {wall:.1f} s)"},
+            "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "repo_libraries_loaded": repo_libraries_loaded()}
 
 
 def main():
@@ -654,8 +778,11 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
-    ap.add_argument("--spinup", type=float, default=2.0, help="simulated seconds before timing")
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--spinup", type=float, default=2.0, help="simulated seconds of the developed-flow measurement")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 whole-run accuracy blocks")
+    ap.add_argument("--no-envelope", action="store_true", help="skip the FP64 envelope run of the headline accuracy block")
+    ap.add_argument("--no-c2-accuracy", action="store_true", help="skip the config-2 accuracy block")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-procs", type=int, default=8)

@@ -54,3 +54,44 @@ def compare_max_heights(box_a, ha: np.ndarray, box_b, hb: np.ndarray, dx: float)
     return {"wet_nodes": int(wet.sum()), "within_1cm_1pct": float(ok[wet].mean()) if wet.any() else 1.0,
             "max_abs_m": float(np.abs(A - B).max()) if A.size else 0.0,
             "runout_diff_m": float(abs(runout(A, dx, i0=u[0]) - runout(B, dx, i0=u[0])))}
+
+
+def v_ok(va: np.ndarray, vb: np.ndarray) -> np.ndarray:
+    """Nodes whose max speeds agree within 0.1 m/s or 1 %."""
+    return np.abs(va - vb) <= np.maximum(0.1, 0.01 * np.maximum(va, vb))
+
+
+def compare_runs(a: dict, b: dict, dx: float) -> dict:
+    """Run a against run b, both {"box", "h_max", "v_max" (speeds, over box),
+    "com" [frames, 2], "mass"}: the max-flow-height map (fraction of wet
+    nodes within 1 cm / 1 %, largest difference), the max-velocity map
+    (fraction within 0.1 m/s / 1 %, largest difference), the runout
+    difference in cells, the largest centre-of-mass distance over the output
+    frames, and the relative difference of the total masses."""
+    u = [min(a["box"][0], b["box"][0]), max(a["box"][1], b["box"][1]), min(a["box"][2], b["box"][2]),
+         max(a["box"][3], b["box"][3])]
+    ha, hb = crop(a["box"], a["h_max"], u), crop(b["box"], b["h_max"], u)
+    va, vb = crop(a["box"], a["v_max"], u), crop(b["box"], b["v_max"], u)
+    wet = (ha > 0) | (hb > 0)
+    n = min(len(a["com"]), len(b["com"]))
+    dcom = np.linalg.norm(np.asarray(a["com"])[:n] - np.asarray(b["com"])[:n], axis=1) if n else np.zeros(1)
+    return {"wet_nodes": int(wet.sum()),
+            "h_within_1cm_1pct": float(h_ok(ha, hb)[wet].mean()) if wet.any() else 1.0,
+            "h_max_abs_m": float(np.abs(ha - hb).max()) if ha.size else 0.0,
+            "v_within_01ms_1pct": float(v_ok(va, vb)[wet].mean()) if wet.any() else 1.0,
+            "v_max_abs_ms": float(np.abs(va - vb).max()) if va.size else 0.0,
+            "runout_diff_cells": float(abs(runout(ha, dx, i0=u[0]) - runout(hb, dx, i0=u[0])) / dx),
+            "com_max_m": float(dcom.max()), "com_final_m": float(dcom[-1]) if n else 0.0, "frames": int(n),
+            "mass_rel": float(abs(a["mass"] - b["mass"]) / b["mass"]) if b["mass"] else 0.0}
+
+
+def summarize(rows: list) -> dict:
+    """Worst case over scenarios of compare_runs results."""
+    if not rows:
+        return {}
+    worst = {"h_within_1cm_1pct": min, "h_max_abs_m": max, "v_within_01ms_1pct": min, "v_max_abs_ms": max,
+             "runout_diff_cells": max, "com_max_m": max, "mass_rel": max}
+    out = {k: f(r[k] for r in rows) for k, f in worst.items()}
+    out["scenarios"] = len(rows)
+    out["median_h_within_1cm_1pct"] = float(np.median([r["h_within_1cm_1pct"] for r in rows]))
+    return out

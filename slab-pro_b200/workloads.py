@@ -250,10 +250,17 @@ def analytical_plane(Lx: float, Ly: float, dx: float):
 
 
 def fractal_slope_dem(n: int, dx: float, seed: int, rms: float = 15.0, hurst: float = 0.8, lowpass_m: float = 20.0,
-                      x_plane_end: float = 2500.0, ease_m: float = 500.0, steep_deg: float = 30.0, flat_deg: float = 5.0):
+                      x_plane_end: float = 2500.0, ease_m: float = 500.0, steep_deg: float = 30.0, flat_deg: float = 5.0,
+                      rim_m: float = 0.0, rim_deg: float = 25.0):
     """Planar 30-degree slope for x < 2500 m easing (smoothstep in tan) to a
     5-degree runout over 500 m, plus seeded fBm roughness: spectrum
-    PSD ~ k^-(2H+2), wavelengths shorter than lowpass_m removed, scaled to rms."""
+    PSD ~ k^-(2H+2), wavelengths shorter than lowpass_m removed, scaled to rms.
+
+    rim_m > 0 adds a containing rim: the runout turns into a rim_deg
+    counter-slope over the last rim_m metres in x, and rim_deg walls rise
+    over the rim_m metres next to each y edge, so that no flow released
+    away from them leaves the terrain (the reference indexes outside its
+    arrays when one does, src/simulation.cpp:603-641)."""
     rng = np.random.default_rng(seed)
     L = n * dx
     x = np.arange(n) * dx
@@ -273,10 +280,63 @@ def fractal_slope_dem(n: int, dx: float, seed: int, rms: float = 15.0, hurst: fl
     ph = rng.standard_normal(K.shape) + 1j * rng.standard_normal(K.shape)
     rough = np.fft.irfft2(amp * ph, s=(n, n))
     rough *= rms / max(rough.std(), 1e-30)
-    return zx[:, None] + rough
+    z = zx[:, None] + rough
+    if rim_m > 0.0:
+        t = math.tan(math.radians(rim_deg))
+        z += (t * np.clip(x - (L - dx - rim_m), 0.0, None))[:, None]
+        dist = np.minimum(x, (n - 1) * dx - x)  # y nodes: the same spacing
+        z += (t * np.clip(rim_m - dist, 0.0, None))[None, :]
+    return z
 
 
 # ----------------------------------------------------------- releases
+
+
+def poisson_disk_np(Lx: float, Ly: float, r: float, seed: int, rounds: int = 4) -> np.ndarray:
+    """Poisson-disk samples in [0, Lx] x [0, Ly] with minimum distance r, by
+    parallel dart throwing (numpy, seeded): a background grid of cells of
+    edge r/sqrt(2) holds at most one sample each; the cells are visited in 9
+    phase groups (i mod 3, j mod 3), whose cells are more than r apart, so
+    one candidate per empty cell of a group can be tested against the
+    accepted samples of its 5 x 5 neighbourhood all at once. `rounds` passes
+    over the groups. Positions are relative to the lower-left corner, like
+    the reference's sampler (src/poisson_disk_sampling.hpp:23-134) returns
+    them; the sample set is a different one of the same kind."""
+    rng = np.random.default_rng(seed)
+    a = r / math.sqrt(2.0)
+    nx, ny = int(math.ceil(Lx / a)), int(math.ceil(Ly / a))
+    W = ny + 4  # row length of the grid with a 2-cell border of empty cells
+    g = np.full(((nx + 4) * W, 2), np.nan)
+    ci_all, cj_all = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    ci_all, cj_all = ci_all.ravel(), cj_all.ravel()
+    grp = (ci_all % 3) * 3 + (cj_all % 3)
+    flat_all = (ci_all + 2) * W + (cj_all + 2)
+    groups = [np.nonzero(grp == k)[0] for k in range(9)]
+    offs = np.array([di * W + dj for di in range(-2, 3) for dj in range(-2, 3) if (di, dj) != (0, 0)])
+    r2 = r * r
+    for _ in range(rounds):
+        added = 0
+        for k in range(9):
+            idx = groups[k]
+            idx = idx[np.isnan(g[flat_all[idx], 0])]
+            groups[k] = idx  # filled cells leave the group for good
+            if not len(idx):
+                continue
+            px = (ci_all[idx] + rng.random(len(idx))) * a
+            py = (cj_all[idx] + rng.random(len(idx))) * a
+            ok = (px <= Lx) & (py <= Ly)
+            f = flat_all[idx]
+            for o in offs:
+                q = g[f + o]
+                d2 = (q[:, 0] - px) ** 2 + (q[:, 1] - py) ** 2
+                ok &= ~(d2 < r2)  # NaN (empty cell) compares false
+            g[f[ok], 0] = px[ok]
+            g[f[ok], 1] = py[ok]
+            added += int(ok.sum())
+        if added == 0:
+            break
+    keep = ~np.isnan(g[flat_all, 0])
+    return g[flat_all[keep]]
 
 
 def star_polygon(seed: int, center, ax: float, ay: float, nvert: int = 12):
@@ -324,6 +384,10 @@ def lognormal_release_raster(seed: int, poly, cellsize: float, median: float = 1
 
 # ------------------------------------------------------------ configs
 
+# containing rim of the benchmark DEMs (fractal_slope_dem rim_m): metres of
+# counter-slope at the far x end and of side wall at each y edge
+RIM_M = 300.0
+
 
 def config1():
     """35-degree slope with circular-arc runout, 1 600 particles, Coulomb."""
@@ -335,16 +399,16 @@ def config1():
     return {"name": "slope35_arc_401x101_dx5", "z": z, "dx": 5.0, "cfg": cfg, "release": rel, "particles": P}
 
 
-def config2(seed: int = 2026, sampler=None):
+def config2(seed: int = 2026, sampler=poisson_disk_np):
     """4096^2 DEM at 1 m (30-degree slope easing to 5 degrees + fBm roughness,
     Hurst 0.8, 15 m RMS, wavelengths < 20 m removed), seeded 12-vertex
     star-convex release polygon with ~500 x 300 m semi-axes rasterised with
     lognormal heights (median 1.5 m, sigma_log 0.4, h_min 0.2 m), POISSON
     sampling at r = 0.5 m (~0.55-0.6 M particles), Voellmy mu=0.2 xi=1500,
-    total_time 120 s. `sampler(Lx, Ly, r, seed)` must return Poisson-disk
-    samples (slab.poisson_disk)."""
+    total_time 120 s. `sampler(Lx, Ly, r, seed)` returns the Poisson-disk
+    samples (default: poisson_disk_np, numpy only)."""
     dx = 1.0
-    z = fractal_slope_dem(4096, dx, seed=seed)
+    z = fractal_slope_dem(4096, dx, seed=seed, rim_m=RIM_M)
     poly = star_polygon(seed + 1, center=(700.0, 2048.0), ax=500.0, ay=300.0)
     rel = lognormal_release_raster(seed + 2, poly, cellsize=dx)
     rel["h_min"] = 0.2
@@ -358,13 +422,18 @@ def config2(seed: int = 2026, sampler=None):
     return {"name": "fractal4096_dx1_star_poisson_voellmy", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}
 
 
+def config3_dem(seed: int = 2027):
+    """The 8192^2, 0.5 m DEM of config 3 (and of the served stream, config 5)."""
+    return fractal_slope_dem(8192, 0.5, seed=seed, rms=7.5, rim_m=RIM_M)
+
+
 def config3(seed: int = 2027):
     """8192^2 DEM at 0.5 m (same construction, roughness amplitude scaled to
     7.5 m RMS), 1200 x 800 m ellipse h0 = 3 m, UNIFORM 2x2 sampling
     (~12 M particles), mu(I) (0.38, 0.64, 0.279, d 0.5 mm, phi 0.6), rho 1500,
     total_time 90 s."""
     dx = 0.5
-    z = fractal_slope_dem(8192, dx, seed=seed, rms=7.5)
+    z = config3_dem(seed)
     cfg = dict(gravity=9.81, rho=1500.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=90.0,
                friction="MU_I", mui_mu1=0.38, mui_mu2=0.64, mui_I0=0.279, mui_d=5e-4, mui_phi=0.6)
     rel = {"type": "ELLIPSE", "center": (800.0, 2048.0), "rx": 600.0, "ry": 400.0, "rotation_deg": 0.0, "h0": 3.0}
@@ -381,7 +450,7 @@ def config4(n_scenarios: int = 256, seed: int = 2028):
     slope case (rho 300, C_cfl 0.5, dt_max 0.01 s, flip_ratio 0.95)."""
     dx = 2.0
     n = 2048
-    z = fractal_slope_dem(n, dx, seed=seed, rms=7.5)
+    z = fractal_slope_dem(n, dx, seed=seed, rms=7.5, rim_m=RIM_M)
     gn = terrain_gradient_norm(z, dx)
     rng = np.random.default_rng(seed + 1)
     L = n * dx
@@ -391,7 +460,7 @@ def config4(n_scenarios: int = 256, seed: int = 2028):
         rot = rng.uniform(0.0, 180.0)
         r = max(rx, ry) + 4 * dx
         cx = rng.uniform(r, max(r + 1.0, L / 3.0))
-        cy = rng.uniform(r, L - r)
+        cy = rng.uniform(r + RIM_M, L - r - RIM_M)  # clear of the side walls
         cfg = dict(gravity=9.81, rho=300.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=60.0,
                    friction="VOELLMY", voellmy_mu=float(rng.uniform(0.1, 0.4)), voellmy_xi=float(rng.uniform(500.0, 3000.0)))
         rel = {"type": "ELLIPSE", "center": (float(cx), float(cy)), "rx": float(rx), "ry": float(ry), "rotation_deg": float(rot),
@@ -424,7 +493,7 @@ def config5_stream(z: np.ndarray, dx: float, window_s: float, seed: int = 2029, 
         ry = area / (math.pi * rx)
         r = max(rx, ry) + 4 * dx
         cx = rng.uniform(r, max(r + 1.0, L / 3.0))
-        cy = rng.uniform(r, z.shape[1] * dx - r)
+        cy = rng.uniform(r + RIM_M, z.shape[1] * dx - r - RIM_M)  # clear of the side walls
         law = ["COULOMB", "VOELLMY", "MU_I"][int(rng.integers(3))]
         cfg = dict(gravity=9.81, rho=1500.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0,
                    total_time=float(rng.uniform(*t_range)), friction=law)

@@ -33,3 +33,4 @@ def test_reference_arm_prints_one_json_line():
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    assert d["repo_libraries_loaded"] == []  # the reference arm runs none of this repository's native code
