@@ -167,6 +167,38 @@ slab_status slab_download_particles(slab_ctx* ctx, double* x_xy, double* v_xy, d
  * the box (Nx, Ny, i_off, j_off) is filled in, to size the buffers. */
 slab_status slab_download_grid(slab_ctx* ctx, slab_grid_view* view);
 
+/* ---- output frames without stopping the step loop ----------------------
+ * The reference writes particles_frame_N.ply and rasters_frame_N.tif at every
+ * output frame from the host loop (src/simulation.cpp:496-497, 504-509;
+ * src/save_function.cpp:36-226). Here a frame is packed on the device into
+ * the files' own float32 layouts, copied to pinned host memory on a separate
+ * copy stream while the next frame's steps run, and handed to the caller's
+ * writer. Two slots: a capture into a slot first waits for that slot's
+ * previous copy, and the caller must be done reading a slot's view before
+ * capturing into it again. */
+typedef struct slab_frame {
+    int32_t frame;     /* output frame counter (Simulation::frame) */
+    int32_t Np;
+    double time;
+    /* Np vertices of 8 float32: x y vx vy vz z h A, in upload order -- the
+     * vertex layout of particles_frame_N.ply (src/save_function.cpp:44-75) */
+    const float* particles;
+    /* the frame's remeshed grid box (as slab_download_grid) and its 6 float32
+     * bands h, |v|, m, vx, vy, vz of Nx*Ny values each in GeoTIFF order: row
+     * 0 is the north edge (j = Ny - 1), x fastest; all bands -9999 where
+     * h == 0 (src/save_function.cpp:96-226) */
+    int32_t Nx, Ny, i_off, j_off;
+    const float* grid;
+} slab_frame;
+
+/* Pack the current state (after slab_initial_pass or an advance call that
+ * ended on a frame) into slot (0 or 1) and start its copy to the host; returns
+ * without waiting for the copy. */
+slab_status slab_frame_capture(slab_ctx* ctx, int32_t slot);
+/* Wait for the slot's copy and fill *out; the pointers stay valid until the
+ * slot is captured again or the context is destroyed. */
+slab_status slab_frame_wait(slab_ctx* ctx, int32_t slot, slab_frame* out);
+
 /* Full-terrain maxima (Grid::h_max, Grid::v_max2), as written by
  * Simulation::saveMaxData (src/save_function.cpp:228-291). Nx*Ny each. */
 slab_status slab_download_max(slab_ctx* ctx, double* h_max, double* v_max2);

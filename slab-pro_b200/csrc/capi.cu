@@ -16,6 +16,18 @@ static thread_local std::string t_last_error;
 void set_thread_error(const std::string& msg) { t_last_error = msg; }
 }  // namespace slab
 
+// One output frame in flight (slab_frame_capture / slab_frame_wait): the
+// packed frame on the device, its pinned host copy, and the event that marks
+// the end of the copy.
+struct FrameSlot {
+    dptr<float> dev;
+    float* host = nullptr;  // pinned
+    size_t cap = 0;         // floats in both buffers
+    cudaEvent_t packed = nullptr, copied = nullptr;
+    bool pending = false;   // a copy was started and not yet waited for
+    slab_frame meta{};
+};
+
 struct slab_ctx {
     Terrain terrain;
     slab_params params{};
@@ -32,6 +44,8 @@ struct slab_ctx {
     std::string err;
     int64_t extra_launches = 0;
     int chunk = 32;
+    cudaStream_t copy_stream = nullptr;  // frame copies to the host
+    FrameSlot frames[2];
 };
 
 namespace {
@@ -350,6 +364,82 @@ slab_status slab_conservation(slab_ctx* c, double out[4]) {
     });
 }
 
+slab_status slab_frame_capture(slab_ctx* c, int32_t slot) {
+    if (!c) return SLAB_E_ARG;
+    return guard(c, [&] {
+        need(slot == 0 || slot == 1, SLAB_E_ARG, "frame slot must be 0 or 1");
+        need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
+        need(c->initial_done, SLAB_E_STATE, "call slab_initial_pass before capturing a frame");
+        pull_ctl(c);
+        raise_device_errors(c);
+        FrameSlot& F = c->frames[slot];
+        if (F.pending) {  // this slot's previous copy must be over before its buffers are reused
+            SLAB_CUDA(cudaEventSynchronize(F.copied));
+            F.pending = false;
+        }
+        const int32_t* box = c->h_ctl->box;
+        const int64_t nI = (int64_t)box[1] - box[0] + 1, nJ = (int64_t)box[3] - box[2] + 1;
+        const int64_t nodes = nI > 0 && nJ > 0 ? nI * nJ : 0;
+        const size_t need_f = (size_t)c->Np * 8 + (size_t)nodes * 6;
+        if (need_f > F.cap) {
+            if (F.host) cudaFreeHost(F.host);
+            F.host = nullptr;
+            F.cap = 0;
+            F.dev = dalloc<float>(need_f);
+            void* h = nullptr;
+            SLAB_CUDA(cudaMallocHost(&h, need_f * sizeof(float)));
+            F.host = static_cast<float*>(h);
+            F.cap = need_f;
+        }
+        if (!F.packed) {
+            SLAB_CUDA(cudaEventCreateWithFlags(&F.packed, cudaEventDisableTiming));
+            SLAB_CUDA(cudaEventCreateWithFlags(&F.copied, cudaEventDisableTiming));
+        }
+        if (!c->copy_stream) SLAB_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        c->path->pack_frame(F.dev.get(), F.dev.get() + (size_t)c->Np * 8, box);
+        // the copy runs on its own stream, beside the steps enqueued after this call
+        SLAB_CUDA(cudaEventRecord(F.packed, c->stream));
+        SLAB_CUDA(cudaStreamWaitEvent(c->copy_stream, F.packed, 0));
+        SLAB_CUDA(cudaMemcpyAsync(F.host, F.dev.get(), need_f * sizeof(float), cudaMemcpyDeviceToHost, c->copy_stream));
+        SLAB_CUDA(cudaEventRecord(F.copied, c->copy_stream));
+        F.pending = true;
+        slab_frame& m = F.meta;
+        m.frame = c->h_ctl->frame;
+        m.Np = c->Np;
+        m.time = c->h_ctl->time;
+        m.particles = F.host;
+        m.Nx = (int32_t)nI;
+        m.Ny = (int32_t)nJ;
+        m.i_off = box[0];
+        m.j_off = box[2];
+        m.grid = F.host + (size_t)c->Np * 8;
+    });
+}
+
+slab_status slab_frame_wait(slab_ctx* c, int32_t slot, slab_frame* out) {
+    // touches only the slot, so a writer thread may call it while another
+    // thread advances the context; its error message goes to this thread's
+    // slab_last_error(NULL)
+    if (!c || !out || (slot != 0 && slot != 1)) {
+        set_thread_error("slab_frame_wait: null argument or slot not 0/1");
+        return SLAB_E_ARG;
+    }
+    FrameSlot& F = c->frames[slot];
+    if (!F.pending && !F.host) {
+        set_thread_error("slab_frame_wait: nothing captured in this slot");
+        return SLAB_E_STATE;
+    }
+    if (F.pending) {
+        const cudaError_t e = cudaEventSynchronize(F.copied);
+        if (e != cudaSuccess) {
+            set_thread_error(std::string("slab_frame_wait: ") + cudaGetErrorString(e));
+            return SLAB_E_CUDA;
+        }
+    }
+    *out = F.meta;
+    return SLAB_OK;
+}
+
 slab_status slab_moments(slab_ctx* c, double out[6]) {
     if (!c || !out) return SLAB_E_ARG;
     return guard(c, [&] {
@@ -414,6 +504,16 @@ const char* slab_last_error(const slab_ctx* c) { return c ? c->err.c_str() : sla
 void slab_destroy(slab_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    for (FrameSlot& F : c->frames) {
+        if (F.host) cudaFreeHost(F.host);
+        if (F.packed) cudaEventDestroy(F.packed);
+        if (F.copied) cudaEventDestroy(F.copied);
+        F.dev.reset();
+    }
     c->path.reset();
     c->terrain.z.reset();
     c->terrain.grad.reset();

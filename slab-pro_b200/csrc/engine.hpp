@@ -171,6 +171,10 @@ struct Path {
     // FP64 particle moments: mass, centre of mass (x, y), momentum (x, y),
     // kinetic energy (moments.cuh)
     virtual void moments(double out[6]) = 0;
+    // enqueue the packing of the current frame on the path's stream:
+    // d_part Np x 8 float32 vertices (x y vx vy vz z h A, upload order),
+    // d_grid 6 GeoTIFF bands over box {i0, i1, j0, j1} (slab_frame)
+    virtual void pack_frame(float* d_part, float* d_grid, const int32_t box[4]) = 0;
     virtual int64_t launches() const = 0;
     virtual void phase_times(double out[5]) { for (int k = 0; k < 5; ++k) out[k] = 0; }
     virtual void set_profiling(bool) {}

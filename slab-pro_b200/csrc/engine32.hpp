@@ -60,6 +60,8 @@ class Engine32 {
     void download_max(int sid, double* hmax, double* vmax2);
     void conservation(int sid, double out[4], double rho);
     void moments(int sid, double out[6]);
+    // the current frame in the output files' float32 layouts (slab_frame_capture)
+    void pack_frame(int sid, float* d_part, float* d_grid, const int32_t box[4], double rho);
     dptr<double> d_mom;  // moment partials and result (moments.cuh)
     Shared shared() const;
 

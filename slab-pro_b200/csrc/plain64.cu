@@ -121,6 +121,45 @@ __global__ void __launch_bounds__(256) k64_p2g(const Ctl* __restrict__ c, P64 p,
     }
 }
 
+// Frame packing (slab_frame_capture): particle q as float32 vertex q, x y vx
+// vy vz z h A (the PLY vertex layout).
+__global__ void k64_pack_particles(P64 p, int Np, float* __restrict__ out) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < Np; q += gridDim.x * blockDim.x) {
+        const double2 x = p.x[q], v = p.v[q];
+        float* o = out + (size_t)q * 8;
+        o[0] = (float)x.x;
+        o[1] = (float)x.y;
+        o[2] = (float)v.x;
+        o[3] = (float)v.y;
+        o[4] = (float)p.vz[q];
+        o[5] = (float)p.z[q];
+        o[6] = (float)p.h[q];
+        o[7] = (float)p.A[q];
+    }
+}
+
+// The grid box's 6 GeoTIFF bands (h, |v|, m, vx, vy, vz): band-major, row 0
+// = the north edge, x fastest, -9999 in every band where h == 0.
+__global__ void k64_pack_grid(N64 n, int Ny, int i0, int j0, int nI, int nJ, float* __restrict__ out) {
+    const int64_t total = (int64_t)nI * nJ;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(k / nI), ci = (int)(k % nI);
+        const int64_t g = (int64_t)(i0 + ci) * Ny + (j0 + nJ - 1 - r);
+        const float h = (float)n.out_h[g];
+        if (h == 0.f) {
+            for (int q = 0; q < 6; ++q) out[q * total + k] = -9999.f;
+            continue;
+        }
+        const double2 v = n.v[g];
+        out[k] = h;
+        out[total + k] = (float)sqrt(v.x * v.x + v.y * v.y);
+        out[2 * total + k] = (float)n.out_m[g];
+        out[3 * total + k] = (float)v.x;
+        out[4 * total + k] = (float)v.y;
+        out[5 * total + k] = (float)n.out_vz[g];
+    }
+}
+
 // computeGridVelocity (src/simulation.cpp:800-875) over the remesh box, then
 // the accumulators are zeroed for the next step.
 __global__ void __launch_bounds__(256) k64_grid(Ctl* c, N64 n, const double2* __restrict__ grad,
@@ -525,6 +564,17 @@ struct Plain64 final : Path {
         out[1] = G;
         out[2] = Px;
         out[3] = Py;
+    }
+
+    void pack_frame(float* d_part, float* d_grid, const int32_t box[4]) override {
+        k64_pack_particles<<<std::max(1, std::min(148 * 8, (Np + 255) / 256)), 256, 0, st>>>(parts(), Np, d_part);
+        const int nI = box[1] - box[0] + 1, nJ = box[3] - box[2] + 1;
+        const int64_t nn = (int64_t)nI * nJ;
+        if (nn > 0)
+            k64_pack_grid<<<(int)std::max<int64_t>(1, std::min<int64_t>((nn + 255) / 256, 148 * 8)), 256, 0, st>>>(
+                nodes(), T.Ny, box[0], box[2], nI, nJ, d_grid);
+        nlaunch += nn > 0 ? 2 : 1;
+        SLAB_CUDA(cudaGetLastError());
     }
 
     dptr<double> mom;

@@ -14,6 +14,7 @@
 #include "engine32.hpp"
 #include "split32_kernels.cuh"
 #include "moments.cuh"
+#include "bin32.hpp"
 
 namespace slab {
 
@@ -76,7 +77,75 @@ __global__ void k_gather_nodes(const int32_t* __restrict__ blk_of, const int32_t
     }
 }
 
+// Frame packing (slab_frame_capture). Particle k of the buffer goes to vertex
+// id[k]: x y vx vy vz z h A as float32 (the PLY vertex layout), A = m / (h rho).
+__global__ void k_pack_particles(PBuf B, int Np, double dx, double rho, float* __restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Np; k += gridDim.x * blockDim.x) {
+        const int32_t c = B.cell[k];
+        const float2 f = B.f[k], v = B.v[k];
+        const float h = B.h[k], m = B.m[k];
+        float* o = out + (size_t)B.id[k] * 8;
+        o[0] = (float)(((double)cell_i(c) + (double)f.x) * dx);
+        o[1] = (float)(((double)cell_j(c) + (double)f.y) * dx);
+        o[2] = v.x;
+        o[3] = v.y;
+        o[4] = B.vz[k];
+        o[5] = B.z[k];
+        o[6] = h;
+        o[7] = (float)((double)m / ((double)h * rho));
+    }
+}
+
+// The grid box's 6 GeoTIFF bands (h, |v|, m, vx, vy, vz) in GDAL order:
+// band-major, row 0 = the north edge (j = j0 + nJ - 1), x fastest; -9999 in
+// every band where h == 0. Nodes of blocks the last step did not update are
+// empty.
+__global__ void k_pack_grid(const int32_t* __restrict__ blk_of, const int32_t* __restrict__ blk_stamp, int stepid, int TY, int i0, int j0,
+                            int nI, int nJ, const float* __restrict__ oh, const float* __restrict__ om, const float* __restrict__ ovz,
+                            const float4* __restrict__ nv, float* __restrict__ out) {
+    const int64_t total = (int64_t)nI * nJ;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(k / nI), ci = (int)(k % nI);
+        const int i = i0 + ci, j = j0 + nJ - 1 - r;
+        const int blk = blk_of[(i / TILE) * TY + (j / TILE)];
+        const bool ok = blk >= 0 && blk_stamp[blk] == stepid;
+        const size_t n = (size_t)blk * NCELL + (i % TILE) * TILE + (j % TILE);
+        const float h = ok ? oh[n] : 0.f;
+        if (h == 0.f) {
+            for (int q = 0; q < 6; ++q) out[q * total + k] = -9999.f;
+            continue;
+        }
+        const float4 v = nv[n];
+        out[k] = h;
+        out[total + k] = (float)sqrt(__dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y)));  // as the host writer: no fused multiply-add
+        out[2 * total + k] = om[n];
+        out[3 * total + k] = v.x;
+        out[4 * total + k] = v.y;
+        out[5 * total + k] = ovz[n];
+    }
+}
+
 }  // namespace k32
+
+void Engine32::pack_frame(int sid, float* d_part, float* d_grid, const int32_t box[4], double rho) {
+    Store& S = (*slots[sid]);
+    const SCnt c = counters(sid);
+    const int b = c.seq & 1;
+    const int Np = S.Np;
+    if (!c.vz_valid) {  // between output frames the step loop does not keep z / vz
+        k32::k_refresh_vz_z<<<std::max(1, std::min(148 * 8, (Np + 255) / 256)), 256, 0, st>>>(shared(), host_scn[sid].buf[b], Np, T.z.get());
+        ++nlaunch;
+    }
+    k32::k_pack_particles<<<std::max(1, std::min(148 * 8, (Np + 255) / 256)), 256, 0, st>>>(host_scn[sid].buf[b], Np, T.dx, rho, d_part);
+    const int nI = box[1] - box[0] + 1, nJ = box[3] - box[2] + 1;
+    const int64_t nodes = (int64_t)nI * nJ;
+    if (nodes > 0)
+        k32::k_pack_grid<<<(int)std::max<int64_t>(1, std::min<int64_t>((nodes + 255) / 256, 148 * 8)), 256, 0, st>>>(
+            S.blk_of.get(), d_blk_stamp.get(), c.stepid, TY, box[0], box[2], nI, nJ, d_oh.get(), d_om.get(), d_ovz.get(), d_nv.get(),
+            d_grid);
+    nlaunch += nodes > 0 ? 2 : 1;
+    SLAB_CUDA(cudaGetLastError());
+}
 
 Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_cap, bool batch)
     : T(t), st(s), max_scn(max_scn), batch(batch) {
@@ -187,17 +256,6 @@ Shared Engine32::shared() const {
 }
 
 namespace k32 {
-// Blocks of a retired scenario: maxima and stamps reset before reuse.
-// initial segment records of the occupied tiles of a new scenario (stamp 0)
-__global__ void k_scatter_tiles(const int32_t* __restrict__ tiles, const int32_t* __restrict__ recs, int n, int32_t* grp,
-                                int32_t* act_stamp) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
-    const int t = tiles[q];
-    for (int k = 0; k < GRP_STRIDE; ++k) grp[(size_t)t * GRP_STRIDE + k] = recs[(size_t)q * GRP_STRIDE + k];
-    act_stamp[t] = 0;
-}
-
 // node blocks of one scenario: ids into out[8...], count into out[0], tile
 // box {ti0, ti1, tj0, tj1} into out[1..4] (out[0..4] preset to 0, big, -1, big, -1)
 __global__ void k_collect_blocks(const int32_t* __restrict__ blk_of, int ntiles, int TY, int32_t* out) {
@@ -379,70 +437,23 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     ensure_work_cap(work_cap_total + S.act_cap);
     work_cap_total += S.act_cap;
 
-    // ---- bin particles into tiles (stable in upload order)
-    const double dx = T.dx, ood = 1.0 / T.dx;
-    std::vector<int32_t> cell(Np), tile(Np);
-    std::vector<float2> f(Np);
-    double mnx = INFINITY, mxx = 0, mny = INFINITY, mxy = 0, vv = 0;
-    for (int q = 0; q < Np; ++q) {
-        const double ux = x[2 * q] * ood, uy = x[2 * q + 1] * ood;
-        int ib = (int)std::floor(ux - 0.5), jb = (int)std::floor(uy - 0.5);
-        float fx = (float)(ux - ib), fy = (float)(uy - jb);
-        if (fx >= 1.5f) { ++ib; fx -= 1.f; }
-        if (fy >= 1.5f) { ++jb; fy -= 1.f; }
-        if (ib < 0 || jb < 0 || ib + 2 > T.Nx - 1 || jb + 2 > T.Ny - 1) throw Error{SLAB_E_DOMAIN, "particle stencil outside the terrain"};
-        cell[q] = pack_cell(ib, jb);
-        f[q] = make_float2(fx, fy);
-        tile[q] = (ib / TILE) * TY + (jb / TILE);
-        const double px = ((double)ib + (double)fx) * dx, py = ((double)jb + (double)fy) * dx;
-        mnx = std::min(mnx, px);
-        mxx = std::max(mxx, px);
-        mny = std::min(mny, py);
-        mxy = std::max(mxy, py);
-        const float vx = (float)v[2 * q], vy = (float)v[2 * q + 1];
-        vv = std::max(vv, (double)(vx * vx + vy * vy));
-    }
-    std::vector<int32_t> cnt(ntiles, 0), start(ntiles + 1, 0);
-    for (int q = 0; q < Np; ++q) cnt[tile[q]]++;
-    for (int t = 0; t < ntiles; ++t) start[t + 1] = start[t] + cnt[t];
-    std::vector<int32_t> pos(start.begin(), start.end() - 1);
-    std::vector<int32_t> o_cell(Np), o_id(Np);
-    std::vector<float2> o_f(Np), o_v(Np);
-    std::vector<float> o_h(Np), o_m(Np), o_vz(Np), o_z(Np);
-    for (int q = 0; q < Np; ++q) {
-        const int k = pos[tile[q]]++;
-        o_cell[k] = cell[q];
-        o_f[k] = f[q];
-        o_v[k] = make_float2((float)v[2 * q], (float)v[2 * q + 1]);
-        o_h[k] = (float)h[q];
-        o_m[k] = (float)m[q];
-        o_vz[k] = (float)vz[q];
-        o_z[k] = (float)z[q];
-        o_id[k] = q;
-    }
-    // segment records of the occupied tiles only (the stamps mark every other
-    // tile's record as stale, so nothing of size ntiles crosses the bus)
-    std::vector<int32_t> recs, alist;
-    for (int t = 0; t < ntiles; ++t) {
-        if (!cnt[t]) continue;
-        int32_t G[GRP_STRIDE] = {0};
-        G[0] = start[t];
-        G[1] = start[t + 1];
-        G[2] = start[t + 1];
-        G[3 + 4] = cnt[t];
-        G[GRP_STAMP] = 0;
-        recs.insert(recs.end(), G, G + GRP_STRIDE);
-        alist.push_back(t);
-    }
-    if ((int)alist.size() > S.act_cap) throw Error{SLAB_E_OOM, "active tile capacity"};
+    // ---- bin the particles into tile segments on the device (stable in upload order)
+    const double ood = 1.0 / T.dx;
+    for (int b = 0; b < 2; ++b)  // every record stale (stamp -1)
+        SLAB_CUDA(cudaMemsetAsync(S.grp[b].get(), 0xff, (size_t)ntiles * GRP_STRIDE * sizeof(int32_t), st));
+    SLAB_CUDA(cudaMemsetAsync(S.act_stamp.get(), 0xff, ntiles * sizeof(int32_t), st));
+    const PBuf out0{S.cell[0].get(), S.f[0].get(), S.v[0].get(), S.h[0].get(), S.m[0].get(), S.id[0].get(), S.vz[0].get(), S.z[0].get()};
+    const BinResult bin = bin_particles(T, TY, ntiles, st, Np, x, v, vz, h, m, z, out0, S.grp[0].get(), S.act_list[0].get(),
+                                        S.act_stamp.get(), S.act_cap);
+    const std::vector<uint32_t>& alist = bin.tiles;
     // node blocks the t=0 pass will take (the grid tiles of the active tiles'
     // node windows): grow the pool now, as the pass runs before any check
     {
         std::vector<char> touched(ntiles, 0);
         int64_t est = 0;
-        for (int t : alist)
+        for (uint32_t t : alist)
             for (int k = 0; k < 4; ++k) {
-                const int gi = t / TY + (k >> 1), gj = t % TY + (k & 1);
+                const int gi = (int)t / TY + (k >> 1), gj = (int)t % TY + (k & 1);
                 if (gi < TX && gj < TY && !touched[gi * TY + gj]) {
                     touched[gi * TY + gj] = 1;
                     ++est;
@@ -455,26 +466,6 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
         const int64_t need = (int64_t)(misc[0] - misc[4]) + pending_blocks;
         if (2 * need > blk_cap) grow_blocks((int)std::min<int64_t>(std::max<int64_t>(2 * (int64_t)blk_cap, 2 * need), INT32_MAX / NCELL));
     }
-    h2d(S.cell[0].get(), o_cell.data(), Np, st);
-    h2d(S.f[0].get(), o_f.data(), Np, st);
-    h2d(S.v[0].get(), o_v.data(), Np, st);
-    h2d(S.h[0].get(), o_h.data(), Np, st);
-    h2d(S.m[0].get(), o_m.data(), Np, st);
-    h2d(S.id[0].get(), o_id.data(), Np, st);
-    h2d(S.vz[0].get(), o_vz.data(), Np, st);
-    h2d(S.z[0].get(), o_z.data(), Np, st);
-    for (int b = 0; b < 2; ++b)  // every record stale (stamp -1)
-        SLAB_CUDA(cudaMemsetAsync(S.grp[b].get(), 0xff, (size_t)ntiles * GRP_STRIDE * sizeof(int32_t), st));
-    SLAB_CUDA(cudaMemsetAsync(S.act_stamp.get(), 0xff, ntiles * sizeof(int32_t), st));
-    h2d(S.act_list[0].get(), alist.data(), alist.size(), st);
-    if (!alist.empty()) {
-        dptr<int32_t> d_recs = dalloc<int32_t>(recs.size());
-        h2d(d_recs.get(), recs.data(), recs.size(), st);
-        const int n = (int)alist.size();
-        k32::k_scatter_tiles<<<(n + 127) / 128, 128, 0, st>>>(S.act_list[0].get(), d_recs.get(), n, S.grp[0].get(), S.act_stamp.get());
-        SLAB_CUDA(cudaGetLastError());
-        SLAB_CUDA(cudaStreamSynchronize(st));  // d_recs is freed on return
-    }
     SLAB_CUDA(cudaMemsetAsync(S.gt_stamp.get(), 0xff, ntiles * sizeof(int32_t), st));
     SLAB_CUDA(cudaMemsetAsync(S.blk_of.get(), 0xff, ntiles * sizeof(int32_t), st));
     SCnt c0{};
@@ -483,11 +474,8 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     c0.vz_valid = 1;
     h2d(S.cnt, &c0, 1, st);
     // particle box and max speed for the first step (Simulation::updateDt / remesh)
-    h_ctl->pos_acc[0] = (uint64_t)__builtin_bit_cast(uint64_t, mnx);
-    h_ctl->pos_acc[1] = (uint64_t)__builtin_bit_cast(uint64_t, mxx);
-    h_ctl->pos_acc[2] = (uint64_t)__builtin_bit_cast(uint64_t, mny);
-    h_ctl->pos_acc[3] = (uint64_t)__builtin_bit_cast(uint64_t, mxy);
-    h_ctl->vmax2_bits = (uint64_t)__builtin_bit_cast(uint64_t, vv);
+    for (int k = 0; k < 4; ++k) h_ctl->pos_acc[k] = bin.box_bits[k];
+    h_ctl->vmax2_bits = bin.vmax2_bits;
     h2d(ctl, h_ctl, 1, st);
     double msum = 0;
     for (int q = 0; q < Np; ++q) msum += m[q];
@@ -980,6 +968,7 @@ struct Split32 final : Path {
     void download_max(double* hm, double* vm) override { E.download_max(sid, hm, vm); }
     void conservation(double out[4]) override { E.conservation(sid, out, prm.rho); }
     void moments(double out[6]) override { E.moments(sid, out); }
+    void pack_frame(float* d_part, float* d_grid, const int32_t box[4]) override { E.pack_frame(sid, d_part, d_grid, box, prm.rho); }
     int64_t launches() const override { return E.nlaunch; }
     void set_profiling(bool on) override {
         E.timer.collect();

@@ -6,7 +6,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
+#include <deque>
+#include <exception>
+#include <mutex>
+#include <thread>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
@@ -489,7 +494,84 @@ void Simulation::pull_frame() {
     if (gv.cap_nodes > 0) check(slab_download_grid(ctx, &gv), ctx, "slab_download_grid");
 }
 
-// src/simulation.cpp:484-522 with the step loop on the GPU
+namespace {
+
+// Writes the frames captured by slab_frame_capture on its own thread, so that
+// the files of frame k are written while the GPU runs frame k+1's steps.
+// Frame k uses capture slot k % 2; the slot can be captured again once job
+// k has been written (wait_written).
+class FrameWriter {
+  public:
+    using WriteFn = std::function<void(const slab_frame&)>;
+    FrameWriter(slab_ctx* ctx, WriteFn fn) : ctx_(ctx), fn_(std::move(fn)), th_([this] { run(); }) {}
+    ~FrameWriter() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        if (th_.joinable()) th_.join();
+    }
+    // queue job k (frames are numbered 0, 1, ... in capture order)
+    void push(int64_t k) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            jobs_.push_back(k);
+        }
+        cv_.notify_all();
+    }
+    // block until job k is written (k < 0: nothing to wait for); rethrows a writer error
+    void wait_written(int64_t k) {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return written_ >= k || err_; });
+        if (err_) std::rethrow_exception(err_);
+    }
+
+  private:
+    void run() {
+        for (;;) {
+            int64_t k;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || !jobs_.empty(); });
+                if (jobs_.empty()) return;
+                k = jobs_.front();
+                jobs_.pop_front();
+            }
+            try {
+                slab_frame f{};
+                const slab_status st = slab_frame_wait(ctx_, (int32_t)(k % 2), &f);
+                if (st != SLAB_OK) throw std::runtime_error(std::string("slab_frame_wait: ") + slab_last_error(nullptr));
+                fn_(f);
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(mu_);
+                err_ = std::current_exception();
+                cv_.notify_all();
+                return;
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                written_ = k;
+            }
+            cv_.notify_all();
+        }
+    }
+    slab_ctx* ctx_;
+    WriteFn fn_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<int64_t> jobs_;
+    int64_t written_ = -1;
+    bool stop_ = false;
+    std::exception_ptr err_;
+    std::thread th_;  // last: starts after the members it reads
+};
+
+}  // namespace
+
+// src/simulation.cpp:484-522 with the step loop on the GPU. Output frames are
+// packed on the device and written by a writer thread while the next frame's
+// steps run (slab_frame_capture / slab_frame_wait).
 void Simulation::simulate() {
     if (Np <= 0) throw std::runtime_error("no particles: call initializeParticles first");
     if (ctx) {
@@ -524,10 +606,22 @@ void Simulation::simulate() {
     time = 0.0;
     frame = 0;
     steps = 0;
+    std::unique_ptr<FrameWriter> writer;
+    int64_t captured = 0;
+    auto capture = [&] {
+        // frame k reuses the slot of frame k - 2: its files must be written first
+        writer->wait_written(captured - 2);
+        check(slab_frame_capture(ctx, (int32_t)(captured % 2)), ctx, "slab_frame_capture");
+        writer->push(captured++);
+    };
     if (write_outputs) {
-        pull_frame();
-        saveParticleData();
-        saveGridData();
+        writer.reset(new FrameWriter(ctx, [this](const slab_frame& f) {
+            write_ply_vertices(particle_path / frame_name("particles_frame_", padding, f.frame, ".ply"), f.Np, f.particles);
+            if (f.Nx > 0 && f.Ny > 0)
+                write_grid_bands_tif(raster_path / frame_name("rasters_frame_", padding, f.frame, ".tif"), f.Nx, f.Ny, f.grid,
+                                     terrain.xllcorner + terrain.x[f.i_off], terrain.yllcorner + terrain.y[f.j_off + f.Ny - 1], dx);
+        }));
+        capture();
     }
     while (time < total_time) {
         int64_t k = 0;
@@ -535,15 +629,15 @@ void Simulation::simulate() {
         check(slab_advance_to_frame(ctx, &time, &f, &k), ctx, "slab_advance_to_frame");
         frame = f;
         steps += k;
-        if (write_outputs) {
-            pull_frame();
-            saveParticleData();
-            saveGridData();
-        }
+        if (write_outputs && k > 0) capture();
         if (k == 0) break;
     }
+    if (writer) {
+        writer->wait_written(captured - 1);
+        writer.reset();
+    }
     check(slab_download_max(ctx, terrain.h_max.data(), terrain.v_max2.data()), ctx, "slab_download_max");
-    if (!write_outputs) pull_frame();
+    pull_frame();  // the final state into particles / grid
     if (write_outputs) saveMaxData();
     std::cout << "Simulation finished: " << steps << " steps, t = " << time << " s" << std::endl;
 }

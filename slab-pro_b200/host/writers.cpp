@@ -228,13 +228,27 @@ void write_geotiff(const fs::path& file, int nx, int ny, const std::vector<std::
     if (!out) throw std::runtime_error("Failed writing GeoTIFF: " + file.string());
 }
 
-void write_particles_ply(const fs::path& file, const Particles& p) {
-    const int n = p.size();
+void write_ply_vertices(const fs::path& file, int n, const float* verts) {
     std::ofstream out(file, std::ios::binary);
     if (!out) throw std::runtime_error("Could not create PLY: " + file.string());
     out << "ply\nformat binary_little_endian 1.0\nelement vertex " << n << "\n";
     for (const char* name : {"x", "y", "vx", "vy", "vz", "z", "h", "A"}) out << "property float " << name << "\n";
     out << "end_header\n";
+    if (n > 0) out.write(reinterpret_cast<const char*>(verts), (std::streamsize)((size_t)n * 8 * sizeof(float)));
+    if (!out) throw std::runtime_error("Failed writing PLY: " + file.string());
+}
+
+void write_grid_bands_tif(const fs::path& file, int nx, int ny, const float* bands, double origin_x, double origin_y, double dx,
+                          TiffCompression comp) {
+    if (nx <= 0 || ny <= 0) return;
+    const size_t n = (size_t)nx * ny;
+    std::vector<std::vector<float>> b(6);
+    for (int q = 0; q < 6; ++q) b[q].assign(bands + q * n, bands + (q + 1) * n);
+    write_geotiff(file, nx, ny, b, {"h", "v_norm", "m", "v_x", "v_y", "v_z"}, origin_x, origin_y, dx, -9999.0f, comp);
+}
+
+void write_particles_ply(const fs::path& file, const Particles& p) {
+    const int n = p.size();
     std::vector<float> buf((size_t)n * 8);
     for (int i = 0; i < n; ++i) {
         float* r = buf.data() + (size_t)i * 8;
@@ -247,8 +261,7 @@ void write_particles_ply(const fs::path& file, const Particles& p) {
         r[6] = (float)p.h[i];
         r[7] = (float)p.A[i];
     }
-    out.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)(buf.size() * sizeof(float)));
-    if (!out) throw std::runtime_error("Failed writing PLY: " + file.string());
+    write_ply_vertices(file, n, buf.data());
 }
 
 void write_grid_tif(const fs::path& file, const Grid& g, double xll, double yll, double dx, TiffCompression comp) {

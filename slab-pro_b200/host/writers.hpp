@@ -33,6 +33,12 @@ void write_geotiff(const std::filesystem::path& file, int nx, int ny, const std:
                    TiffCompression comp);
 
 void write_particles_ply(const std::filesystem::path& file, const Particles& p);
+// n vertices of 8 float32 (x y vx vy vz z h A), as packed by slab_frame_capture
+void write_ply_vertices(const std::filesystem::path& file, int n, const float* verts);
+// the 6 bands of rasters_frame_N.tif (h, v_norm, m, v_x, v_y, v_z), already in
+// GDAL order with nodata -9999, as packed by slab_frame_capture
+void write_grid_bands_tif(const std::filesystem::path& file, int nx, int ny, const float* bands, double origin_x, double origin_y, double dx,
+                          TiffCompression comp = default_tiff_compression());
 void write_grid_tif(const std::filesystem::path& file, const Grid& grid, double xll, double yll, double dx,
                     TiffCompression comp = default_tiff_compression());
 void write_max_tif(const std::filesystem::path& file, const Grid& terrain, double dx, TiffCompression comp = default_tiff_compression());

@@ -52,6 +52,11 @@ class GridView(C.Structure):
                 ("a", C.POINTER(C.c_double))]
 
 
+class Frame(C.Structure):
+    _fields_ = [("frame", C.c_int32), ("Np", C.c_int32), ("time", C.c_double), ("particles", C.POINTER(C.c_float)),
+                ("Nx", C.c_int32), ("Ny", C.c_int32), ("i_off", C.c_int32), ("j_off", C.c_int32), ("grid", C.POINTER(C.c_float))]
+
+
 _lib = None
 
 
@@ -78,6 +83,8 @@ def lib():
         L.slab_download_max.argtypes = [vp, dp, dp]
         L.slab_conservation.argtypes = [vp, dp]
         L.slab_moments.argtypes = [vp, dp]
+        L.slab_frame_capture.argtypes = [vp, C.c_int32]
+        L.slab_frame_wait.argtypes = [vp, C.c_int32, C.POINTER(Frame)]
         L.slab_batch_moments.argtypes = [vp, C.c_int32, dp]
         L.slab_get_state.argtypes = [vp, dp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
         L.slab_set_profiling.argtypes = [vp, C.c_int32]
@@ -229,6 +236,23 @@ class Slab:
         out = np.zeros(4)
         self._check(self.L.slab_conservation(self.h, _dp(out)))
         return out
+
+    def frame_capture(self, slot: int):
+        """Pack the current frame on the device and start its copy to the host."""
+        self._check(self.L.slab_frame_capture(self.h, int(slot)))
+
+    def frame_wait(self, slot: int) -> dict:
+        """The captured frame: particles [Np, 8] float32 (x y vx vy vz z h A)
+        and grid [6, Ny, Nx] float32 bands in GeoTIFF order (copies)."""
+        f = Frame()
+        code = self.L.slab_frame_wait(self.h, int(slot), C.byref(f))
+        if code != 0:
+            raise SlabError(code, (self.L.slab_last_error(None) or b"").decode())
+        parts = np.ctypeslib.as_array(f.particles, shape=(f.Np * 8,)).reshape(f.Np, 8).copy() if f.Np else np.zeros((0, 8), np.float32)
+        n = f.Nx * f.Ny
+        grid = np.ctypeslib.as_array(f.grid, shape=(6 * n,)).reshape(6, f.Ny, f.Nx).copy() if n else np.zeros((6, 0, 0), np.float32)
+        return {"frame": f.frame, "time": f.time, "particles": parts, "grid": grid, "Nx": f.Nx, "Ny": f.Ny, "i_off": f.i_off,
+                "j_off": f.j_off}
 
     def moments(self) -> dict:
         """FP64 particle moments summed on the device: mass, centre of mass,
