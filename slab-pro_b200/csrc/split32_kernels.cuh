@@ -230,97 +230,135 @@ __device__ __forceinline__ int p2g_count(const Shared& sh, int cls) {
 }
 __device__ __forceinline__ int p2g_item(const Shared& sh, int cls, int i) { return cls < 0 ? i : sh.wlist[cls * sh.work_cap + i]; }
 
-// K1 (bookkeeping half): one thread per active tile t. Its particles are
-// the stayers of its own segment in the current buffer plus the movers of
-// the 8 neighbour segments that moved to t (those are filtered by cell when
-// read). The descriptor records these 9 candidate ranges and the exact count,
-// reserves t's segment in the next buffer, and puts the 4 tiles owning t's
-// node window on the grid-tile list.
-__global__ void __launch_bounds__(256) k_prep(Shared sh) {
+// K1 (bookkeeping half): a tile's particles are the stayers of its own
+// segment in the current buffer plus the movers of the 8 neighbour segments
+// that moved to it (those are filtered by cell when read). The descriptor
+// records these 9 candidate ranges and the exact count, reserves the tile's
+// segment in the next buffer, and puts the 4 tiles owning its node window on
+// the grid-tile list.
+// Sixteen lanes (half a warp) per active tile, so that its independent
+// global accesses go out together: lanes 0-8 read the 9 segment records,
+// lanes 9-12 stamp the 4 grid tiles, lane 0 takes the segment cursor and the
+// class-list slot; the counts and range prefixes are half-warp shuffles, and
+// the lanes write the descriptor's words side by side.
+constexpr int PREP_LANES = 16;
+constexpr int PREP_THREADS = 256;
+static_assert(sizeof(TileDesc) == 28 * 4 && offsetof(TileDesc, rstart) == 4 * 4 && offsetof(TileDesc, rpref) == 13 * 4 &&
+                  offsetof(TileDesc, blk4) == 23 * 4,
+              "k_prep writes the descriptor word by word");
+
+__global__ void __launch_bounds__(PREP_THREADS) k_prep(Shared sh) {
     const int nwork = sh.work_pref[sh.nscn];
-    const int stride = gridDim.x * blockDim.x;
-    for (int w0 = blockIdx.x * blockDim.x; w0 < nwork; w0 += stride) {
-        const int w = w0 + threadIdx.x;
+    const int lane = threadIdx.x & 31, r = lane & (PREP_LANES - 1);
+    const int per_block = PREP_THREADS / PREP_LANES;
+    const int stride = gridDim.x * per_block;
+    // whole warps run every iteration (the shuffles need both halves); a half
+    // without a tile computes with valid = false
+    for (int w0 = blockIdx.x * per_block; w0 + (int)(threadIdx.x & ~31u) / PREP_LANES < nwork; w0 += stride) {
+        const int w = w0 + threadIdx.x / PREP_LANES;
         const bool valid = w < nwork;
-        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-        if (!valid) continue;
-        int sid, loc;
-        find_work(sh.work_pref, sh.nscn, w, sid, loc);
+        int sid = 0, loc = 0;
+        if (valid) find_work(sh.work_pref, sh.nscn, w, sid, loc);
         const Scn& S = sh.scn[sid];
         SCnt* n = sh.cnt + sid;  // no load of S.cnt in the chain
-        const int seq = n->seq, cur = seq & 1;
-        const int stamp = n->stepid;
-        const int t = S.act_list[cur][loc];
+        int seq = 0, stamp = 0, t = 0;
+        if (valid) {
+            seq = n->seq;
+            stamp = n->stepid;
+            t = S.act_list[seq & 1][loc];
+        }
+        const int cur = seq & 1;
         const int ti = t / sh.TY, tj = t % sh.TY;
-        TileDesc D;
-        D.t = t;
-        D.sid = sid;
-        int rs[9], rl[9], cnt = 0;
-#pragma unroll
-        for (int d = 0; d < 9; ++d) {
-            const int si = ti - dir_i(d), sj = tj - dir_j(d);
-            rs[d] = rl[d] = 0;
+        // lanes 0-8: the record of neighbour d = r (its particles that moved to t)
+        int rs = 0, rl = 0, c = 0;
+        if (valid && r < 9) {
+            const int si = ti - dir_i(r), sj = tj - dir_j(r);
             if (si >= 0 && sj >= 0 && si < sh.TX && sj < sh.TY) {
-                const int s = si * sh.TY + sj;
-                const int32_t* G = S.grp[cur] + (size_t)s * GRP_STRIDE;
+                const int32_t* G = S.grp[cur] + (size_t)(si * sh.TY + sj) * GRP_STRIDE;
                 if (G[GRP_STAMP] == seq) {
-                    if (d == 4) {
-                        rs[d] = G[0];
-                        rl[d] = G[1] - G[0];
-                    } else {
-                        rs[d] = G[1];
-                        rl[d] = G[2] - G[1];
-                    }
-                    cnt += G[3 + d];
+                    const int g0 = G[0], g1 = G[1], g2 = G[2];
+                    rs = r == 4 ? g0 : g1;
+                    rl = r == 4 ? g1 - g0 : g2 - g1;
+                    c = G[3 + r];
                 }
             }
         }
-        int acc = 0;
-#pragma unroll
-        for (int d = 0; d < 9; ++d) {
-            D.rstart[d] = rs[d];
-            D.rpref[d] = acc;
-            acc += rl[d];
-        }
-        D.rpref[9] = acc;
-        D.total = cnt;
-        // every atomic of the tile is issued before the first result is used
-        // (grid-tile stamps, segment cursor, class list), so they share one round
-        int old[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        // lanes 9-12: the grid tiles of t's node window, stamped with this step
+        bool new_gt = false;
+        int gt = 0;
+        if (valid && r >= 9 && r < 13) {
+            const int k = r - 9;
             const int gi = ti + (k >> 1), gj = tj + (k & 1);
-            old[k] = (gi < sh.TX && gj < sh.TY) ? atomicMax(&S.gt_stamp[gi * sh.TY + gj], stamp) : stamp;
+            if (gi < sh.TX && gj < sh.TY) {
+                gt = gi * sh.TY + gj;
+                new_gt = atomicMax(&S.gt_stamp[gt], stamp) < stamp;
+            }
         }
-        const WarpAdd a_cur = warp_add_issue(&n->cursor, cnt, vmask);
-        const int cls = cnt > sh.split_min ? 0 : 1;
-        WarpAdd a_cls{};
-        if (sh.split_min >= 0) a_cls = warp_add_issue(sh.wcount + cls, 1, vmask);
-        D.nxt_off = warp_add_finish(a_cur);
-        if (sh.split_min >= 0) {  // dense tiles to the cell-sorted P2G, sparse ones to the fixed-point P2G
-            const int at = warp_add_finish(a_cls);
-            if (at < sh.work_cap) sh.wlist[cls * sh.work_cap + at] = w;
+        // half-warp shuffles: the tile's particle count and the range prefixes
+        int incl = rl;
+#pragma unroll
+        for (int o = 1; o < PREP_LANES; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o, PREP_LANES);
+            if (r >= o) incl += y;
         }
-        D.pad_ = 0;
+        int cnt = c;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) D.blk4[k] = -1;  // grid tiles off the terrain keep -1
-        S.slot_of[t] = w;
-        int gl[4], ng = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (old[k] < stamp) gl[ng++] = (ti + (k >> 1)) * sh.TY + (tj + (k & 1));
-        const int at = warp_atomic_add(sh.gcount, ng, vmask);
-        for (int k = 0; k < ng; ++k) {
-            if (at + k < sh.gcap) {
-                sh.gflat[2 * (at + k)] = sid;
-                sh.gflat[2 * (at + k) + 1] = gl[k];
+        for (int o = PREP_LANES / 2; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o, PREP_LANES);
+        const int ncand = __shfl_sync(0xffffffffu, incl, 8, PREP_LANES);
+        // lane 0: the segment cursor and the class list (one atomic per address and warp)
+        const bool leader = valid && r == 0;
+        const unsigned lmask = __ballot_sync(0xffffffffu, leader);
+        int nxt_off = 0;
+        if (leader) {
+            const WarpAdd a_cur = warp_add_issue(&n->cursor, cnt, lmask);
+            const int cls = cnt > sh.split_min ? 0 : 1;
+            WarpAdd a_cls{};
+            if (sh.split_min >= 0) a_cls = warp_add_issue(sh.wcount + cls, 1, lmask);
+            nxt_off = warp_add_finish(a_cur);
+            if (sh.split_min >= 0) {  // dense tiles to the cell-sorted P2G, sparse ones to the fixed-point P2G
+                const int at = warp_add_finish(a_cls);
+                if (at < sh.work_cap) sh.wlist[cls * sh.work_cap + at] = w;
+            }
+            S.slot_of[t] = w;
+        }
+        // the new grid tiles onto the flat grid-tile list, in lane order
+        const unsigned gmask = __ballot_sync(0xffffffffu, new_gt);
+        const unsigned hbits = (lane < PREP_LANES ? 0x0000ffffu : 0xffff0000u);
+        const int ng = __popc(gmask & hbits);
+        int at_g = 0;
+        if (leader) at_g = warp_atomic_add(sh.gcount, ng, lmask);
+        at_g = __shfl_sync(0xffffffffu, at_g, lane & ~(PREP_LANES - 1));
+        nxt_off = __shfl_sync(0xffffffffu, nxt_off, lane & ~(PREP_LANES - 1));
+        if (new_gt) {
+            const int at = at_g + __popc(gmask & hbits & ((1u << lane) - 1u));
+            if (at < sh.gcap) {
+                sh.gflat[2 * at] = sid;
+                sh.gflat[2 * at + 1] = gt;
             } else {
                 atomicOr(&S.ctl->err, ERR_CAPACITY);
             }
         }
-        sh.desc[w] = D;
+        // the descriptor, word by word (TileDesc: t, total, nxt_off, sid,
+        // rstart[9], rpref[10], blk4[4], pad)
+        if (valid) {
+            int* D = reinterpret_cast<int*>(sh.desc + w);
+            if (r < 9) {
+                D[4 + r] = rs;
+                D[13 + r] = incl - rl;  // candidates before range r
+            } else if (r == 9) {
+                D[22] = ncand;
+            } else if (r < 14) {
+                D[23 + (r - 10)] = -1;  // grid tiles off the terrain keep -1; k_grid fills the others
+            } else if (r == 14) {
+                D[27] = 0;
+            } else {
+                D[0] = t;
+                D[1] = cnt;
+                D[2] = nxt_off;
+                D[3] = sid;
+            }
+        }
     }
-
 }
 
 // ------------------------------------------------------------------- P2G
