@@ -8,6 +8,8 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <deque>
 #include <exception>
 #include <mutex>
@@ -217,19 +219,110 @@ void Simulation::initialize() {
 // src/complex_terrain.cpp:31-65: the ESRI ASCII grid, rows stored from the
 // south edge (z[i * nrows + j], j = 0 the last row of the file); nodata is
 // not masked
+namespace {
+
+// Binary cache of a parsed .asc file, written next to it as <file>.slabbin:
+// the header values, the source file's size and modification time, and the
+// heights in the terrain's i * nrows + j order. A later read of the same,
+// unchanged file loads the doubles the parse produced instead of parsing the
+// text again (the ASCII parse of a 28 MB DEM takes seconds).
+constexpr char CACHE_MAGIC[8] = {'S', 'L', 'A', 'B', 'D', 'E', 'M', '1'};
+struct CacheHeader {
+    char magic[8];
+    int64_t src_size, src_mtime;
+    int32_t ncols, nrows;
+    double xllcorner, yllcorner, cellsize, nodata;
+};
+
+int64_t mtime_of(const fs::path& p) {
+    std::error_code ec;
+    const auto t = fs::last_write_time(p, ec);
+    return ec ? -1 : (int64_t)t.time_since_epoch().count();
+}
+
+bool read_asc_cache(const fs::path& src, RasterData& r) {
+    std::error_code ec;
+    const fs::path cp = fs::path(src.string() + ".slabbin");
+    if (!fs::exists(cp, ec)) return false;
+    std::ifstream f(cp, std::ios::binary);
+    CacheHeader h{};
+    if (!f.read(reinterpret_cast<char*>(&h), sizeof h)) return false;
+    if (std::memcmp(h.magic, CACHE_MAGIC, 8) != 0 || h.ncols <= 0 || h.nrows <= 0) return false;
+    if (h.src_size != (int64_t)fs::file_size(src, ec) || ec || h.src_mtime != mtime_of(src)) return false;
+    r.ncols = h.ncols;
+    r.nrows = h.nrows;
+    r.xllcorner = h.xllcorner;
+    r.yllcorner = h.yllcorner;
+    r.cellsize = h.cellsize;
+    r.nodata = h.nodata;
+    r.z.resize((size_t)r.ncols * r.nrows);
+    if (!f.read(reinterpret_cast<char*>(r.z.data()), (std::streamsize)(r.z.size() * sizeof(double)))) return false;
+    return true;
+}
+
+void write_asc_cache(const fs::path& src, const RasterData& r) {
+    std::error_code ec;
+    CacheHeader h{};
+    std::memcpy(h.magic, CACHE_MAGIC, 8);
+    h.src_size = (int64_t)fs::file_size(src, ec);
+    if (ec) return;
+    h.src_mtime = mtime_of(src);
+    h.ncols = r.ncols;
+    h.nrows = r.nrows;
+    h.xllcorner = r.xllcorner;
+    h.yllcorner = r.yllcorner;
+    h.cellsize = r.cellsize;
+    h.nodata = r.nodata;
+    const fs::path cp = fs::path(src.string() + ".slabbin"), tmp = fs::path(cp.string() + ".tmp");
+    {
+        std::ofstream f(tmp, std::ios::binary);
+        if (!f) return;  // read-only directory: no cache, nothing else changes
+        f.write(reinterpret_cast<const char*>(&h), sizeof h);
+        f.write(reinterpret_cast<const char*>(r.z.data()), (std::streamsize)(r.z.size() * sizeof(double)));
+        if (!f) {
+            f.close();
+            fs::remove(tmp, ec);
+            return;
+        }
+    }
+    fs::rename(tmp, cp, ec);
+    if (ec) fs::remove(tmp, ec);
+}
+
+}  // namespace
+
+// src/complex_terrain.cpp:31-65: header, then the rows from the north edge
+// down, stored so that j grows northwards. The values are parsed with
+// strtod, as the stream extraction of the reference does, so the doubles are
+// the same; the parsed raster is cached in binary next to the file.
 RasterData Simulation::readASC(const fs::path& path) const {
-    std::ifstream file(path);
-    if (!file.is_open()) throw std::runtime_error("Failed to open ASC file: " + path.string());
     RasterData r;
+    if (read_asc_cache(path, r)) {
+        for (int i = 0; i < r.ncols; ++i) r.x.push_back(i * r.cellsize);
+        for (int j = 0; j < r.nrows; ++j) r.y.push_back(j * r.cellsize);
+        return r;
+    }
+    std::ifstream file(path, std::ios::binary);
+    if (!file.is_open()) throw std::runtime_error("Failed to open ASC file: " + path.string());
+    std::string text((std::istreambuf_iterator<char>(file)), std::istreambuf_iterator<char>());
+    std::istringstream head(text);
     std::string key;
-    file >> key >> r.ncols >> key >> r.nrows >> key >> r.xllcorner >> key >> r.yllcorner >> key >> r.cellsize >> key >> r.nodata;
-    if (!file || r.ncols <= 0 || r.nrows <= 0) throw std::runtime_error("Bad ASC header: " + path.string());
+    head >> key >> r.ncols >> key >> r.nrows >> key >> r.xllcorner >> key >> r.yllcorner >> key >> r.cellsize >> key >> r.nodata;
+    if (!head || r.ncols <= 0 || r.nrows <= 0) throw std::runtime_error("Bad ASC header: " + path.string());
+    const std::streamoff off = head.tellg();
     for (int i = 0; i < r.ncols; ++i) r.x.push_back(i * r.cellsize);
     for (int j = 0; j < r.nrows; ++j) r.y.push_back(j * r.cellsize);
     r.z.resize((size_t)r.ncols * r.nrows);
+    const char* p = text.c_str() + (off < 0 ? text.size() : (size_t)off);
     for (int j = r.nrows - 1; j >= 0; --j)
-        for (int i = 0; i < r.ncols; ++i) file >> r.z[ind(i, j, r.nrows)];
-    if (!file) throw std::runtime_error("ASC file ended early: " + path.string());
+        for (int i = 0; i < r.ncols; ++i) {
+            char* end = nullptr;
+            const double v = std::strtod(p, &end);
+            if (end == p) throw std::runtime_error("ASC file ended early: " + path.string());
+            r.z[ind(i, j, r.nrows)] = v;
+            p = end;
+        }
+    write_asc_cache(path, r);
     return r;
 }
 

@@ -196,3 +196,24 @@ int main() {
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stderr
     assert r.stdout.split() == ["12", "12", "12", "0", "1", "2", "2"]
+
+
+def test_dem_binary_cache(golden, tmp_path):
+    """readASC keeps a binary copy of a parsed DEM next to it
+    (<file>.slabbin); a second run loads it and sets up the same particles, a
+    damaged or stale cache is ignored and the text parsed again."""
+    c = cases.case_fractal_mui()  # a DEM terrain and a raster release, both .asc
+    cfg = MG.write_inputs(c, str(tmp_path))
+    dem = os.path.join(str(tmp_path), "dem.asc")
+    digest = str(golden("fractal_mui")["frame0_digest"])
+    P = _init_only(cfg, str(tmp_path / "p1.bin"))
+    assert cases.particle_digest(P) == digest
+    cache = dem + ".slabbin"
+    assert os.path.exists(cache)
+    assert cases.particle_digest(_init_only(cfg, str(tmp_path / "p2.bin"))) == digest  # from the cache
+    with open(cache, "r+b") as f:  # damaged: ignored
+        f.write(b"XXXXXXXX")
+    assert cases.particle_digest(_init_only(cfg, str(tmp_path / "p3.bin"))) == digest
+    with open(dem, "a") as f:  # the source changed (size and time): the cache is stale
+        f.write("\n")
+    assert cases.particle_digest(_init_only(cfg, str(tmp_path / "p4.bin"))) == digest
