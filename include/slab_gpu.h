@@ -122,6 +122,29 @@ slab_status slab_set_params(slab_ctx* ctx, const slab_params* params);
  * context's own stream. */
 slab_status slab_set_stream(slab_ctx* ctx, void* cuda_stream);
 
+/* A release area of Simulation::initializeParticles (src/simulation.cpp:
+ * 259-476) with UNIFORM 2x2 sampling: a RECTANGLE (a = Lx, b = Ly) or an
+ * ELLIPSE (a = rx, b = ry) around (cx, cy), rotated by rotation_deg, of
+ * uniform release height h0. Coordinates are relative to the terrain's
+ * lower-left node, as the reference's release shapes are. */
+enum { SLAB_RELEASE_RECTANGLE = 0, SLAB_RELEASE_ELLIPSE = 1 };
+typedef struct slab_release {
+    int32_t type; /* SLAB_RELEASE_* */
+    int32_t pad_;
+    double cx, cy;
+    double a, b;
+    double rotation_deg;
+    double h0;
+} slab_release;
+
+/* Build the release's particles on the device -- the reference's setup
+ * arithmetic, so the particles equal the reference's bit for bit: the
+ * snapped bounding box, the 2x2 samples per cell filtered by the shape,
+ * A = V / sum(h), mass = rho h A, z from the 4x4 stencil of terrain heights --
+ * and upload them like slab_upload_particles (v = vz = 0). Np_out: the
+ * particle count. SLAB_E_DOMAIN if the release reaches the terrain edge. */
+slab_status slab_upload_release(slab_ctx* ctx, const slab_release* release, int32_t* Np_out);
+
 /* Upload the particle set built by Simulation::initializeParticles
  * (src/simulation.cpp:259-476) -- the arrays of class Particles
  * (src/data_arrays.hpp:22-47). theta is derived on the device. Resets time,
@@ -265,6 +288,9 @@ slab_status slab_batch_add(slab_batch* b, const slab_params* params, int32_t Np,
                            const double* vz, const double* h, const double* A, const double* mass, const double* z, int32_t* scenario_id);
 /* Advance every scenario until each has reached its total_time, or for at
  * most max_steps steps of the batch. */
+/* Add a scenario whose particles are built on the device from a release
+ * (as slab_upload_release; the same particles as the reference's setup). */
+slab_status slab_batch_add_release(slab_batch* b, const slab_params* params, const slab_release* release, int32_t* scenario_id);
 slab_status slab_batch_run(slab_batch* b, int64_t max_steps, int64_t* steps_out);
 slab_status slab_batch_state(slab_batch* b, int32_t scenario_id, double* time, int32_t* frame, int64_t* steps);
 /* The scenario's own outcome: SLAB_OK, or the error that stopped it
@@ -282,6 +308,8 @@ slab_status slab_batch_moments(slab_batch* b, int32_t scenario_id, double out[6]
  * i1 < i0. */
 slab_status slab_batch_download_max_box(slab_batch* b, int32_t scenario_id, int32_t box[4], double* h_max, double* v_max2,
                                         int64_t cap_nodes);
+/* The scenario's particle count (-1 for an unknown scenario). */
+int32_t slab_batch_scenario_particles(const slab_batch* b, int32_t scenario_id);
 /* out[0] = particle-steps, out[1] = active node-steps, over all scenarios. */
 slab_status slab_batch_work_counters(slab_batch* b, int64_t out[2]);
 int64_t slab_batch_kernel_launches(const slab_batch* b);
@@ -327,6 +355,12 @@ slab_status slab_server_create(const slab_terrain_desc* terrain, const double* z
  * be SLAB_FP32_SPLIT; arrays as slab_upload_particles). */
 slab_status slab_server_submit(slab_server* s, const slab_params* params, int32_t Np, const double* x_xy, const double* v_xy,
                                const double* vz, const double* h, const double* A, const double* mass, const double* z, int64_t* request_id);
+/* Queue a scenario given as a release: its particles are built on the
+ * device when it is admitted (as slab_upload_release), so the setup is part
+ * of the time to result and costs no host work. */
+slab_status slab_server_submit_release(slab_server* s, const slab_params* params, const slab_release* release, int64_t* request_id);
+/* The request's particle count (known for a release once it is admitted). */
+slab_status slab_server_particles(slab_server* s, int64_t request_id, int32_t* Np);
 slab_status slab_server_poll(slab_server* s, int64_t request_id, int32_t* state, double* seconds_to_result);
 /* Block until the request is done (SLAB_E_TIMEOUT after timeout_s). */
 slab_status slab_server_wait(slab_server* s, int64_t request_id, double timeout_s);

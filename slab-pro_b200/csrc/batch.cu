@@ -13,6 +13,7 @@
 
 #include "engine.hpp"
 #include "engine32.hpp"
+#include "release.hpp"
 
 namespace slab {
 void set_thread_error(const std::string& msg);
@@ -136,29 +137,48 @@ slab_status slab_batch_create(const slab_terrain_desc* td, const double* z, int3
     return SLAB_OK;
 }
 
+namespace {
+// a new scenario from host or device particle arrays
+int batch_add_arrays(slab_batch* b, const slab_params* p, int32_t Np, const double* x, const double* v, const double* vz, const double* h,
+                     const double* m, const double* z) {
+    bneed(p->precision == SLAB_FP32_SPLIT, SLAB_E_ARG, "batches run the FP32_SPLIT arithmetic");
+    bneed(b->E->nscn < b->max_scn, SLAB_E_OOM, "batch is full");
+    const int sid = b->E->nscn;
+    Ctl& c = b->h_ctl[sid];
+    std::memset(&c, 0, sizeof(Ctl));
+    c.dx = b->terrain.dx;
+    c.one_over_dx = 1. / b->terrain.dx;
+    c.C_cfl = p->C_cfl;
+    c.dt_max = p->dt_max;
+    c.output_dt = p->output_dt;
+    c.total_time = p->total_time;
+    c.stop = 1;
+    const int got = b->E->add_scenario(*p, b->d_ctl + sid, &c, Np, x, v, vz, h, m, z);
+    bneed(got == sid, SLAB_E_STATE, "scenario id mismatch");
+    b->params.push_back(*p);
+    b->Np.push_back(Np);
+    return sid;
+}
+}  // namespace
+
 slab_status slab_batch_add(slab_batch* b, const slab_params* p, int32_t Np, const double* x, const double* v, const double* vz,
                            const double* h, const double* A, const double* m, const double* z, int32_t* sid_out) {
     if (!b || !p) return SLAB_E_ARG;
     (void)A;
     return bguard(b, [&] {
         bneed(Np > 0 && x && v && vz && h && m && z, SLAB_E_ARG, "invalid particle arrays");
-        bneed(p->precision == SLAB_FP32_SPLIT, SLAB_E_ARG, "batches run the FP32_SPLIT arithmetic");
-        bneed(b->E->nscn < b->max_scn, SLAB_E_OOM, "batch is full");
         for (int q = 0; q < Np; ++q) bneed(h[q] > 0 && m[q] > 0, SLAB_E_ARG, "particle h and mass must be > 0");
-        const int sid = b->E->nscn;
-        Ctl& c = b->h_ctl[sid];
-        std::memset(&c, 0, sizeof(Ctl));
-        c.dx = b->terrain.dx;
-        c.one_over_dx = 1. / b->terrain.dx;
-        c.C_cfl = p->C_cfl;
-        c.dt_max = p->dt_max;
-        c.output_dt = p->output_dt;
-        c.total_time = p->total_time;
-        c.stop = 1;
-        const int got = b->E->add_scenario(*p, b->d_ctl + sid, &c, Np, x, v, vz, h, m, z);
-        bneed(got == sid, SLAB_E_STATE, "scenario id mismatch");
-        b->params.push_back(*p);
-        b->Np.push_back(Np);
+        const int sid = batch_add_arrays(b, p, Np, x, v, vz, h, m, z);
+        if (sid_out) *sid_out = sid;
+    });
+}
+
+slab_status slab_batch_add_release(slab_batch* b, const slab_params* p, const slab_release* r, int32_t* sid_out) {
+    if (!b || !p || !r) return SLAB_E_ARG;
+    return bguard(b, [&] {
+        bneed(std::isfinite(p->rho) && p->rho > 0, SLAB_E_ARG, "rho must be > 0");
+        const DevRelease R = generate_release(b->terrain, *r, p->rho, b->stream);
+        const int sid = batch_add_arrays(b, p, R.Np, R.x, R.v, R.vz, R.h, R.m, R.z);  // binning synchronises before R is freed
         if (sid_out) *sid_out = sid;
     });
 }
@@ -267,6 +287,11 @@ slab_status slab_batch_set_stream(slab_batch* b, void* stream) {
         b->E->st = s;
         b->stream = s;
     });
+}
+
+int32_t slab_batch_scenario_particles(const slab_batch* b, int32_t sid) {
+    if (!b || sid < 0 || sid >= (int32_t)b->Np.size()) return -1;
+    return b->Np[sid];
 }
 
 int64_t slab_batch_kernel_launches(const slab_batch* b) { return b && b->E ? b->E->nlaunch : 0; }

@@ -97,8 +97,9 @@ __global__ void k_bin_records(int n, const uint32_t* __restrict__ tiles, const i
     }
 }
 
+// the caller's arrays may be host or device memory (a release generated on the device)
 template <typename T> void cpy_h2d(T* d, const T* h, size_t n, cudaStream_t s) {
-    if (n) SLAB_CUDA(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    if (n) SLAB_CUDA(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyDefault, s));
 }
 
 }  // namespace

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "engine.hpp"
+#include "release.hpp"
 
 using namespace slab;
 
@@ -259,6 +260,26 @@ slab_status slab_set_stream(slab_ctx* c, void* s) {
     });
 }
 
+namespace {
+// a new path over the context's terrain with these particles (host or device arrays)
+void upload_arrays(slab_ctx* c, int32_t Np, const double* x, const double* v, const double* vz, const double* h, const double* A,
+                   const double* m, const double* z) {
+    c->uploaded = false;
+    c->path.reset();
+    reset_ctl(c);
+    if (c->params.precision == SLAB_FP64_PLAIN)
+        c->path = make_plain64(c->terrain, c->params, c->stream, c->d_ctl, c->h_ctl);
+    else
+        c->path = make_split32(c->terrain, c->params, c->stream, c->d_ctl, c->h_ctl);
+    c->path->upload(Np, x, v, vz, h, A, m, z);
+    pull_ctl(c);
+    raise_device_errors(c);
+    c->Np = Np;
+    c->uploaded = true;
+    c->initial_done = false;
+}
+}  // namespace
+
 slab_status slab_upload_particles(slab_ctx* c, int32_t Np, const double* x, const double* v, const double* vz, const double* h,
                                   const double* A, const double* m, const double* z) {
     if (!c) return SLAB_E_ARG;
@@ -270,19 +291,17 @@ slab_status slab_upload_particles(slab_ctx* c, int32_t Np, const double* x, cons
             need(std::isfinite(x[2 * q]) && std::isfinite(x[2 * q + 1]), SLAB_E_ARG, "non-finite particle position");
             need(h[q] > 0 && m[q] > 0, SLAB_E_ARG, "particle h and mass must be > 0");
         }
-        c->uploaded = false;
-        c->path.reset();
-        reset_ctl(c);
-        if (c->params.precision == SLAB_FP64_PLAIN)
-            c->path = make_plain64(c->terrain, c->params, c->stream, c->d_ctl, c->h_ctl);
-        else
-            c->path = make_split32(c->terrain, c->params, c->stream, c->d_ctl, c->h_ctl);
-        c->path->upload(Np, x, v, vz, h, A, m, z);
-        pull_ctl(c);
-        raise_device_errors(c);
-        c->Np = Np;
-        c->uploaded = true;
-        c->initial_done = false;
+        upload_arrays(c, Np, x, v, vz, h, A, m, z);
+    });
+}
+
+slab_status slab_upload_release(slab_ctx* c, const slab_release* r, int32_t* Np_out) {
+    if (!c || !r) return SLAB_E_ARG;
+    return guard(c, [&] {
+        need(c->have_params, SLAB_E_STATE, "slab_set_params first");
+        const DevRelease R = generate_release(c->terrain, *r, c->params.rho, c->stream);
+        upload_arrays(c, R.Np, R.x, R.v, R.vz, R.h, R.A, R.m, R.z);  // synchronises before R is freed
+        if (Np_out) *Np_out = R.Np;
     });
 }
 

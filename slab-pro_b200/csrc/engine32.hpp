@@ -20,7 +20,6 @@ class Engine32 {
         int act_alloc = 0;  // tile list length
         Ctl* ctl = nullptr;
         Ctl* h_ctl = nullptr;
-        double mass_fp64 = 0;
         dptr<int32_t> cell[2], id[2], grp[2], act_list[2];
         dptr<float2> f[2], v[2];
         dptr<float> h[2], m[2], vz[2], z[2];

@@ -415,13 +415,14 @@ struct Plain64 final : Path {
         A = dalloc<double>(np);
         m = dalloc<double>(np);
         z = dalloc<double>(np);
-        SLAB_CUDA(cudaMemcpyAsync(x.get(), hx, np * sizeof(double2), cudaMemcpyHostToDevice, st));
-        SLAB_CUDA(cudaMemcpyAsync(v.get(), hv, np * sizeof(double2), cudaMemcpyHostToDevice, st));
-        SLAB_CUDA(cudaMemcpyAsync(vz.get(), hvz, np * sizeof(double), cudaMemcpyHostToDevice, st));
-        SLAB_CUDA(cudaMemcpyAsync(h.get(), hh, np * sizeof(double), cudaMemcpyHostToDevice, st));
-        SLAB_CUDA(cudaMemcpyAsync(A.get(), hA, np * sizeof(double), cudaMemcpyHostToDevice, st));
-        SLAB_CUDA(cudaMemcpyAsync(m.get(), hm, np * sizeof(double), cudaMemcpyHostToDevice, st));
-        SLAB_CUDA(cudaMemcpyAsync(z.get(), hz, np * sizeof(double), cudaMemcpyHostToDevice, st));
+        // host arrays, or device arrays of a release generated on the device
+        SLAB_CUDA(cudaMemcpyAsync(x.get(), hx, np * sizeof(double2), cudaMemcpyDefault, st));
+        SLAB_CUDA(cudaMemcpyAsync(v.get(), hv, np * sizeof(double2), cudaMemcpyDefault, st));
+        SLAB_CUDA(cudaMemcpyAsync(vz.get(), hvz, np * sizeof(double), cudaMemcpyDefault, st));
+        SLAB_CUDA(cudaMemcpyAsync(h.get(), hh, np * sizeof(double), cudaMemcpyDefault, st));
+        SLAB_CUDA(cudaMemcpyAsync(A.get(), hA, np * sizeof(double), cudaMemcpyDefault, st));
+        SLAB_CUDA(cudaMemcpyAsync(m.get(), hm, np * sizeof(double), cudaMemcpyDefault, st));
+        SLAB_CUDA(cudaMemcpyAsync(z.get(), hz, np * sizeof(double), cudaMemcpyDefault, st));
         // the control block was reset by the caller; collect the initial box / max speed
         k64_stats<<<(np + 255) / 256, 256, 0, st>>>(dc, parts(), np);
         SLAB_CUDA(cudaGetLastError());

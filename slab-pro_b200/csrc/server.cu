@@ -29,6 +29,7 @@
 
 #include "engine.hpp"
 #include "engine32.hpp"
+#include "release.hpp"
 
 namespace slab {
 void set_thread_error(const std::string& msg);
@@ -47,6 +48,8 @@ struct Request {
     slab_params p{};
     int Np = 0;
     std::vector<double> x, v, vz, h, m, z;
+    bool has_release = false;  // particles built on the device at admission (slab_server_submit_release)
+    slab_release rel{};
     int state = REQ_QUEUED;
     bool cancel = false;
     int slot = -1;
@@ -209,8 +212,15 @@ void worker_loop(slab_server* s) {
                 c.output_dt = r->p.output_dt;
                 c.total_time = r->p.total_time;
                 c.stop = 1;
-                const int got = s->E->add_scenario(r->p, s->d_ctl + slot, &c, r->Np, r->x.data(), r->v.data(), r->vz.data(), r->h.data(),
-                                                   r->m.data(), r->z.data(), slot);
+                int got;
+                if (r->has_release) {  // the release's particles, built on the device
+                    const DevRelease R = generate_release(s->terrain, r->rel, r->p.rho, s->stream);
+                    r->Np = R.Np;
+                    got = s->E->add_scenario(r->p, s->d_ctl + slot, &c, R.Np, R.x, R.v, R.vz, R.h, R.m, R.z, slot);
+                } else {
+                    got = s->E->add_scenario(r->p, s->d_ctl + slot, &c, r->Np, r->x.data(), r->v.data(), r->vz.data(), r->h.data(),
+                                             r->m.data(), r->z.data(), slot);
+                }
                 std::lock_guard<std::mutex> lk(s->mu);
                 s->slot_req[got] = id;
                 r->slot = got;
@@ -401,6 +411,47 @@ slab_status slab_server_submit(slab_server* s, const slab_params* p, int32_t Np,
         s->queue.push_back(r.id);
         s->reqs.emplace(r.id, std::move(r));
         s->cv.notify_all();
+    });
+}
+
+slab_status slab_server_submit_release(slab_server* s, const slab_params* p, const slab_release* rel, int64_t* request_id) {
+    if (!s || !p || !rel || !request_id) return SLAB_E_ARG;
+    return sguard(s, [&] {
+        sneed(p->precision == SLAB_FP32_SPLIT, SLAB_E_ARG, "the server runs the FP32_SPLIT arithmetic");
+        sneed(p->total_time >= 0 && p->dt_max > 0 && p->output_dt > 0 && p->C_cfl > 0 && p->rho > 0, SLAB_E_ARG, "invalid parameters");
+        sneed(rel->a > 0 && rel->b > 0 && rel->h0 > 0 && (rel->type == SLAB_RELEASE_RECTANGLE || rel->type == SLAB_RELEASE_ELLIPSE), SLAB_E_ARG,
+              "invalid release");
+        Request r;
+        r.p = *p;
+        r.has_release = true;
+        r.rel = *rel;
+        const int64_t est = release_estimate(*rel, s->terrain.dx);
+        sneed(est < INT32_MAX, SLAB_E_ARG, "release too large");
+        r.Np = (int)est;  // until admission builds the particles
+        r.footprint = footprint_of(s, (int)est);
+        r.t_submit = clk::now();
+        std::lock_guard<std::mutex> lk(s->mu);
+        sneed(!s->stopping, SLAB_E_STATE, "server is shutting down");
+        r.id = s->next_id++;
+        if (!s->any_submit) {
+            s->any_submit = true;
+            s->t_first_submit = r.t_submit;
+        }
+        *request_id = r.id;
+        s->queue.push_back(r.id);
+        s->reqs.emplace(r.id, std::move(r));
+        s->cv.notify_all();
+    });
+}
+
+slab_status slab_server_particles(slab_server* s, int64_t id, int32_t* Np) {
+    if (!s || !Np) return SLAB_E_ARG;
+    return sguard(s, [&] {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(id);
+        sneed(it != s->reqs.end(), SLAB_E_NOTFOUND, "unknown request");
+        sneed(it->second.state != REQ_QUEUED || !it->second.has_release, SLAB_E_STATE, "the release has not been built yet");
+        *Np = it->second.Np;
     });
 }
 

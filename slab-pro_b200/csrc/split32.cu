@@ -477,9 +477,6 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     for (int k = 0; k < 4; ++k) h_ctl->pos_acc[k] = bin.box_bits[k];
     h_ctl->vmax2_bits = bin.vmax2_bits;
     h2d(ctl, h_ctl, 1, st);
-    double msum = 0;
-    for (int q = 0; q < Np; ++q) msum += m[q];
-    S.mass_fp64 = msum;
 
     Scn& D = host_scn[sid];
     D = Scn{};

@@ -52,6 +52,23 @@ class GridView(C.Structure):
                 ("a", C.POINTER(C.c_double))]
 
 
+class Release(C.Structure):
+    _fields_ = [("type", C.c_int32), ("pad_", C.c_int32), ("cx", C.c_double), ("cy", C.c_double), ("a", C.c_double),
+                ("b", C.c_double), ("rotation_deg", C.c_double), ("h0", C.c_double)]
+
+
+RELEASE_RECTANGLE, RELEASE_ELLIPSE = 0, 1
+
+
+def make_release(rel: dict) -> Release:
+    """A RECTANGLE / ELLIPSE release in the form of workloads.release_particles."""
+    if rel["type"] == "RECTANGLE":
+        return Release(RELEASE_RECTANGLE, 0, rel["center"][0], rel["center"][1], rel["Lx"], rel["Ly"], rel["rotation_deg"], rel["h0"])
+    if rel["type"] == "ELLIPSE":
+        return Release(RELEASE_ELLIPSE, 0, rel["center"][0], rel["center"][1], rel["rx"], rel["ry"], rel["rotation_deg"], rel["h0"])
+    raise ValueError(f"release type {rel['type']} is built on the host only")
+
+
 class Frame(C.Structure):
     _fields_ = [("frame", C.c_int32), ("Np", C.c_int32), ("time", C.c_double), ("particles", C.POINTER(C.c_float)),
                 ("Nx", C.c_int32), ("Ny", C.c_int32), ("i_off", C.c_int32), ("j_off", C.c_int32), ("grid", C.POINTER(C.c_float))]
@@ -84,6 +101,7 @@ def lib():
         L.slab_conservation.argtypes = [vp, dp]
         L.slab_moments.argtypes = [vp, dp]
         L.slab_frame_capture.argtypes = [vp, C.c_int32]
+        L.slab_upload_release.argtypes = [vp, C.POINTER(Release), C.POINTER(C.c_int32)]
         L.slab_frame_wait.argtypes = [vp, C.c_int32, C.POINTER(Frame)]
         L.slab_batch_moments.argtypes = [vp, C.c_int32, dp]
         L.slab_get_state.argtypes = [vp, dp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
@@ -180,6 +198,15 @@ class Slab:
         arrs = [np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "v", "vz", "h", "A", "mass", "z")]
         self._check(self.L.slab_upload_particles(self.h, n, *[_dp(a) for a in arrs]))
         self.Np = n
+
+    def upload_release(self, rel: dict) -> int:
+        """Particles of a RECTANGLE / ELLIPSE release (UNIFORM sampling) built
+        on the device; returns their count."""
+        r = make_release(rel)
+        n = C.c_int32()
+        self._check(self.L.slab_upload_release(self.h, C.byref(r), C.byref(n)))
+        self.Np = n.value
+        return n.value
 
     def initial_pass(self):
         self._check(self.L.slab_initial_pass(self.h))
@@ -300,6 +327,9 @@ class Batch:
         L.slab_batch_create.argtypes = [C.POINTER(TerrainDesc), dp, C.c_int32, C.c_int64, C.POINTER(vp)]
         L.slab_batch_set_stream.argtypes = [vp, vp]
         L.slab_batch_add.argtypes = [vp, C.POINTER(Params), C.c_int32] + [dp] * 7 + [C.POINTER(C.c_int32)]
+        L.slab_batch_add_release.argtypes = [vp, C.POINTER(Params), C.POINTER(Release), C.POINTER(C.c_int32)]
+        L.slab_batch_scenario_particles.argtypes = [vp, C.c_int32]
+        L.slab_batch_scenario_particles.restype = C.c_int32
         L.slab_batch_run.argtypes = [vp, C.c_int64, C.POINTER(C.c_int64)]
         L.slab_batch_state.argtypes = [vp, C.c_int32, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
         L.slab_batch_scenario_status.argtypes = [vp, C.c_int32]
@@ -350,6 +380,16 @@ class Batch:
         sid = C.c_int32()
         self._check(self.L.slab_batch_add(self.h, C.byref(prm), n, *[_dp(a) for a in arrs], C.byref(sid)))
         self.Np.append(n)
+        return sid.value
+
+    def add_release(self, cfg: dict, rel: dict) -> int:
+        """A scenario whose particles are built on the device from a release."""
+        prm = make_params(cfg, FP32_SPLIT)
+        self._params.append(prm)
+        r = make_release(rel)
+        sid = C.c_int32()
+        self._check(self.L.slab_batch_add_release(self.h, C.byref(prm), C.byref(r), C.byref(sid)))
+        self.Np.append(self.L.slab_batch_scenario_particles(self.h, sid.value))
         return sid.value
 
     def run(self, max_steps: int = 1 << 40) -> int:
@@ -439,6 +479,8 @@ class Server:
         dp = C.POINTER(C.c_double)
         L.slab_server_create.argtypes = [C.POINTER(TerrainDesc), dp, C.POINTER(ServerConfig), C.POINTER(vp)]
         L.slab_server_submit.argtypes = [vp, C.POINTER(Params), C.c_int32] + [dp] * 7 + [C.POINTER(C.c_int64)]
+        L.slab_server_submit_release.argtypes = [vp, C.POINTER(Params), C.POINTER(Release), C.POINTER(C.c_int64)]
+        L.slab_server_particles.argtypes = [vp, C.c_int64, C.POINTER(C.c_int32)]
         L.slab_server_poll.argtypes = [vp, C.c_int64, C.POINTER(C.c_int32), dp]
         L.slab_server_wait.argtypes = [vp, C.c_int64, C.c_double]
         L.slab_server_result.argtypes = [vp, C.c_int64, C.POINTER(C.c_int32), dp, dp, C.c_int64, dp, dp, dp, dp, dp]
@@ -481,6 +523,16 @@ class Server:
         self.Np[rid.value] = n
         return rid.value
 
+    def submit_release(self, cfg: dict, rel: dict) -> int:
+        """Queue a scenario given as a release; its particles are built on the
+        device at admission."""
+        prm = make_params(cfg, FP32_SPLIT)
+        r = make_release(rel)
+        rid = C.c_int64()
+        self._check(self.L.slab_server_submit_release(self.h, C.byref(prm), C.byref(r), C.byref(rid)))
+        self.Np[rid.value] = None  # known once admitted
+        return rid.value
+
     def poll(self, rid: int):
         st, t = C.c_int32(), C.c_double()
         self._check(self.L.slab_server_poll(self.h, rid, C.byref(st), C.byref(t)))
@@ -496,6 +548,10 @@ class Server:
         nI, nJ = box[1] - box[0] + 1, box[3] - box[2] + 1
         cap = max(nI, 0) * max(nJ, 0)
         n = self.Np[rid]
+        if n is None:
+            k = C.c_int32()
+            self._check(self.L.slab_server_particles(self.h, rid, C.byref(k)))
+            n = self.Np[rid] = k.value
         hm, vm = np.zeros(max(cap, 1)), np.zeros(max(cap, 1))
         x, v, h, m = np.zeros(2 * n), np.zeros(2 * n), np.zeros(n), np.zeros(n)
         self._check(self.L.slab_server_result(self.h, rid, box, _dp(hm), _dp(vm), cap, _dp(x), _dp(v), _dp(h), _dp(m), _dp(info)))
