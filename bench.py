@@ -71,6 +71,8 @@ def load_workload(name: str):
         return W.config2()
     if name == "c3":
         return W.config3()
+    if name == "c3s":
+        return W.config3_small()
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -615,6 +617,22 @@ def ensemble(args, stream, dev):
         else:
             seq[name]["batched_equals_alone_bitwise"] = same
     out.update(seq)
+    # whole-run accuracy with the FP64 envelope on a stratified sample (the batch gives each
+    # scenario the bits of its solo FP32 run, checked above)
+    if args.c4_acc_sample > 0 and ok:
+        import accuracy as Acc2
+        rows32, rows_env = [], []
+        for i in [ok[q] for q in _stratified(Nps[ok], args.c4_acc_sample)]:
+            cfg, P = scen[i]
+            try:
+                a = accuracy_block(z, dx, cfg, P, stream)
+            except slab.SlabError:
+                continue
+            rows32.append(a["fp32_vs_fp64"])
+            rows_env.append(a["fp64_envelope"])
+        out["accuracy"] = {"scenarios": len(rows32), "fp32_vs_fp64": Acc2.summarize(rows32), "fp64_envelope": Acc2.summarize(rows_env),
+                           "note": "worst case over the sample; fp64_envelope: FP64 against FP64 started from positions moved by "
+                                   "up to 1e-7 dx"}
     f64 = seq["fp64_sequential"]
     out["speedup_vs_fp64_sequential"] = {"device": round(out["fp32_batched"]["scenarios_per_s"] / f64["scenarios_per_s"], 2),
                                          "e2e": round(out["fp32_batched"]["e2e_scenarios_per_s"] / f64["e2e_scenarios_per_s"], 2)}
@@ -834,7 +852,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c3s"],
+                    help="c3s: a smaller config-3 case for kernel captures")
     ap.add_argument("--spinup", type=float, default=2.0, help="simulated seconds of the developed-flow measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 whole-run accuracy blocks")
     ap.add_argument("--no-envelope", action="store_true", help="skip the FP64 envelope run of the headline accuracy block")
@@ -849,6 +868,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served-stream section (config 5)")
     ap.add_argument("--c4-scenarios", type=int, default=256)
     ap.add_argument("--c4-sample", type=int, default=16, help="scenarios run one after another for the sequential rates")
+    ap.add_argument("--c4-acc-sample", type=int, default=8, help="scenarios of the whole-run accuracy block (with the FP64 envelope)")
     ap.add_argument("--c5-window", type=float, default=20.0, help="seconds of Poisson arrivals (the full stream is 300 s)")
     ap.add_argument("--c5-slots", type=int, default=512)
     ap.add_argument("--c5-sample", type=int, default=12, help="requests timed on the plain FP64 path")

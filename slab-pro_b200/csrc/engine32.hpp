@@ -38,6 +38,8 @@ class Engine32 {
     void launch_step();
     void launch_kernel(int k, const Shared& sh);
     void launch_p2g(const Shared& sh);
+    void launch_p2g_cell(const Shared& sh, int cls);
+    bool p2g_tma = false;  // k_p2g_cell<true>: the next tile's loads staged by TMA bulk copies (SLAB_P2G_TMA=1)
     void arm(int64_t steps_left, int stop_at_frame);
     int acc_mode = 5;  // P2G scheme (k32::ACC_*): dense tiles cell-sorted, sparse tiles fixed point
     int split_min = 3 * NCELL / 4;  // ACC_MIXED: tiles with more particles take the cell-sorted P2G (measured)

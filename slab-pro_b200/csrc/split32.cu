@@ -181,7 +181,9 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g<k32::ACC_I64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2GSmem)));
-    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_cell, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2CSmem)));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_cell<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2CSmem)));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_cell<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2CSmemTma)));
+    if (const char* e = std::getenv("SLAB_P2G_TMA")) p2g_tma = std::atoi(e) != 0;
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(k32::P2W_WARPS * sizeof(k32::P2WWarp))));
     if (const char* e = std::getenv("SLAB_P2G_ACC")) acc_mode = std::atoi(e);
@@ -193,7 +195,10 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k32::k_p2g_warp, k32::P2W_THREADS,
                                                             k32::P2W_WARPS * sizeof(k32::P2WWarp)));
     int occ_c = 0, occ_h = 0;
-    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k32::k_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem)));
+    if (p2g_tma)
+        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k32::k_p2g_cell<true>, k32::P2C_THREADS, sizeof(k32::P2CSmemTma)));
+    else
+        SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, k32::k_p2g_cell<false>, k32::P2C_THREADS, sizeof(k32::P2CSmem)));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k32::k_p2g<k32::ACC_HILO>, k32::P2G_THREADS, sizeof(k32::P2GSmem)));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, k32::k_g2p, NCELL, 0));
     SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k32::k_grid, NCELL, 0));
@@ -411,14 +416,15 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     const bool new_parts = S.Np_alloc < Np, new_lists = S.act_alloc < S.act_cap, new_tiles = !S.blk_of;
     for (int b = 0; b < 2; ++b) {
         if (new_parts) {
-            S.cell[b] = dalloc<int32_t>(Np);
-            S.f[b] = dalloc<float2>(Np);
-            S.v[b] = dalloc<float2>(Np);
-            S.h[b] = dalloc<float>(Np);
-            S.m[b] = dalloc<float>(Np);
-            S.id[b] = dalloc<int32_t>(Np);
-            S.vz[b] = dalloc<float>(Np);
-            S.z[b] = dalloc<float>(Np);
+            // padded past Np: P2G's bulk copies round a range's end up to 16 bytes
+            S.cell[b] = dalloc<int32_t>(Np + PARTICLE_PAD);
+            S.f[b] = dalloc<float2>(Np + PARTICLE_PAD);
+            S.v[b] = dalloc<float2>(Np + PARTICLE_PAD);
+            S.h[b] = dalloc<float>(Np + PARTICLE_PAD);
+            S.m[b] = dalloc<float>(Np + PARTICLE_PAD);
+            S.id[b] = dalloc<int32_t>(Np + PARTICLE_PAD);
+            S.vz[b] = dalloc<float>(Np + PARTICLE_PAD);
+            S.z[b] = dalloc<float>(Np + PARTICLE_PAD);
         }
         if (new_tiles) S.grp[b] = dalloc<int32_t>((size_t)ntiles * GRP_STRIDE);
         if (new_lists) S.act_list[b] = dalloc<int32_t>(S.act_cap);
@@ -531,14 +537,23 @@ void Engine32::launch_t0() {
     pending_blocks = 0;  // later reads of the pool count see these blocks
 }
 
+// the cell-sorted P2G; SLAB_P2G_TMA=1 stages the next tile's loads with TMA
+// bulk copies (same sums, in the same order)
+void Engine32::launch_p2g_cell(const Shared& sh, int cls) {
+    if (p2g_tma)
+        k32::k_p2g_cell<true><<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmemTma), st>>>(sh, cls);
+    else
+        k32::k_p2g_cell<false><<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, cls);
+}
+
 void Engine32::launch_p2g(const Shared& sh) {
     if (acc_mode == k32::ACC_MIXED) {  // dense tiles, then sparse tiles
-        k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, 0);
+        launch_p2g_cell(sh, 0);
         k32::k_p2g_sparse<<<grid_p2g_sparse, k32::P2S_THREADS, sizeof(k32::P2SSmem), st>>>(sh, 1);
     } else if (acc_mode == k32::ACC_WARP) {
         k32::k_p2g_warp<<<grid_p2g, k32::P2W_THREADS, k32::P2W_WARPS * sizeof(k32::P2WWarp), st>>>(sh, -1);
     } else if (acc_mode == k32::ACC_CELL) {
-        k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, -1);
+        launch_p2g_cell(sh, -1);
     } else if (acc_mode == k32::ACC_I32) {
         k32::k_p2g<k32::ACC_I32><<<grid_p2g_hilo, k32::P2G_THREADS, sizeof(k32::P2GSmem), st>>>(sh, -1);
     } else if (acc_mode == k32::ACC_I64) {
@@ -599,7 +614,7 @@ void Engine32::launch_step_timed(const Shared& sh, cudaEvent_t* e) {
     SLAB_CUDA(cudaEventRecord(e[0], st));
     k32::k_prep<<<grid_prep, 256, 0, st>>>(sh);
     SLAB_CUDA(cudaEventRecord(e[1], st));
-    k32::k_p2g_cell<<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, 0);
+    launch_p2g_cell(sh, 0);
     SLAB_CUDA(cudaEventRecord(e[2], st));
     k32::k_p2g_sparse<<<grid_p2g_sparse, k32::P2S_THREADS, sizeof(k32::P2SSmem), st>>>(sh, 1);
     SLAB_CUDA(cudaEventRecord(e[3], st));

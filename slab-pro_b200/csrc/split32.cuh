@@ -38,6 +38,7 @@ constexpr int NCELL = TILE * TILE;    // cells per tile = threads per CTA
 constexpr int NQ = 7;                 // P2G sums: m, m vx, m vy, m h, Fx, Fy, m vz
 constexpr int PART_STRIDE = NQ * TN * TN;  // floats per tile partial
 constexpr int CHUNK = 1024;           // particles staged per pass of P2G/G2P
+constexpr int PARTICLE_PAD = 16;      // elements allocated past the last particle of every particle array
 
 __host__ __device__ inline int32_t pack_cell(int ib, int jb) { return (ib << 16) | jb; }
 __host__ __device__ inline int cell_i(int32_t c) { return (int)((uint32_t)c >> 16); }

@@ -25,7 +25,10 @@
 // reproducible, alone or inside a batch.
 #pragma once
 
+#include <type_traits>
+
 #include "split32.cuh"
+#include "tma.cuh"
 
 namespace slab {
 namespace k32 {
@@ -127,7 +130,9 @@ __device__ __forceinline__ int cand_to_index(int q, const TileDesc& D, int& d) {
     return D.rstart[d] + (q - D.rpref[d]);
 }
 
-// copy a descriptor to shared memory (threads 0..23)
+constexpr int DESC_WORDS = (int)(sizeof(TileDesc) / 4);
+
+// copy a descriptor to shared memory (threads 0..27)
 __device__ __forceinline__ void load_desc(const TileDesc* g, TileDesc* s) {
     if (threadIdx.x < (int)(sizeof(TileDesc) / 4)) reinterpret_cast<int*>(s)[threadIdx.x] = reinterpret_cast<const int*>(g)[threadIdx.x];
 }
@@ -819,7 +824,91 @@ struct P2CSmem {
     int wcur[P2C_WARPS][NCELL];  // per-warp cell counts, then per-warp write cursors
     int s_warp[33];
     TileDesc d;
+    // the scenario of the CTA's current run of tiles (loaded when it changes)
+    PBuf B;             // current particle buffer
+    int32_t* nxt_cell;  // cell array of the next buffer (sorted index lists of large tiles)
+    Ctl* ctl;
+    float g, hod;
+    int csid, outs;
 };
+
+// Bulk-copy staging of the next tile (k_p2g_cell<true>): its 9 candidate
+// ranges of the particle arrays, each rounded out to 16-byte boundaries, and
+// its terrain window, copied by the TMA engine while the current tile is
+// summed. 4-byte arrays take at most 6 extra elements per range, 8-byte ones 2.
+constexpr int P2C_SCAP4 = (P2C_CAP + 9 * 6 + 3) / 4 * 4;
+constexpr int P2C_SCAP8 = (P2C_CAP + 9 * 2 + 1) / 2 * 2;
+constexpr int DEM_W = TILE + 1;  // terrain window edge (nodes)
+
+struct alignas(16) P2CTmaStage {
+    int32_t cell[P2C_SCAP4];
+    float h[P2C_SCAP4];
+    float m[P2C_SCAP4];
+    float vz[P2C_SCAP4];
+    float2 f[P2C_SCAP8];
+    float2 v[P2C_SCAP8];
+};
+static_assert(P2C_SCAP4 * 4 % 16 == 0 && P2C_SCAP8 * 8 % 16 == 0, "16-byte aligned stage arrays");
+
+struct P2CSmemTma : P2CSmem {
+    P2CTmaStage ts;                             // the tile's candidates (until its phase 1 has read them)
+    alignas(16) float4 dem2[2][DEM_W * DEM_W];  // terrain windows of this and the next tile
+    alignas(8) uint64_t bar;                    // completion of the staged copies
+    TileDesc dnext;                             // the next tile's descriptor
+    int lead4[9], lead8[9];                     // stage index of each range's first candidate (4-byte / 8-byte arrays)
+    int use_stage, dem_staged[2];               // the tile's candidates / terrain windows came by bulk copy
+};
+
+// Thread 0: lays out the 9 ranges of tile D in the stage and starts their
+// bulk copies (and the terrain window's rows into dem2[slot]) on sm.bar.
+// Candidates that do not fit leave the tile to the load path (use_stage 0).
+// The particle arrays are padded past Np, so a range rounded up to 16 bytes
+// stays inside its allocation.
+__device__ __forceinline__ void p2c_issue_stage(P2CSmemTma& sm, const TileDesc& D, const PBuf& B, bool outs, const Shared& sh, int slot) {
+    int o4 = 0, o8 = 0;
+    bool fit = D.rpref[9] <= P2C_CAP;
+    int a4[9], n4[9], a8[9], n8[9];
+#pragma unroll
+    for (int d = 0; d < 9; ++d) {
+        const int rs = D.rstart[d], rl = D.rpref[d + 1] - D.rpref[d];
+        a4[d] = rs & ~3;
+        n4[d] = rl > 0 ? ((rs + rl + 3) & ~3) - a4[d] : 0;
+        a8[d] = rs & ~1;
+        n8[d] = rl > 0 ? ((rs + rl + 1) & ~1) - a8[d] : 0;
+        sm.lead4[d] = o4 + (rs - a4[d]);
+        sm.lead8[d] = o8 + (rs - a8[d]);
+        o4 += n4[d];
+        o8 += n8[d];
+    }
+    if (o4 > P2C_SCAP4 || o8 > P2C_SCAP8) fit = false;
+    // the terrain window by rows when it lies inside the terrain
+    const int ti = D.t / sh.TY, tj = D.t % sh.TY;
+    const bool dem_in = ti * TILE + TILE < sh.Nx && tj * TILE + TILE < sh.Ny;
+    sm.dem_staged[slot] = dem_in ? 1 : 0;
+    sm.use_stage = fit ? 1 : 0;
+    uint32_t bytes = dem_in ? DEM_W * DEM_W * 16 : 0;
+    if (fit) bytes += (uint32_t)o4 * 4u * (outs ? 4u : 3u) + (uint32_t)o8 * 8u * 2u;
+    tma::fence_proxy_async();  // the CTA's earlier ordinary reads of these bytes come first
+    tma::mbar_arrive_expect_tx(&sm.bar, bytes);
+    if (dem_in)
+        for (int r = 0; r < DEM_W; ++r)
+            tma::bulk_g2s(&sm.dem2[slot][r * DEM_W], sh.dem + (int64_t)(ti * TILE + r) * sh.Ny + tj * TILE, DEM_W * 16, &sm.bar);
+    if (!fit) return;
+    int q4 = 0, q8 = 0;
+#pragma unroll
+    for (int d = 0; d < 9; ++d) {
+        if (n4[d]) {
+            tma::bulk_g2s(sm.ts.cell + q4, B.cell + a4[d], n4[d] * 4, &sm.bar);
+            tma::bulk_g2s(sm.ts.h + q4, B.h + a4[d], n4[d] * 4, &sm.bar);
+            tma::bulk_g2s(sm.ts.m + q4, B.m + a4[d], n4[d] * 4, &sm.bar);
+            if (outs) tma::bulk_g2s(sm.ts.vz + q4, B.vz + a4[d], n4[d] * 4, &sm.bar);
+            tma::bulk_g2s(sm.ts.f + q8, B.f + a8[d], n8[d] * 8, &sm.bar);
+            tma::bulk_g2s(sm.ts.v + q8, B.v + a8[d], n8[d] * 8, &sm.bar);
+        }
+        q4 += n4[d];
+        q8 += n8[d];
+    }
+}
 
 // P2G quantities of a staged particle (as load_pq)
 __device__ __forceinline__ PQ staged_pq(float4 a, float2 v, float vz, int li, int lj, const float4* dem, float g, float hod) {
@@ -867,8 +956,9 @@ __device__ __forceinline__ void add_particle_row(float (&acc)[NQ][3], const PQ& 
 // memory, or (tiles over P2C_CAP candidates) read through the sorted index
 // list in global memory.
 template <bool OUTS, int A>
-__device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, const P2CSmem& sm, const int32_t* __restrict__ order,
-                                              int c0, int nn, const PBuf& B, int li, int lj, float g, float hod) {
+__device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, const P2CSmem& sm, const float4* dem,
+                                              const int32_t* __restrict__ order, int c0, int nn, const PBuf& B, int li, int lj, float g,
+                                              float hod) {
 #pragma unroll
     for (int q = 0; q < NQ; ++q)
 #pragma unroll
@@ -876,7 +966,7 @@ __device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, 
     if (staged) {
         for (int r = c0; r < c0 + nn; ++r) {
             const int k = sm.idx[r];
-            add_particle_row<OUTS, A>(acc, staged_pq(sm.st.sa[k], sm.st.sv[k], sm.st.svz[k], li, lj, sm.dem, g, hod));
+            add_particle_row<OUTS, A>(acc, staged_pq(sm.st.sa[k], sm.st.sv[k], sm.st.svz[k], li, lj, dem, g, hod));
         }
         return;
     }
@@ -884,7 +974,7 @@ __device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, 
     for (int r = 0; r < nn; ++r) {
         const int src = nsrc;
         if (r + 1 < nn) nsrc = order[c0 + r + 1];
-        add_particle_row<OUTS, A>(acc, load_pq(B, src, li, lj, sm.dem, g, hod, OUTS));
+        add_particle_row<OUTS, A>(acc, load_pq(B, src, li, lj, dem, g, hod, OUTS));
     }
 }
 
@@ -892,10 +982,11 @@ __device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, 
 // receives the row sum of exactly one cell, so the rounds need no atomics and
 // every node adds its <= 9 cells in (a, b) order.
 template <bool OUTS, int A>
-__device__ __forceinline__ void p2c_row(P2CSmem& sm, bool staged, const int32_t* __restrict__ order, int c0, int nn, const PBuf& B,
+__device__ __forceinline__ void p2c_row(P2CSmem& sm, bool staged, const float4* dem, const int32_t* __restrict__ order, int c0, int nn,
+                                        const PBuf& B,
                                         int li, int lj, float g, float hod) {
     float acc[NQ][3];
-    cell_row_sums<OUTS, A>(acc, staged, sm, order, c0, nn, B, li, lj, g, hod);
+    cell_row_sums<OUTS, A>(acc, staged, sm, dem, order, c0, nn, B, li, lj, g, hod);
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
         __syncthreads();
@@ -906,11 +997,12 @@ __device__ __forceinline__ void p2c_row(P2CSmem& sm, bool staged, const int32_t*
 }
 
 template <bool OUTS>
-__device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const int32_t* __restrict__ order, int c0, int nn, const PBuf& B,
+__device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const float4* dem, const int32_t* __restrict__ order, int c0, int nn,
+                                         const PBuf& B,
                                          int li, int lj, float g, float hod) {
-    p2c_row<OUTS, 0>(sm, staged, order, c0, nn, B, li, lj, g, hod);
-    p2c_row<OUTS, 1>(sm, staged, order, c0, nn, B, li, lj, g, hod);
-    p2c_row<OUTS, 2>(sm, staged, order, c0, nn, B, li, lj, g, hod);
+    p2c_row<OUTS, 0>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+    p2c_row<OUTS, 1>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+    p2c_row<OUTS, 2>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
 }
 
 // K2: P2G of one tile (src/simulation.cpp:726-798) as a segmented reduction
@@ -935,36 +1027,120 @@ __device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const int32_t
 // reproducible and the same alone or inside a batch. A tile costs two
 // dependent rounds of global loads (descriptor, candidates); each CTA takes
 // a contiguous run of work items.
-__global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared sh, int cls) {
+// With TMA = true the loads of a tile leave its critical path: while tile n
+// is summed (phases 2-5), thread 0 has the TMA engine copy tile n+1's
+// candidate ranges and terrain window into shared memory (p2c_issue_stage),
+// and the descriptor after that is read into registers. Tiles whose
+// candidates do not fit the stage load them as before.
+
+// the CTA's scenario values for a run of its tiles (thread 0)
+template <typename Sm> __device__ __forceinline__ void p2c_load_scenario(Sm& sm, const Shared& sh, int sid) {
+    const Scn& S = sh.scn[sid];
+    const SCnt* n = S.cnt;
+    const int cur = n->seq & 1;
+    sm.B = S.buf[cur];
+    sm.nxt_cell = S.buf[cur ^ 1].cell;
+    sm.ctl = S.ctl;
+    sm.g = S.g;
+    sm.hod = 0.5f * S.ood;
+    sm.outs = n->outs != 0;
+    sm.csid = sid;
+}
+
+// thread 0: the copies of the tile in sm.dnext, from its scenario's buffer
+__device__ __forceinline__ void p2c_issue_next(P2CSmemTma& sm, const Shared& sh, int slot) {
+    const TileDesc& D = sm.dnext;
+    if (D.sid == sm.csid) {
+        p2c_issue_stage(sm, D, sm.B, sm.outs != 0, sh, slot);
+    } else {
+        const Scn& S = sh.scn[D.sid];
+        const SCnt* n = S.cnt;
+        p2c_issue_stage(sm, D, S.buf[n->seq & 1], n->outs != 0, sh, slot);
+    }
+}
+
+// candidate k of tile D: its range and its position in that range
+__device__ __forceinline__ int cand_range(int k, const TileDesc& D, int& off) {
+    int d = 0;
+    while (d < 8 && D.rpref[d + 1] <= k) ++d;
+    off = k - D.rpref[d];
+    return d;
+}
+
+constexpr int P2C_TMA_MIN_BLOCKS = NCELL == 64 ? 6 : 2;  // the stage doubles the shared memory of a CTA
+
+template <bool TMA>
+__global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MIN_BLOCKS) k_p2g_cell(Shared sh, int cls) {
+    using Sm = typename std::conditional<TMA, P2CSmemTma, P2CSmem>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    P2CSmem& sm = *reinterpret_cast<P2CSmem*>(smem_raw);
+    Sm& sm = *reinterpret_cast<Sm*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const int li = tid / TILE, lj = tid % TILE;
     int i0, i1;
     work_range(p2g_count(sh, cls), i0, i1);
+    // the first descriptor now; each later one is read while the tile before it runs
+    int w_cur = i0 < i1 ? p2g_item(sh, cls, i0) : 0;
+    int w_nxt = i0 + 1 < i1 ? p2g_item(sh, cls, i0 + 1) : 0;
+    if (i0 < i1) load_desc(sh.desc + w_cur, &sm.d);
+    if (tid == 0) {
+        sm.csid = -1;
+        if constexpr (TMA) {
+            tma::mbar_init(&sm.bar, 1);
+            tma::fence_mbar_init();
+        }
+    }
+    __syncthreads();
+    if constexpr (TMA) {
+        if (tid == 0 && i0 < i1) {  // the first tile's copies
+            p2c_load_scenario(sm, sh, sm.d.sid);
+            sm.dnext = sm.d;
+            p2c_issue_next(sm, sh, 0);
+        }
+    }
     SLAB_PHASE_BEGIN;
-    for (int i = i0; i < i1; ++i) {
-        const int w = p2g_item(sh, cls, i);
-        load_desc(sh.desc + w, &sm.d);
+    for (int i = i0, n = 0; i < i1; ++i, ++n) {
+        const int w = w_cur;
         for (int k = tid; k < P2C_WARPS * NCELL; k += P2C_THREADS) (&sm.wcur[0][0])[k] = 0;
         for (int k = tid; k < NQ * TN * TN; k += P2C_THREADS) sm.nsum[k] = 0.f;
         __syncthreads();
         SLAB_PHASE_MARK(0);
-        const Scn& S = sh.scn[sm.d.sid];
+        // the next tile's descriptor (one word per thread) and the item after it
+        int dn = 0, w_nn = 0;
+        if (i + 1 < i1 && tid < DESC_WORDS) dn = reinterpret_cast<const int*>(sh.desc + w_nxt)[tid];
+        if (i + 2 < i1) w_nn = p2g_item(sh, cls, i + 2);
+        if (sm.d.sid != sm.csid) {  // uniform: a new scenario in this CTA's run
+            __syncthreads();
+            if (tid == 0) p2c_load_scenario(sm, sh, sm.d.sid);
+            __syncthreads();
+        }
         const int t = sm.d.t;
         const int ti = t / sh.TY, tj = t % sh.TY;
-        SCnt* n = S.cnt;
-        const int cur = n->seq & 1;
-        const bool outs = n->outs != 0;
-        for (int k = tid; k < (TILE + 1) * (TILE + 1); k += P2C_THREADS) {
-            const int i = ti * TILE + k / (TILE + 1), j = tj * TILE + k % (TILE + 1);
-            sm.dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
+        const bool outs = sm.outs != 0;
+        Ctl* const ctl = sm.ctl;
+        float4* dem;
+        bool from_stage = false;
+        if constexpr (TMA) {
+            const int slot = n & 1;
+            dem = sm.dem2[slot];
+            if (!tma::mbar_wait(&sm.bar, (uint32_t)(n & 1))) atomicOr(&ctl->err, ERR_TIMEOUT);  // this tile's copies
+            from_stage = sm.use_stage != 0;
+            if (!sm.dem_staged[slot])
+                for (int k = tid; k < DEM_W * DEM_W; k += P2C_THREADS) {
+                    const int i = ti * TILE + k / DEM_W, j = tj * TILE + k % DEM_W;
+                    dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
+                }
+        } else {
+            dem = sm.dem;
+            for (int k = tid; k < DEM_W * DEM_W; k += P2C_THREADS) {
+                const int i = ti * TILE + k / DEM_W, j = tj * TILE + k % DEM_W;
+                dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
+            }
         }
         const int ncand = sm.d.rpref[9];
         const int total = sm.d.total;
         const bool staged = ncand <= P2C_CAP;
-        const PBuf B = S.buf[cur];
+        const PBuf B = sm.B;
         const int per = (ncand + P2C_WARPS - 1) / P2C_WARPS;
         const int k_lo = min(warp * per, ncand), k_hi = min(k_lo + per, ncand);
         // 1. load (stage) and count per (warp, cell)
@@ -973,20 +1149,35 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
             int lc = -1;
             if (k < k_hi) {
                 int d;
-                const int src = cand_to_index(k, sm.d, d);
-                const int32_t cell = B.cell[src];
-                float2 f, v;
-                float m, h, vz = 0.f;
-                if (staged) {  // issued together with the cell load
-                    f = B.f[src];
-                    v = B.v[src];
-                    m = B.m[src];
-                    h = B.h[src];
-                    if (outs) vz = B.vz[src];
+                int32_t cell;
+                float2 f = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
+                float m = 0.f, h = 0.f, vz = 0.f;
+                if (TMA && from_stage) {  // from the bulk-copied stage
+                    int off;
+                    d = cand_range(k, sm.d, off);
+                    if constexpr (TMA) {
+                        const int s4 = sm.lead4[d] + off, s8 = sm.lead8[d] + off;
+                        cell = sm.ts.cell[s4];
+                        f = sm.ts.f[s8];
+                        v = sm.ts.v[s8];
+                        m = sm.ts.m[s4];
+                        h = sm.ts.h[s4];
+                        if (outs) vz = sm.ts.vz[s4];
+                    }
+                } else {
+                    const int src = cand_to_index(k, sm.d, d);
+                    cell = B.cell[src];
+                    if (staged) {  // issued together with the cell load
+                        f = B.f[src];
+                        v = B.v[src];
+                        m = B.m[src];
+                        h = B.h[src];
+                        if (outs) vz = B.vz[src];
+                    }
                 }
                 const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
                 if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
-                else if (d == 4) atomicOr(&S.ctl->err, ERR_MOVE);  // a stayer outside its tile
+                else if (d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
                 if (staged) {
                     sm.lc[k] = (int16_t)lc;
                     if (lc >= 0) {
@@ -1003,7 +1194,14 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
             }
             __syncwarp();
         }
+        if constexpr (TMA) {
+            if (tid < DESC_WORDS) reinterpret_cast<int*>(&sm.dnext)[tid] = dn;
+        }
         __syncthreads();
+        if constexpr (TMA) {
+            // the stage is free: the next tile's copies run beside phases 2-5 of this one
+            if (tid == 0 && i + 1 < i1) p2c_issue_next(sm, sh, (n + 1) & 1);
+        }
         SLAB_PHASE_MARK(1);
         // 2. cursors: cell-major, warp-minor
         int n_c = 0;
@@ -1014,13 +1212,13 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
             n_c += x;
         }
         const int c0 = block_exclusive_scan(n_c, sm.s_warp);
-        if (tid == P2C_THREADS - 1 && c0 + n_c != total) atomicOr(&S.ctl->err, ERR_CAPACITY);
+        if (tid == P2C_THREADS - 1 && c0 + n_c != total) atomicOr(&ctl->err, ERR_CAPACITY);
 #pragma unroll
         for (int q = 0; q < P2C_WARPS; ++q) sm.wcur[q][tid] += c0;
         __syncthreads();
         SLAB_PHASE_MARK(2);
         // 3. stable placement by cell
-        int32_t* order = S.buf[cur ^ 1].cell + sm.d.nxt_off;
+        int32_t* order = sm.nxt_cell + sm.d.nxt_off;
         for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
             const int k = k0 + lane;
             int lc = -1, src = 0;
@@ -1040,7 +1238,7 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
             if (lc >= 0) {
                 peers = __match_any_sync(vm, lc);
                 const int pos = sm.wcur[warp][lc] + __popc(peers & lt);
-                if (pos >= total) atomicOr(&S.ctl->err, ERR_CAPACITY);
+                if (pos >= total) atomicOr(&ctl->err, ERR_CAPACITY);
                 else if (staged) sm.idx[pos] = (int16_t)k;
                 else order[pos] = src;
             }
@@ -1053,9 +1251,9 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
         // 4. per-cell row sums into the node sums
         {
             const int nn = max(0, min(n_c, total - c0));
-            const float g = S.g, hod = 0.5f * S.ood;
-            if (outs) p2c_rows<true>(sm, staged, order, c0, nn, B, li, lj, g, hod);
-            else p2c_rows<false>(sm, staged, order, c0, nn, B, li, lj, g, hod);
+            const float g = sm.g, hod = sm.hod;
+            if (outs) p2c_rows<true>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+            else p2c_rows<false>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
         }
         __syncthreads();
         SLAB_PHASE_MARK(4);
@@ -1063,6 +1261,9 @@ __global__ void __launch_bounds__(P2C_THREADS, P2C_MIN_BLOCKS) k_p2g_cell(Shared
         float* P = sh.part + (size_t)w * PART_STRIDE;
         for (int k = tid; k < PART_STRIDE; k += P2C_THREADS) P[k] = sm.nsum[k];
         __syncthreads();
+        if (i + 1 < i1 && tid < DESC_WORDS) reinterpret_cast<int*>(&sm.d)[tid] = dn;
+        w_cur = w_nxt;
+        w_nxt = w_nn;
         SLAB_PHASE_MARK(5);
         SLAB_PHASE_TILE();
     }
@@ -1088,7 +1289,6 @@ constexpr int P2S_MIN_BLOCKS = NCELL == 64 ? 16 : 4;
 constexpr int P2S_CAP = NCELL;  // particles of a sparse tile (split_min is capped to it)
 constexpr int P2S_DEMW = (TILE + 1) * (TILE + 1);
 constexpr int P2S_DEM_PER = (P2S_DEMW + P2S_THREADS - 1) / P2S_THREADS;
-constexpr int DESC_WORDS = (int)(sizeof(TileDesc) / 4);
 static_assert(DESC_WORDS <= P2S_THREADS, "one descriptor word per thread");
 
 struct P2SSmem {

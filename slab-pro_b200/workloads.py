@@ -441,6 +441,19 @@ def config3(seed: int = 2027):
     return {"name": "fractal8192_dx05_ellipse_uniform_mui", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}
 
 
+def config3_small(seed: int = 2027):
+    """A smaller case of config 3 for kernel captures: the same construction
+    on a 4096^2 DEM at 0.5 m, a 900 x 600 m ellipse (h0 = 3 m, ~6.8 M
+    particles, more than the L2 holds), mu(I) as config 3."""
+    dx = 0.5
+    z = fractal_slope_dem(4096, dx, seed=seed, rms=7.5, rim_m=RIM_M)
+    cfg = dict(gravity=9.81, rho=1500.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=90.0,
+               friction="MU_I", mui_mu1=0.38, mui_mu2=0.64, mui_I0=0.279, mui_d=5e-4, mui_phi=0.6)
+    rel = {"type": "ELLIPSE", "center": (700.0, 1024.0), "rx": 450.0, "ry": 300.0, "rotation_deg": 0.0, "h0": 3.0}
+    P = release_particles(z, dx, rel, cfg["rho"], fast_theta=True)
+    return {"name": "fractal4096_dx05_ellipse_uniform_mui", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}
+
+
 def config4(n_scenarios: int = 256, seed: int = 2028):
     """Ensemble on a shared 2048^2 DEM at 2 m (fractal-slope construction,
     roughness 7.5 m RMS): elliptical releases with semi-axes U(20, 300) m,

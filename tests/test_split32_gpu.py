@@ -120,3 +120,25 @@ def test_frames_particle_positions_close():
     com = (P["x"] * P["mass"][:, None]).sum(0) / P["mass"].sum()
     como = (Po["x"] * Po["mass"][:, None]).sum(0) / Po["mass"].sum()
     assert np.abs(com - como).max() < c["dx"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_tma_staged_p2g_equals_load_path(name, monkeypatch):
+    """The cell-sorted P2G with the next tile's loads staged by TMA bulk
+    copies (SLAB_P2G_TMA=1) and with plain loads (SLAB_P2G_TMA=0) sum the
+    same values in the same order: bitwise-equal runs."""
+    c = cases.CASES[name]()
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("SLAB_P2G_TMA", flag)
+        s = _gpu(c)
+        s.initial_pass()
+        s.advance_steps(150)
+        P = s.particles()
+        hm, vm = s.max_maps()
+        out.append((P, hm, vm))
+        s.close()
+    (P1, h1, v1), (P2, h2, v2) = out
+    for k in P1:
+        assert np.array_equal(P1[k], P2[k]), k
+    assert np.array_equal(h1, h2) and np.array_equal(v1, v2)
