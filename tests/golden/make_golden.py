@@ -4,6 +4,7 @@ reference's own step-loop sources (oracle/_ref/slab_ref, built by
 
     python tests/golden/make_golden.py [case ...]
     python tests/golden/make_golden.py setup_poisson
+    SLAB_REF_ROOT=<reference checkout> python tests/golden/make_golden.py brienz5m
 
 Each fixture holds, from the reference run:
   frame0_digest   sha256 of the initial particle arrays (setup parity)
@@ -142,12 +143,67 @@ def make_setup_poisson():
     print("setup_poisson.json:", {k: v["Np"] for k, v in out.items()})
 
 
+BRIENZ_FRAMES = (1, 6)  # output frames (10 s apart) kept in the fixture
+
+
+def make_brienz5m():
+    """brienz5m.npz: the reference's own example (examples/brienz_raster.json)
+    on its 5 m DEM and release raster, run to its 60 s end by the reference
+    binary. Holds the DEM, the parameters, the reference's initial particles
+    (POISSON sampling with std::rand seeded 1), its particle positions and
+    heights at 10 s and 60 s, its final h_max / v_max2 and step count. The DEM keeps the
+    file's nodata cells (-9999), which the reference does not mask."""
+    root = os.environ.get("SLAB_REF_ROOT")
+    if not root:
+        sys.exit("set SLAB_REF_ROOT to the reference checkout")
+    ex = os.path.join(root, "examples")
+    with open(os.path.join(ex, "brienz_raster.json")) as f:
+        j = json.load(f)
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        j["project_dir"] = os.path.join(d, "out")
+        j["sim_name"] = "brienz5m"
+        j["terrain"]["dem"]["filepath"] = os.path.join(ex, "brienz_terrain_5m.asc")
+        j["release"]["raster"]["filepath"] = os.path.join(ex, "brienz_release_raster_5m.asc")
+        cfg_path = os.path.join(d, "brienz5m.json")
+        with open(cfg_path, "w") as f:
+            json.dump(j, f)
+        sim_dir = os.path.join(d, "out", "brienz5m")
+        run_ref(cfg_path, "--init-only")
+        P0 = O.read_particles_bin(sorted(glob.glob(os.path.join(sim_dir, "particles", "particles_frame_*.bin")))[0])
+        for fld in O.PARTICLE_FIELDS:
+            out[f"p0_{fld}"] = P0[fld]
+        log = run_ref(cfg_path)
+        out["nsteps"] = np.array(int([ln for ln in log.splitlines() if ln.startswith("Time step:")][-1].split()[2]))
+        for k in BRIENZ_FRAMES:
+            P = O.read_particles_bin(_frame_file(sim_dir, k))
+            for fld in ("x", "h"):
+                out[f"f{k}_{fld}"] = P[fld]
+            out[f"f{k}_time"] = np.array(P["time"])
+        hm, vm = O.read_max_bin(os.path.join(sim_dir, "max_values.bin"))
+    z, hdr = W.read_asc(os.path.join(ex, "brienz_terrain_5m.asc"))
+    out["z"] = z
+    out["dx"] = np.array(hdr["cellsize"])
+    idx = np.nonzero((hm != 0) | (vm != 0))
+    out["max_idx"] = np.stack(idx, axis=1).astype(np.int32)
+    out["max_h"] = hm[idx]
+    out["max_v2"] = vm[idx]
+    fr = j["friction"]["mu_I"]
+    out["params"] = np.array([j["physical_params"]["gravity"], j["physical_params"]["rho"], j["numerical_params"]["C_cfl"],
+                              j["numerical_params"]["dt_max"], j["numerical_params"]["flip_ratio"], j["time_params"]["output_dt"],
+                              j["time_params"]["total_time"], fr["mu_1"], fr["mu_2"], fr["I0"], fr["d"], fr["phi"]])
+    np.savez_compressed(os.path.join(HERE, "brienz5m.npz"), **out)
+    print(f"brienz5m: Np={len(P0['h'])} steps={int(out['nsteps'])} DEM {z.shape} -> brienz5m.npz")
+
+
 if __name__ == "__main__":
     if not os.path.exists(O.REF_BIN):
         sys.exit("oracle/_ref/slab_ref is not built (make -C oracle ref)")
     args = sys.argv[1:]
     if args == ["setup_poisson"]:
         make_setup_poisson()
+    elif args == ["brienz5m"]:
+        make_brienz5m()
     else:
         for n in (args or list(cases.CASES)):
             make(n)

@@ -165,3 +165,37 @@ def test_fp64_sensitivity_envelope():
         out[eps] = d.max()
     assert out[1e-13] < 1e-6
     assert out[1e-7] > 0.005
+
+
+def brienz5m_case(golden):
+    """The reference's own example on its 5 m DEM (tests/golden/brienz5m.npz,
+    written by the reference binary): parameters, DEM and initial particles."""
+    g = golden("brienz5m")
+    prm = g["params"]
+    cfg = dict(gravity=prm[0], rho=prm[1], C_cfl=prm[2], dt_max=prm[3], flip_ratio=prm[4], output_dt=prm[5], total_time=prm[6],
+               friction="MU_I", mui_mu1=prm[7], mui_mu2=prm[8], mui_I0=prm[9], mui_d=prm[10], mui_phi=prm[11])
+    P0 = {k[3:]: g[k] for k in g if k.startswith("p0_")}
+    return g, cfg, P0
+
+
+def test_oracle_matches_reference_brienz_fixture(golden):
+    """The C oracle over the whole 60 s of the reference's Brienz example
+    (5 m DEM with nodata cells, raster release, POISSON particles, mu(I)):
+    particles at 10 s and 60 s, the step count and the max maps equal the
+    reference binary's, bit for bit."""
+    g, cfg, P0 = brienz5m_case(golden)
+    o = O.Oracle(cfg, g["z"], float(g["dx"]))
+    o.set_particles(P0)
+    o.t0()
+    k = 0
+    while o.state()[0] < cfg["total_time"]:
+        if o.step() == 1:
+            k += 1
+            if f"f{k}_x" in g:
+                P = o.particles()
+                assert np.array_equal(P["x"], g[f"f{k}_x"]) and np.array_equal(P["h"], g[f"f{k}_h"]), k
+    assert o.state()[3] == int(g["nsteps"])
+    hm, vm = o.max_maps()
+    idx = tuple(g["max_idx"].T)
+    assert np.array_equal(hm[idx], g["max_h"]) and np.array_equal(vm[idx], g["max_v2"])
+    assert (hm != 0).sum() == len(g["max_h"])
