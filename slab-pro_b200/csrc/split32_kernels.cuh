@@ -1068,6 +1068,16 @@ __device__ __forceinline__ int cand_range(int k, const TileDesc& D, int& off) {
 }
 
 constexpr int P2C_TMA_MIN_BLOCKS = NCELL == 64 ? 6 : 2;  // the stage doubles the shared memory of a CTA
+constexpr int P2C_BATCH = 4;  // chunks of 32 candidates whose loads a warp issues together
+
+// one candidate of phase 1: its range, cell and the quantities to stage
+struct P2CCand {
+    int d;
+    int32_t cell;
+    float2 f, v;
+    float m, h, vz;
+    bool valid;
+};
 
 template <bool TMA>
 __global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MIN_BLOCKS) k_p2g_cell(Shared sh, int cls) {
@@ -1143,56 +1153,69 @@ __global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MI
         const PBuf B = sm.B;
         const int per = (ncand + P2C_WARPS - 1) / P2C_WARPS;
         const int k_lo = min(warp * per, ncand), k_hi = min(k_lo + per, ncand);
-        // 1. load (stage) and count per (warp, cell)
-        for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
-            const int k = k0 + lane;
-            int lc = -1;
-            if (k < k_hi) {
-                int d;
-                int32_t cell;
-                float2 f = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
-                float m = 0.f, h = 0.f, vz = 0.f;
+        // 1. load (stage) and count per (warp, cell). The loads of P2C_BATCH
+        // chunks of 32 candidates go out together before any is used, so a
+        // warp's candidates cost one round of global loads, not one per chunk.
+        for (int kb = k_lo; kb < k_hi; kb += 32 * P2C_BATCH) {
+            P2CCand q[P2C_BATCH];
+#pragma unroll
+            for (int u = 0; u < P2C_BATCH; ++u) {
+                const int k = kb + u * 32 + lane;
+                q[u].valid = k < k_hi;
+                q[u].d = 0;
+                q[u].cell = 0;
+                q[u].f = q[u].v = make_float2(0.f, 0.f);
+                q[u].m = q[u].h = q[u].vz = 0.f;
+                if (!q[u].valid) continue;
                 if (TMA && from_stage) {  // from the bulk-copied stage
                     int off;
-                    d = cand_range(k, sm.d, off);
+                    q[u].d = cand_range(k, sm.d, off);
                     if constexpr (TMA) {
-                        const int s4 = sm.lead4[d] + off, s8 = sm.lead8[d] + off;
-                        cell = sm.ts.cell[s4];
-                        f = sm.ts.f[s8];
-                        v = sm.ts.v[s8];
-                        m = sm.ts.m[s4];
-                        h = sm.ts.h[s4];
-                        if (outs) vz = sm.ts.vz[s4];
+                        const int s4 = sm.lead4[q[u].d] + off, s8 = sm.lead8[q[u].d] + off;
+                        q[u].cell = sm.ts.cell[s4];
+                        q[u].f = sm.ts.f[s8];
+                        q[u].v = sm.ts.v[s8];
+                        q[u].m = sm.ts.m[s4];
+                        q[u].h = sm.ts.h[s4];
+                        if (outs) q[u].vz = sm.ts.vz[s4];
                     }
                 } else {
-                    const int src = cand_to_index(k, sm.d, d);
-                    cell = B.cell[src];
+                    const int src = cand_to_index(k, sm.d, q[u].d);
+                    q[u].cell = B.cell[src];
                     if (staged) {  // issued together with the cell load
-                        f = B.f[src];
-                        v = B.v[src];
-                        m = B.m[src];
-                        h = B.h[src];
-                        if (outs) vz = B.vz[src];
-                    }
-                }
-                const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
-                if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
-                else if (d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
-                if (staged) {
-                    sm.lc[k] = (int16_t)lc;
-                    if (lc >= 0) {
-                        sm.st.sa[k] = make_float4(f.x, f.y, m, h);
-                        sm.st.sv[k] = v;
-                        sm.st.svz[k] = vz;
+                        q[u].f = B.f[src];
+                        q[u].v = B.v[src];
+                        q[u].m = B.m[src];
+                        q[u].h = B.h[src];
+                        if (outs) q[u].vz = B.vz[src];
                     }
                 }
             }
-            const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
-            if (lc >= 0) {
-                const unsigned peers = __match_any_sync(vm, lc);
-                if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
+#pragma unroll
+            for (int u = 0; u < P2C_BATCH; ++u) {
+                const int k = kb + u * 32 + lane;
+                if (kb + u * 32 >= k_hi) break;  // uniform: no candidate of this chunk in the warp's block
+                int lc = -1;
+                if (q[u].valid) {
+                    const int ci = cell_i(q[u].cell) - ti * TILE, cj = cell_j(q[u].cell) - tj * TILE;
+                    if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
+                    else if (q[u].d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
+                    if (staged) {
+                        sm.lc[k] = (int16_t)lc;
+                        if (lc >= 0) {
+                            sm.st.sa[k] = make_float4(q[u].f.x, q[u].f.y, q[u].m, q[u].h);
+                            sm.st.sv[k] = q[u].v;
+                            sm.st.svz[k] = q[u].vz;
+                        }
+                    }
+                }
+                const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
+                if (lc >= 0) {
+                    const unsigned peers = __match_any_sync(vm, lc);
+                    if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
+                }
+                __syncwarp();
             }
-            __syncwarp();
         }
         if constexpr (TMA) {
             if (tid < DESC_WORDS) reinterpret_cast<int*>(&sm.dnext)[tid] = dn;
@@ -1870,8 +1893,11 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         const double dx = Z.dx;
         double mnx = INFINITY, mxx = 0.0, mny = INFINITY, mxy = 0.0, vv = 0.0;
         int front = 0, back = 0;  // stayers / movers placed so far (same in every thread)
+        G2PCand nxt = pre;
         for (int k0 = 0; k0 < ncand; k0 += NCELL) {
-            const G2PCand q = k0 == 0 ? pre : load_g2p_cand(sm.d, B, k0 + tid, ncand, t, sh.TY);
+            // this chunk's candidates, and the next chunk's requested before this one is computed
+            const G2PCand q = nxt;
+            if (k0 + NCELL < ncand) nxt = load_g2p_cand(sm.d, B, k0 + NCELL + tid, ncand, t, sh.TY);
             const bool valid = q.valid;
             const int32_t cell = q.cell;
             int d = 4, ib = 0, jb = 0;

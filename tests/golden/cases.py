@@ -64,3 +64,24 @@ def particle_digest(P: dict) -> str:
     for k in ("x", "z", "v", "vz", "h", "A", "mass", "theta"):
         h.update(np.ascontiguousarray(P[k], dtype=np.float64).tobytes())
     return h.hexdigest()
+
+
+def case_c2_window():
+    """A small window of the config-2 construction for GPU parity over whole
+    runs: a 512 x 512 DEM at 1 m (30-degree slope easing to 5 degrees over
+    100 m from x = 300 m, fBm roughness of 4 m RMS, a 40 m containing rim), a
+    seeded star-polygon raster release (~70 x 45 m, lognormal heights,
+    h_min 0.2 m), POISSON sampling at 0.5 m with the numpy sampler (~17 k
+    particles), Voellmy mu 0.2, xi 1500, 40 s. Not a golden case: the tests
+    run the oracle on it."""
+    dx = 1.0
+    z = W.fractal_slope_dem(512, dx, seed=2026, rms=4.0, x_plane_end=300.0, ease_m=100.0, rim_m=40.0)
+    poly = W.star_polygon(2027, center=(110.0, 256.0), ax=70.0, ay=45.0)
+    rel = W.lognormal_release_raster(2028, poly, cellsize=dx)
+    rel["h_min"] = 0.2
+    cfg = dict(gravity=9.81, rho=300.0, C_cfl=0.5, dt_max=0.01, flip_ratio=0.95, output_dt=1.0, total_time=40.0,
+               friction="VOELLMY", voellmy_mu=0.2, voellmy_xi=1500.0)
+    h = rel["h"]
+    samples = W.poisson_disk_np((h.shape[0] - 1) * dx, (h.shape[1] - 1) * dx, 0.5, 2029)
+    P = W.release_particles(z, dx, rel, cfg["rho"], sampling="GIVEN", samples=samples)
+    return {"name": "c2_window512_dx1_star_voellmy", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}
