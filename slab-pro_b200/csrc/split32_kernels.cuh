@@ -1068,8 +1068,6 @@ __device__ __forceinline__ int cand_range(int k, const TileDesc& D, int& off) {
 }
 
 constexpr int P2C_TMA_MIN_BLOCKS = NCELL == 64 ? 6 : 2;  // the stage doubles the shared memory of a CTA
-constexpr int P2C_BATCH = 4;  // chunks of 32 candidates whose loads a warp issues together
-
 // one candidate of phase 1: its range, cell and the quantities to stage
 struct P2CCand {
     int d;
@@ -1153,69 +1151,66 @@ __global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MI
         const PBuf B = sm.B;
         const int per = (ncand + P2C_WARPS - 1) / P2C_WARPS;
         const int k_lo = min(warp * per, ncand), k_hi = min(k_lo + per, ncand);
-        // 1. load (stage) and count per (warp, cell). The loads of P2C_BATCH
-        // chunks of 32 candidates go out together before any is used, so a
-        // warp's candidates cost one round of global loads, not one per chunk.
-        for (int kb = k_lo; kb < k_hi; kb += 32 * P2C_BATCH) {
-            P2CCand q[P2C_BATCH];
-#pragma unroll
-            for (int u = 0; u < P2C_BATCH; ++u) {
-                const int k = kb + u * 32 + lane;
-                q[u].valid = k < k_hi;
-                q[u].d = 0;
-                q[u].cell = 0;
-                q[u].f = q[u].v = make_float2(0.f, 0.f);
-                q[u].m = q[u].h = q[u].vz = 0.f;
-                if (!q[u].valid) continue;
-                if (TMA && from_stage) {  // from the bulk-copied stage
-                    int off;
-                    q[u].d = cand_range(k, sm.d, off);
-                    if constexpr (TMA) {
-                        const int s4 = sm.lead4[q[u].d] + off, s8 = sm.lead8[q[u].d] + off;
-                        q[u].cell = sm.ts.cell[s4];
-                        q[u].f = sm.ts.f[s8];
-                        q[u].v = sm.ts.v[s8];
-                        q[u].m = sm.ts.m[s4];
-                        q[u].h = sm.ts.h[s4];
-                        if (outs) q[u].vz = sm.ts.vz[s4];
-                    }
-                } else {
-                    const int src = cand_to_index(k, sm.d, q[u].d);
-                    q[u].cell = B.cell[src];
-                    if (staged) {  // issued together with the cell load
-                        q[u].f = B.f[src];
-                        q[u].v = B.v[src];
-                        q[u].m = B.m[src];
-                        q[u].h = B.h[src];
-                        if (outs) q[u].vz = B.vz[src];
+        // 1. load (stage) and count per (warp, cell). A warp requests its next
+        // chunk of 32 candidates before it stages the current one, so the
+        // chunks' load rounds overlap.
+        auto load_cand = [&](int k, P2CCand& c) {
+            c.valid = k < k_hi;
+            c.d = 0;
+            c.cell = 0;
+            c.f = c.v = make_float2(0.f, 0.f);
+            c.m = c.h = c.vz = 0.f;
+            if (!c.valid) return;
+            if (TMA && from_stage) {  // from the bulk-copied stage
+                int off;
+                c.d = cand_range(k, sm.d, off);
+                if constexpr (TMA) {
+                    const int s4 = sm.lead4[c.d] + off, s8 = sm.lead8[c.d] + off;
+                    c.cell = sm.ts.cell[s4];
+                    c.f = sm.ts.f[s8];
+                    c.v = sm.ts.v[s8];
+                    c.m = sm.ts.m[s4];
+                    c.h = sm.ts.h[s4];
+                    if (outs) c.vz = sm.ts.vz[s4];
+                }
+            } else {
+                const int src = cand_to_index(k, sm.d, c.d);
+                c.cell = B.cell[src];
+                if (staged) {  // issued together with the cell load
+                    c.f = B.f[src];
+                    c.v = B.v[src];
+                    c.m = B.m[src];
+                    c.h = B.h[src];
+                    if (outs) c.vz = B.vz[src];
+                }
+            }
+        };
+        P2CCand nx;
+        load_cand(k_lo + lane, nx);
+        for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+            const int k = k0 + lane;
+            const P2CCand q = nx;
+            if (k0 + 32 < k_hi) load_cand(k0 + 32 + lane, nx);
+            int lc = -1;
+            if (q.valid) {
+                const int ci = cell_i(q.cell) - ti * TILE, cj = cell_j(q.cell) - tj * TILE;
+                if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
+                else if (q.d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
+                if (staged) {
+                    sm.lc[k] = (int16_t)lc;
+                    if (lc >= 0) {
+                        sm.st.sa[k] = make_float4(q.f.x, q.f.y, q.m, q.h);
+                        sm.st.sv[k] = q.v;
+                        sm.st.svz[k] = q.vz;
                     }
                 }
             }
-#pragma unroll
-            for (int u = 0; u < P2C_BATCH; ++u) {
-                const int k = kb + u * 32 + lane;
-                if (kb + u * 32 >= k_hi) break;  // uniform: no candidate of this chunk in the warp's block
-                int lc = -1;
-                if (q[u].valid) {
-                    const int ci = cell_i(q[u].cell) - ti * TILE, cj = cell_j(q[u].cell) - tj * TILE;
-                    if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
-                    else if (q[u].d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
-                    if (staged) {
-                        sm.lc[k] = (int16_t)lc;
-                        if (lc >= 0) {
-                            sm.st.sa[k] = make_float4(q[u].f.x, q[u].f.y, q[u].m, q[u].h);
-                            sm.st.sv[k] = q[u].v;
-                            sm.st.svz[k] = q[u].vz;
-                        }
-                    }
-                }
-                const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
-                if (lc >= 0) {
-                    const unsigned peers = __match_any_sync(vm, lc);
-                    if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
-                }
-                __syncwarp();
+            const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
+            if (lc >= 0) {
+                const unsigned peers = __match_any_sync(vm, lc);
+                if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
             }
+            __syncwarp();
         }
         if constexpr (TMA) {
             if (tid < DESC_WORDS) reinterpret_cast<int*>(&sm.dnext)[tid] = dn;
