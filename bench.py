@@ -278,10 +278,11 @@ def ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream()
-    if args.only in ("ensemble", "serving"):
+    if args.only in ("ensemble", "serving", "e2e_cli"):
         if rank != 0:
             return None
-        sec = ensemble(args, stream, dev) if args.only == "ensemble" else serving(args, stream, dev)
+        sec = {"ensemble": lambda: ensemble(args, stream, dev), "serving": lambda: serving(args, stream, dev),
+               "e2e_cli": lambda: e2e_cli(args)}[args.only]()
         return {"section": args.only, args.only: sec}
     c = load_workload(args.workload)
     P0 = c["particles"]
@@ -489,6 +490,11 @@ def ours(args, rank, world):
                                            particles=len(c2["particles"]["h"]))
             except Exception as ex:
                 line["accuracy_c2"] = {"error": f"{type(ex).__name__}: {ex}"}
+    if world == 1 and not args.no_e2e_cli:
+        try:
+            line["e2e_cli"] = e2e_cli(args)
+        except Exception as ex:
+            line["e2e_cli"] = {"error": f"{type(ex).__name__}: {ex}"}
     if world == 1 and not args.no_ensemble and args.only != "serving":
         try:
             line["ensemble"] = ensemble(args, stream, dev)
@@ -693,98 +699,176 @@ def ensemble_sharded(args, stream, dev, rank, world):
             "scaling": "strong (the same 256 scenarios split over the ranks)"}
 
 
+def e2e_cli(args):
+    """End to end through the drop-in program, as a reference user runs it:
+    `bin/slab_b200 <config.json>` (loadFromJSON, initialize, DEM read,
+    POISSON setup on the host, simulate with the step loop on the GPU and
+    every output frame written as .ply / .tif by the writer thread while the
+    GPU runs on, max_values.tif) on a window of the config-2 construction
+    (512 x 512 DEM at 1 m, raster release, Voellmy, 40 s, a frame every
+    second), beside the reference's own step loop on the same JSON
+    (oracle/_ref/slab_ref, its output writers stubbed, one host core).
+    Rates are particle-steps per second of wall time, setup included."""
+    import workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cli = os.path.join(ROOT, "slab-pro_b200", "bin", "slab_b200")
+    dx = 1.0
+    z = W.fractal_slope_dem(512, dx, seed=2026, rms=4.0, x_plane_end=300.0, ease_m=100.0, rim_m=40.0)
+    poly = W.star_polygon(2027, center=(110.0, 256.0), ax=70.0, ay=45.0)
+    rel = W.lognormal_release_raster(2028, poly, cellsize=dx)
+    out = {"workload": "c2_window512_dx1_star_raster_poisson_voellmy_40s"}
+    with tempfile.TemporaryDirectory() as d:
+        W.write_asc(os.path.join(d, "dem.asc"), z, dx)
+        W.write_asc(os.path.join(d, "release.asc"), rel["h"], rel["cellsize"], xll=rel["x0"], yll=rel["y0"])
+        j = {"project_dir": os.path.join(d, "out"), "sim_name": "e2e",
+             "physical_params": {"gravity": 9.81, "rho": 300.0}, "time_params": {"output_dt": 1.0, "total_time": 40.0},
+             "numerical_params": {"C_cfl": 0.5, "dt_max": 0.01, "flip_ratio": 0.95, "sampling_method": "POISSON"},
+             "friction": {"type": "VOELLMY", "voellmy": {"mu": 0.2, "xi": 1500.0}},
+             "terrain": {"type": "DEM", "dem": {"filepath": os.path.join(d, "dem.asc")}},
+             "release": {"type": "RASTER", "h0": 0.0, "raster": {"filepath": os.path.join(d, "release.asc"), "h_min": 0.2}}}
+        cfg = os.path.join(d, "e2e.json")
+        with open(cfg, "w") as f:
+            json.dump(j, f)
+
+        def timed_run(cmd, env=None):
+            t0 = time.perf_counter()
+            r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise RuntimeError(f"{os.path.basename(cmd[0])} failed: {r.stderr.strip()[-300:]}")
+            return r.stdout, wall
+
+        subprocess.run([cli, cfg, "--no-output"], capture_output=True)  # DEM cache and first-use costs outside the timings
+        for label, extra in (("fp32_outputs", []), ("fp32_no_output", ["--no-output"]), ("fp64_outputs", ["--fp64"])):
+            txt, wall = timed_run([cli, cfg] + extra)
+            np_ = int([ln for ln in txt.splitlines() if ln.startswith("Number of particles:")][-1].split()[-1])
+            steps = int([ln for ln in txt.splitlines() if ln.startswith("Simulation finished:")][-1].split()[2])
+            out[label] = {"wall_s": round(wall, 3), "particles": np_, "steps": steps, "particle_steps_per_s": round(np_ * steps / wall, 1)}
+        nfiles = len(os.listdir(os.path.join(d, "out", "e2e", "particles"))) if os.path.isdir(os.path.join(d, "out", "e2e", "particles")) else 0
+        out["fp32_outputs"]["frames_written"] = nfiles
+        if os.path.exists(O.REF_BIN) and not args.no_cpu:
+            txt, wall = timed_run([O.REF_BIN, cfg], env=dict(os.environ, SLAB_REF_NO_DUMP="1"))
+            steps = int([ln for ln in txt.splitlines() if ln.startswith("Time step:")][-1].split()[2])
+            np_ = int([ln for ln in txt.splitlines() if ln.startswith("Number of particles:")][-1].split()[-1])
+            out["reference_cpu"] = {"wall_s": round(wall, 3), "particles": np_, "steps": steps, "cores": 1,
+                                    "particle_steps_per_s": round(np_ * steps / wall, 1),
+                                    "note": "the reference's step loop with its output writers stubbed (no files)"}
+            out["speedup_fp32_outputs_vs_reference"] = round(out["fp32_outputs"]["particle_steps_per_s"] /
+                                                             out["reference_cpu"]["particle_steps_per_s"], 2)
+    return out
+
+
+def _serve(srv, reqs, arrivals, dev):
+    """Submit every request (a release, built on the device when admitted) at
+    its arrival time, replayed in real time; drain; per-request time to
+    result and steps, and the server's figures."""
+    import slab
+    ids, late = [], 0.0
+    with ClockSampler(dev) as clk:
+        t_start = time.perf_counter()
+        for ta, (_, cfg, rel) in zip(arrivals, reqs):
+            now = time.perf_counter() - t_start
+            if ta > now:
+                time.sleep(ta - now)
+            late = max(late, time.perf_counter() - t_start - ta)
+            ids.append(srv.submit_release(cfg, rel))
+        srv.drain(timeout=1800.0)
+        t_end = time.perf_counter()
+    st, tm = srv.stats(), srv.timing()
+    ttr, ok = [], 0
+    for rid in ids:
+        state, secs = srv.poll(rid)
+        if state == slab.REQ_DONE:
+            ttr.append(secs)
+            ok += 1
+    ttr = np.array(ttr) if ttr else np.array([np.nan])
+    span = t_end - t_start
+    return {"completed": ok, "failed": len(ids) - ok, "p50_s": round(float(np.percentile(ttr, 50)), 3),
+            "p99_s": round(float(np.percentile(ttr, 99)), 3), "scenarios_per_s": round(ok / span, 3),
+            "particle_steps_per_s": round(st["particle_steps"] / span, 1), "makespan_s": round(span, 3),
+            "busy_s": round(st["busy_s"], 3), "saturation_scenarios_per_s": round(ok / max(st["busy_s"], 1e-9), 3),
+            "max_submit_lateness_s": round(late, 4), "worker": {k: round(v, 3) for k, v in tm.items()}, "clocks": clk.summary()}
+
+
+def _fifo(arrivals, service):
+    """Times to result of a FIFO queue of one server with these service times."""
+    t, fin = 0.0, np.empty(len(arrivals))
+    for q in range(len(arrivals)):
+        t = max(t, arrivals[q]) + service[q]
+        fin[q] = t
+    lat = fin - np.asarray(arrivals)
+    return {"p50_s": round(float(np.percentile(lat, 50)), 3), "p99_s": round(float(np.percentile(lat, 99)), 3),
+            "scenarios_per_s": round(len(arrivals) / (fin[-1] - arrivals[0]), 3), "busy_s": round(float(np.sum(service)), 3)}
+
+
 def serving(args, stream, dev):
-    """Served request stream: Poisson arrivals on the config-3 DEM into the
-    continuous-batching server, time to result per request; against the same
-    stream through the plain FP64 path one request at a time (service times
-    measured on a stratified sample, modelled for the rest, FIFO queue)."""
+    """Served request stream (config 5): Poisson arrivals at 20/s on the
+    config-3 DEM into the continuous-batching server; each request is an
+    ELLIPSE release whose particles are built on the device when it is
+    admitted. Against it, every request of the same window runs alone
+    through the plain FP64 path (each one's device time measured, release
+    built on the device as well), and those service times are replayed as a
+    FIFO queue on the same arrival times. The stream is replayed twice: at
+    its own rate (20/s, more than either path sustains), and at 70 % of the
+    rate the FP32 server sustains, where times to result are not queueing."""
+    import torch
     import slab
     import workloads as W
     g0 = time.perf_counter()
     dx = 0.5
     z = W.config3_dem()
-    reqs = W.config5_stream(z, dx, args.c5_window)
+    reqs = W.config5_stream(z, dx, args.c5_window, particles=False)
     gen_s = time.perf_counter() - g0
     n = len(reqs)
-    Nps = np.array([len(P["h"]) for _, _, P in reqs])
     arr = np.array([t for t, _, _ in reqs])
-    out = {"workload": f"poisson{20}/s_window{args.c5_window:g}s_fractal8192_dx0.5", "requests": n,
-           "particles": int(Nps.sum()), "particles_median_max": [int(np.median(Nps)), int(Nps.max())], "generate_s": round(gen_s, 1),
-           "window_s": args.c5_window}
+    out = {"workload": f"poisson20/s_window{args.c5_window:g}s_fractal8192_dx0.5", "requests": n, "window_s": args.c5_window,
+           "window_note": f"the first {args.c5_window:g} s of the 300 s stream", "generate_s": round(gen_s, 1)}
     srv = slab.Server(z, dx, max_scenarios=args.c5_slots, chunk_steps=32)
-    ids = []
-    late = 0.0
-    with ClockSampler(dev) as clk:
-        t_start = time.perf_counter()
-        for ta, cfg, P in reqs:
-            now = time.perf_counter() - t_start
-            if ta > now:
-                time.sleep(ta - now)
-            late = max(late, time.perf_counter() - t_start - ta)
-            ids.append(srv.submit(cfg, P))
-        srv.drain(timeout=1800.0)
-        t_end = time.perf_counter()
-    st = srv.stats()
-    tm = srv.timing()
-    ttr, failed = [], 0
-    # steps of each request (failed ones: total_time / dt_max, the fewest it could take)
-    steps = np.array([cfg["total_time"] / cfg["dt_max"] for _, cfg, _ in reqs])
-    for q, rid in enumerate(ids):
-        state, _ = srv.poll(rid)
-        if state != slab.REQ_DONE:
-            failed += 1
-            continue
-        r = srv.result(rid)
-        ttr.append(r["seconds_to_result"])
-        steps[q] = r["steps"]
+    out["fp32_served"] = _serve(srv, reqs, arr, dev)
     srv.close()
-    ttr = np.array(ttr) if ttr else np.array([np.nan])
-    out["fp32_served"] = {"completed": int(np.isfinite(ttr).sum()), "failed": failed, "p50_s": round(float(np.percentile(ttr, 50)), 3),
-                          "p99_s": round(float(np.percentile(ttr, 99)), 3),
-                          "scenarios_per_s": round(int(np.isfinite(ttr).sum()) / (t_end - t_start), 3),
-                          "particle_steps_per_s": round(st["particle_steps"] / (t_end - t_start), 1),
-                          "makespan_s": round(t_end - t_start, 3), "busy_s": round(st["busy_s"], 3),
-                          "max_submit_lateness_s": round(late, 4), "worker": {k: round(v, 3) for k, v in tm.items()},
-                          "clocks": clk.summary()}
-    # plain FP64, one request at a time: service time measured on a sample
-    pick = _stratified(Nps * np.array([cfg["total_time"] for _, cfg, _ in reqs]), args.c5_sample)
+    # plain FP64, every request alone
     s = slab.Slab(z, dx)
     s.set_stream(stream.cuda_stream)
-    meas = []
-    for i in pick:
-        _, cfg, P = reqs[i]
+    svc, nps, fails = np.zeros(n), np.zeros(n), 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    for q, (_, cfg, rel) in enumerate(reqs):
+        s.set_params(cfg, slab.FP64_PLAIN)
         try:
-            d, w, k, _, _ = _solo_run(s, cfg, P, slab.FP64_PLAIN, stream)
+            e0.record(stream)
+            nps[q] = s.upload_release(rel)
+            s.initial_pass()
+            s.advance_steps(1 << 40)
+            e1.record(stream)
+            e1.synchronize()
+            svc[q] = e0.elapsed_time(e1) * 1e-3
         except slab.SlabError:
-            continue
-        meas.append((i, d, w, k))
+            fails += 1
+            torch.cuda.synchronize()
     s.close()
-    if len(meas) < 2:
-        out["fp64_sequential"] = {"error": "fewer than 2 sample requests completed"}
-        return out
-    # service = a*steps + b*particle-steps, least squares on the sample (device seconds)
-    Asm = np.array([[k, k * Nps[i]] for i, _, _, k in meas], dtype=np.float64)
-    ysm = np.array([d for _, d, _, _ in meas])
-    coef, *_ = np.linalg.lstsq(Asm, ysm, rcond=None)
-    f64 = {"sample": len(pick), "service_model_s": {"per_step": float(coef[0]), "per_particle_step": float(coef[1])},
-           "sample_fit_max_rel_err": round(float(np.max(np.abs(Asm @ coef - ysm) / ysm)), 4),
-           "sample_particle_steps_per_s": round(float((Asm[:, 1]).sum() / ysm.sum()), 1)}
-    svc = np.maximum(steps * coef[0] + steps * Nps * coef[1], 0.0)
-    fin = np.empty(n)
-    t = 0.0
-    for q in range(n):
-        t = max(t, arr[q]) + svc[q]
-        fin[q] = t
-    lat = fin - arr
-    f64.update({"p50_s": round(float(np.percentile(lat, 50)), 3), "p99_s": round(float(np.percentile(lat, 99)), 3),
-                "scenarios_per_s": round(n / (fin[-1] - arr[0]), 3), "busy_s": round(float(svc.sum()), 3)})
-    if len(ttr):
-        out["speedup_vs_fp64_sequential"] = {"scenarios_per_s": round(out["fp32_served"]["scenarios_per_s"] / f64["scenarios_per_s"], 2),
-                                             "p50": round(f64["p50_s"] / out["fp32_served"]["p50_s"], 2),
-                                             "p99": round(f64["p99_s"] / out["fp32_served"]["p99_s"], 2)}
+    f64 = {"requests_run": n, "failed": fails, "particles": int(nps.sum()), "device_s": round(float(svc.sum()), 3),
+           "wall_s": round(time.perf_counter() - w0, 1), "saturation_scenarios_per_s": round((n - fails) / max(svc.sum(), 1e-9), 3)}
+    f64.update(_fifo(arr, svc))
     out["fp64_sequential"] = f64
-    out["note"] = ("time to result from submission to the result on the host; arrivals replayed in real time; the FP64 "
-                   "sequential queue uses device-only service times (upload and download excluded) fitted on the sample")
+    fs = out["fp32_served"]
+    out["speedup_vs_fp64_sequential"] = {"scenarios_per_s": round(fs["scenarios_per_s"] / f64["scenarios_per_s"], 2),
+                                         "saturation": round(fs["saturation_scenarios_per_s"] / max(f64["saturation_scenarios_per_s"], 1e-9), 2),
+                                         "p50": round(f64["p50_s"] / fs["p50_s"], 2), "p99": round(f64["p99_s"] / fs["p99_s"], 2)}
+    # the same requests at 70 % of the rate the FP32 server sustains
+    rate = 0.7 * fs["saturation_scenarios_per_s"]
+    if args.c5_sustained and rate > 0:
+        arr2 = (arr - arr[0]) * (20.0 / rate)
+        srv = slab.Server(z, dx, max_scenarios=args.c5_slots, chunk_steps=32)
+        sus = _serve(srv, reqs, arr2, dev)
+        srv.close()
+        f2 = _fifo(arr2, svc)
+        out["sustained"] = {"arrivals_per_s": round(rate, 3), "fp32_served": sus, "fp64_sequential": f2,
+                            "speedup_vs_fp64_sequential": {"p50": round(f2["p50_s"] / sus["p50_s"], 2),
+                                                           "p99": round(f2["p99_s"] / sus["p99_s"], 2)}}
+    out["note"] = ("time to result from submission to the result on the host; arrivals replayed in real time; FP64 "
+                   "sequential: every request of the window run alone, its device time (release setup, t=0 pass, steps) "
+                   "replayed as a FIFO queue on the same arrival times")
     return out
 
 
@@ -858,20 +942,21 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 whole-run accuracy blocks")
     ap.add_argument("--no-envelope", action="store_true", help="skip the FP64 envelope run of the headline accuracy block")
     ap.add_argument("--no-c2-accuracy", action="store_true", help="skip the config-2 accuracy block")
+    ap.add_argument("--no-e2e-cli", action="store_true", help="skip the end-to-end run of the drop-in program")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-procs", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--only", default="", choices=["", "fp32", "ensemble", "serving"],
+    ap.add_argument("--only", default="", choices=["", "fp32", "ensemble", "serving", "e2e_cli"],
                     help="fp32: only the FP32 path (profiling runs); ensemble / serving: only that section")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble section (config 4)")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-stream section (config 5)")
     ap.add_argument("--c4-scenarios", type=int, default=256)
     ap.add_argument("--c4-sample", type=int, default=16, help="scenarios run one after another for the sequential rates")
     ap.add_argument("--c4-acc-sample", type=int, default=8, help="scenarios of the whole-run accuracy block (with the FP64 envelope)")
-    ap.add_argument("--c5-window", type=float, default=20.0, help="seconds of Poisson arrivals (the full stream is 300 s)")
+    ap.add_argument("--c5-window", type=float, default=6.0, help="seconds of Poisson arrivals (the full stream is 300 s)")
+    ap.add_argument("--c5-sustained", type=int, default=1, help="also replay the stream at 70 %% of the FP32 saturation rate")
     ap.add_argument("--c5-slots", type=int, default=512)
-    ap.add_argument("--c5-sample", type=int, default=12, help="requests timed on the plain FP64 path")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         log("warmup raised to 3")

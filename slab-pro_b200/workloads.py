@@ -483,13 +483,15 @@ def config4(n_scenarios: int = 256, seed: int = 2028):
 
 
 def config5_stream(z: np.ndarray, dx: float, window_s: float, seed: int = 2029, rate: float = 20.0, median: float = 20000.0,
-                   sigma_log: float = 1.0, cap: int = 2_000_000, t_range=(30.0, 120.0)):
+                   sigma_log: float = 1.0, cap: int = 2_000_000, t_range=(30.0, 120.0), particles: bool = True):
     """Poisson arrivals at `rate` per second over `window_s` seconds of requests
     on DEM z: particle count lognormal (median, sigma_log) capped at `cap`, an
     ellipse of area N/16 m^2 (UNIFORM at 0.5 m) with random aspect and
     position in the upper third, friction law uniform over COULOMB / VOELLMY /
     MU_I with coefficients from the ranges of the other workloads, total_time
-    uniform in t_range. Yields (arrival time, cfg, particles)."""
+    uniform in t_range. Returns (arrival time, cfg, particles) per request,
+    or (arrival time, cfg, release) with particles=False (the release is then
+    built where it runs, e.g. on the device)."""
     rng = np.random.default_rng(seed)
     gn = terrain_gradient_norm(z, dx)
     L = z.shape[0] * dx
@@ -518,5 +520,5 @@ def config5_stream(z: np.ndarray, dx: float, window_s: float, seed: int = 2029, 
             cfg.update(mui_mu1=float(rng.uniform(0.3, 0.45)), mui_mu2=float(rng.uniform(0.55, 0.7)), mui_I0=0.279, mui_d=5e-4, mui_phi=0.6)
         rel = {"type": "ELLIPSE", "center": (float(cx), float(cy)), "rx": rx, "ry": ry, "rotation_deg": float(rng.uniform(0, 180)),
                "h0": float(rng.uniform(0.5, 3.0))}
-        reqs.append((t, cfg, release_particles(z, dx, rel, cfg["rho"], fast_theta=True, grad_norm=gn)))
+        reqs.append((t, cfg, release_particles(z, dx, rel, cfg["rho"], fast_theta=True, grad_norm=gn) if particles else rel))
     return reqs
