@@ -335,8 +335,60 @@ def ours(args, rank, world):
             if s.advance_steps(max(1, int(round((t_target - s.state()[0]) / cfg["dt_max"])))) == 0:
                 break
 
+    def e2e_block():
+        """The same metric through the public API from pinned FP64 host
+        arrays: upload, t=0 pass, K steps, particle and max-map download."""
+        K_e2e = args.e2e_steps
+
+        def pinned(n):  # page-locked host memory, allocated before the timed region
+            return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+
+        hb = {}
+        for k in ("x", "v", "vz", "h", "A", "mass", "z"):
+            a = np.ascontiguousarray(P0[k], dtype=np.float64)
+            hb[k] = pinned(a.size).reshape(a.shape)
+            hb[k][...] = a
+        ob = {k: pinned(hb[k].size) for k in hb}
+        mb = (pinned(c["z"].size), pinned(c["z"].size))
+        e = slab.Slab(c["z"], c["dx"])
+        e.set_stream(stream.cuda_stream)
+        e.set_params(cfg, slab.FP32_SPLIT)
+        e2e_runs = []
+        for it in range(2):
+            torch.cuda.synchronize()
+            tt = [time.perf_counter()]
+            e.upload(hb)
+            tt.append(time.perf_counter())
+            e.initial_pass()
+            tt.append(time.perf_counter())
+            e.advance_steps(K_e2e)
+            tt.append(time.perf_counter())
+            out = e.particles(out=ob)
+            tt.append(time.perf_counter())
+            hmx, _ = e.max_maps(out=mb)
+            tt.append(time.perf_counter())
+            e2e_runs.append(tt)
+        best = min(e2e_runs, key=lambda tt: tt[-1] - tt[0])
+        h2d = sum(hb[k].nbytes for k in hb)
+        d2h = sum(out[k].nbytes for k in out) + 2 * hmx.nbytes
+        e2e = {"value": round(Np * K_e2e / (best[-1] - best[0]), 1), "unit": METRIC,
+               "h2d_bytes_per_step": int(h2d / K_e2e), "d2h_bytes_per_step": int(d2h / K_e2e),
+               "phases_s": {name: round(best[q + 1] - best[q], 4)
+                            for q, name in enumerate(("upload", "t0_pass", "steps", "particles_download", "max_maps_download"))},
+               "window": f"upload + t=0 pass + {K_e2e} steps + particle and max-map download, host FP64 arrays in pinned memory "
+                         f"allocated before the timed region, best of 2; d2h counts the host arrays returned (the library copies "
+                         f"only the node box the flow touched of the max maps)"}
+        e.close()
+        del hmx, out, ob, mb, hb
+        return e2e
+
     # ---- FP32 split path (the product): W warm-up steps from the workload's
     # initial state, then K timed steps -- the state the reference arm times
+    # the end-to-end run comes first: its first steps tune the launch shapes,
+    # which the library keeps for later contexts of the same size, so the
+    # timed steps below run on tuned shapes (the tuner's trial shapes would
+    # otherwise fall inside the timed window)
+    e2e = e2e_block()
     s32 = make(slab.FP32_SPLIT)
     s32.advance_steps(args.warmup)
     with ClockSampler(dev) as clk:
@@ -358,7 +410,8 @@ def ours(args, rank, world):
                     "developed": {"sim_time_s": round(t32, 3), "ms_per_step": round(ms_dev / args.steps, 5),
                                   "phases_ms": [round(p / args.steps, 5) for p in phases_dev],
                                   "active_nodes_per_step": work_dev[1] / args.steps},
-                    "active_nodes_per_step": work_prof[1] / args.steps, "gpu_launches": int(launches)}
+                    "active_nodes_per_step": work_prof[1] / args.steps, "gpu_launches": int(launches),
+                    "e2e": e2e}
         return None
 
     # ---- plain FP64 path on the same schedule
@@ -429,30 +482,6 @@ def ours(args, rank, world):
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
-    # ---- e2e through the public API with host buffers
-    K_e2e = args.e2e_steps
-    hb = {k: np.ascontiguousarray(P0[k]) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
-    e = slab.Slab(c["z"], c["dx"])
-    e.set_stream(stream.cuda_stream)
-    e.set_params(cfg, slab.FP32_SPLIT)
-    e2e_times = []
-    for it in range(2):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e.upload(hb)
-        e.initial_pass()
-        e.advance_steps(K_e2e)
-        out = e.particles()
-        hmx, _ = e.max_maps()
-        e2e_times.append(time.perf_counter() - t0)
-    h2d = sum(hb[k].nbytes for k in hb)
-    d2h = sum(out[k].nbytes for k in out) + 2 * hmx.nbytes
-    e2e = {"value": round(Np * K_e2e / min(e2e_times), 1), "unit": METRIC,
-           "h2d_bytes_per_step": int(h2d / K_e2e), "d2h_bytes_per_step": int(d2h / K_e2e),
-           "window": f"upload + t=0 pass + {K_e2e} steps + particle and max-map download, host FP64 arrays, best of 2; "
-                     f"d2h counts the host arrays returned (the library copies only the node box the flow touched of the max maps)"}
-    e.close()
-    del hmx, out
 
     clocks = clk.summary()
     line = {
@@ -473,7 +502,8 @@ def ours(args, rank, world):
                       "fp32_speedup": round(ms64_dev / ms_dev, 2), "active_nodes_per_step": round(nodes_dev, 1),
                       "per_kernel": pk_dev},
         "gpu_launches": int(launches),
-        "launch_shapes": {"ctas": dict(zip(("prep", "p2g_dense", "p2g_sparse", "grid", "g2p"), shapes)), "tuning_passes": tunes},
+        "launch_shapes": {"ctas": dict(zip(("prep", "p2g_dense", "p2g_sparse", "grid", "g2p"), shapes)), "tuning_passes": tunes,
+                          "source": "picked on the e2e run's first steps of the same workload size, kept by the library for the process"},
         "clocks": clocks,
         "wall_s_timed": round(wall, 4),
     }

@@ -255,7 +255,11 @@ slab_status slab_get_phase_times(slab_ctx* ctx, double out[5]);
 slab_status slab_work_counters(slab_ctx* ctx, int64_t out[2]);
 
 /* FP32_SPLIT: CTA counts of the step's five work kernels now in use and the
- * tuning passes completed (as slab_batch_launch_shapes); zeros for FP64. */
+ * tuning passes completed (as slab_batch_launch_shapes); zeros for FP64.
+ * The shapes a context picks are remembered for the process, by device, tile
+ * count and particle count (half-octave buckets): a later context of the same
+ * size starts from them and measures none on its first steps (out[5] stays 0
+ * until its next tuning pass). Shapes never change results. */
 slab_status slab_launch_shapes(slab_ctx* ctx, int32_t out[6]);
 
 /* Number of kernels this context has launched since creation. */

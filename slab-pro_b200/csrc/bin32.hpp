@@ -19,8 +19,9 @@ struct BinResult {
 // the occupied tiles' segment records (stamp 0) into grp0, the first active
 // list and the active stamps. Throws SLAB_E_DOMAIN if a stencil leaves the
 // terrain and SLAB_E_OOM if more than act_cap tiles are occupied.
+// Its temporaries come from `scratch`.
 BinResult bin_particles(const Terrain& T, int TY, int ntiles, cudaStream_t st, int Np, const double* x, const double* v, const double* vz,
                         const double* h, const double* m, const double* z, const PBuf& out, int32_t* grp0, int32_t* act_list0,
-                        int32_t* act_stamp, int act_cap);
+                        int32_t* act_stamp, int act_cap, Scratch& scratch);
 
 }  // namespace slab

@@ -74,6 +74,19 @@ template <typename R> __device__ __forceinline__ void bspline3(R f, R w[3], R dw
     dw[2] = c;
 }
 
+// FP32: every operation rounded as written (no multiply-add contraction), so
+// each kernel that evaluates the weights gets the same bits whatever code the
+// compiler schedules around it.
+template <> __device__ __forceinline__ void bspline3<float>(float f, float w[3], float dw[3]) {
+    const float a = __fsub_rn(1.5f, f), b = __fsub_rn(f, 1.0f), c = __fsub_rn(f, 0.5f);
+    w[0] = __fmul_rn(__fmul_rn(0.5f, a), a);
+    w[1] = __fsub_rn(0.75f, __fmul_rn(b, b));
+    w[2] = __fmul_rn(__fmul_rn(0.5f, c), c);
+    dw[0] = __fsub_rn(f, 1.5f);
+    dw[1] = __fmul_rn(-2.0f, b);
+    dw[2] = c;
+}
+
 // Fixed-point P2G sums keep each contribution as an int32 pair: hi, the
 // contribution rounded to the quantum, and lo, the rest below the quantum in
 // units of 2^-L quanta (|lo| <= 2^(L-1)). With at most n contributions to a

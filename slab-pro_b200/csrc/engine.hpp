@@ -47,6 +47,33 @@ struct DFree {
 template <typename T> using dptr = std::unique_ptr<T, DFree>;
 template <typename T> dptr<T> dalloc(size_t n) { return dptr<T>(dmalloc<T>(n)); }
 
+// Grow-only device scratch for the transient buffers of one call (binning an
+// upload, building a download): kept at the largest size asked so far, so
+// repeated calls allocate nothing. Callers finish their work on it (stream
+// synchronised) before they return.
+struct Scratch {
+    dptr<char> buf;
+    size_t cap = 0;
+    char* get(size_t bytes) {
+        if (bytes > cap) {
+            buf.reset();  // cudaFree waits for the device: no work still uses the old buffer
+            buf = dalloc<char>(bytes);
+            cap = bytes;
+        }
+        return buf.get();
+    }
+};
+
+// Carves 256-byte aligned pieces out of one scratch block.
+struct Carve {
+    size_t off = 0;
+    template <typename T> size_t take(size_t n) {
+        const size_t at = off;
+        off += (n * sizeof(T) + 255) / 256 * 256;
+        return at;
+    }
+};
+
 // A grid download with no field pointer set only reports the box.
 inline bool grid_view_wants_fields(const slab_grid_view& g) { return g.h || g.mass || g.v || g.vz || g.flip || g.F || g.a; }
 

@@ -2,6 +2,8 @@
 // scenarios on a shared terrain and launches their steps together.
 #pragma once
 
+#include <string>
+
 #include <deque>
 #include <memory>
 #include <vector>
@@ -100,6 +102,8 @@ class Engine32 {
         int pick[NK] = {2, 2, 2, 2, 2};
         int fixed[NK] = {};    // > 0: grid set by the caller, not tuned
         int tunes = 0;
+        std::string key;       // a single scenario's workload size: picks shared by later contexts of the same size
+        bool from_cache = false;
         std::vector<cudaEvent_t> ev;  // NK + 2 per schedule step
         ~Tuner() {
             for (auto e : ev) cudaEventDestroy(e);
@@ -113,6 +117,7 @@ class Engine32 {
     void launch_shapes(int out[5]) const;
     // grids[k] > 0 fixes kernel k's grid (NULL: none fixed); tune_on: the tuner runs
     void fix_shapes(const int32_t* grids, bool tune_on);
+    void tune_key_for(int Np);  // single scenario: picks of an earlier context of the same size, if any
     int work_cap = 0;
     int64_t work_cap_total = 0;
     void ensure_work_cap(int64_t need);
@@ -123,6 +128,8 @@ class Engine32 {
     dptr<float> d_gather;                       // node-field downloads
     size_t gather_cap = 0;
     dptr<const float*> d_gather_fp;
+    Scratch scratch;                            // transient buffers of uploads (binning) and particle downloads
+    dptr<int32_t> d_unpack_bad;                 // flag: a particle id out of range
     // node blocks of scenario sid: their ids into d_collect[8...], count and
     // tile box {ti0, ti1, tj0, tj1} to the host; returns the count
     int collect_blocks(int sid, int tbox[4]);

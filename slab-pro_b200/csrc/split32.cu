@@ -6,6 +6,9 @@
 #include <cstdlib>
 #include <type_traits>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <system_error>
 #include <thread>
 #include <vector>
@@ -93,6 +96,39 @@ __global__ void k_pack_particles(PBuf B, int Np, double dx, double rho, float* _
         o[5] = B.z[k];
         o[6] = h;
         o[7] = (float)((double)m / ((double)h * rho));
+    }
+}
+
+// Particle downloads in the reference layout (src/data_arrays.hpp:22-47):
+// particle k of the buffer goes to index id[k] (upload order) of FP64 arrays;
+// x = (cell + offset) dx and A = m / (h rho), each operation rounded as
+// written. A null array is skipped; an id out of range raises *bad.
+struct Unpack {
+    double *x, *v, *vz, *h, *A, *m, *z;
+};
+__global__ void k_unpack_particles(PBuf B, int Np, double dx, double rho, Unpack o, int* __restrict__ bad) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Np; k += gridDim.x * blockDim.x) {
+        const int q = B.id[k];
+        if ((unsigned)q >= (unsigned)Np) {
+            atomicOr(bad, 1);
+            continue;
+        }
+        const int32_t c = B.cell[k];
+        const float2 f = B.f[k];
+        if (o.x) {
+            o.x[2 * q] = __dmul_rn(__dadd_rn((double)cell_i(c), (double)f.x), dx);
+            o.x[2 * q + 1] = __dmul_rn(__dadd_rn((double)cell_j(c), (double)f.y), dx);
+        }
+        if (o.v) {
+            const float2 v = B.v[k];
+            o.v[2 * q] = v.x;
+            o.v[2 * q + 1] = v.y;
+        }
+        if (o.vz) o.vz[q] = B.vz[k];
+        if (o.h) o.h[q] = B.h[k];
+        if (o.m) o.m[q] = B.m[k];
+        if (o.A) o.A[q] = __ddiv_rn((double)B.m[k], __dmul_rn((double)B.h[k], rho));
+        if (o.z) o.z[q] = B.z[k];
     }
 }
 
@@ -450,7 +486,7 @@ int Engine32::add_scenario(const slab_params& p, Ctl* ctl, Ctl* h_ctl, int Np, c
     SLAB_CUDA(cudaMemsetAsync(S.act_stamp.get(), 0xff, ntiles * sizeof(int32_t), st));
     const PBuf out0{S.cell[0].get(), S.f[0].get(), S.v[0].get(), S.h[0].get(), S.m[0].get(), S.id[0].get(), S.vz[0].get(), S.z[0].get()};
     const BinResult bin = bin_particles(T, TY, ntiles, st, Np, x, v, vz, h, m, z, out0, S.grp[0].get(), S.act_list[0].get(),
-                                        S.act_stamp.get(), S.act_cap);
+                                        S.act_stamp.get(), S.act_cap, scratch);
     const std::vector<uint32_t>& alist = bin.tiles;
     // node blocks the t=0 pass will take (the grid tiles of the active tiles'
     // node windows): grow the pool now, as the pass runs before any check
@@ -586,6 +622,30 @@ void Engine32::launch_step() {
 
 constexpr int Engine32::Tuner::FACTOR4[];
 
+namespace {
+// Launch shapes picked for single scenarios, by device, tile count and
+// particle count (half-octave buckets), kept for the process: a later context
+// of the same size starts from them instead of measuring its first steps
+// again. Shapes never change results, only time.
+std::mutex g_tune_mu;
+std::map<std::string, std::vector<int>> g_tune_cache;
+}  // namespace
+
+void Engine32::tune_key_for(int Np) {
+    int dev = 0;
+    SLAB_CUDA(cudaGetDevice(&dev));
+    const int bucket = Np > 0 ? (int)std::floor(2.0 * std::log2((double)Np)) : 0;
+    tune.key = std::to_string(dev) + ":" + std::to_string(TILE) + ":" + std::to_string(ntiles) + ":" + std::to_string(bucket);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const auto it = g_tune_cache.find(tune.key);
+    if (it == g_tune_cache.end() || !tune.enabled) return;
+    std::copy(it->second.begin(), it->second.end(), tune.pick);
+    apply_shapes(tune.pick);
+    graphs.clear();
+    tune.from_cache = true;
+    tune.next = 256;  // no schedule on the first steps; the usual cadence after them
+}
+
 int Engine32::tuned_grid(int k, int c) const {
     if (tune.fixed[k] > 0) return tune.fixed[k];
     return std::max(1, tune.base[k] * Tuner::FACTOR4[c] / 4);
@@ -649,6 +709,10 @@ void Engine32::tune_pick() {
     }
     apply_shapes(tune.pick);
     graphs.clear();  // the step graphs carry the grid sizes
+    if (!tune.key.empty()) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[tune.key] = std::vector<int>(tune.pick, tune.pick + Tuner::NK);
+    }
     tune.state = 0;
     tune.tunes += 1;
     tune.next = std::max<int64_t>(4 * tune.steps, tune.steps + 256);
@@ -781,36 +845,35 @@ void Engine32::download_particles(int sid, double* x, double* v, double* vz, dou
         k32::k_refresh_vz_z<<<std::min(148 * 8, (Np + 255) / 256), 256, 0, st>>>(shared(), host_scn[sid].buf[b], Np, T.z.get());
         SLAB_CUDA(cudaGetLastError());
     }
-    std::vector<int32_t> cell(Np), id(Np);
-    std::vector<float2> f(Np), vv(Np);
-    std::vector<float> hh(Np), mm(Np), vzz(Np), zz(Np);
-    d2h(cell.data(), S.cell[b].get(), Np, st);
-    d2h(id.data(), S.id[b].get(), Np, st);
-    d2h(f.data(), S.f[b].get(), Np, st);
-    d2h(vv.data(), S.v[b].get(), Np, st);
-    d2h(hh.data(), S.h[b].get(), Np, st);
-    d2h(mm.data(), S.m[b].get(), Np, st);
-    d2h(vzz.data(), S.vz[b].get(), Np, st);
-    d2h(zz.data(), S.z[b].get(), Np, st);
+    if (Np <= 0) return;
+    // the reference layout is built on the device, then each requested array
+    // is one copy into the caller's memory (full link speed when it is pinned)
+    double* const host[7] = {x, v, vz, h, A, m, z};
+    const int width[7] = {2, 2, 1, 1, 1, 1, 1};
+    size_t need = 0;
+    for (int a = 0; a < 7; ++a)
+        if (host[a]) need += (size_t)width[a] * Np;
+    if (need == 0) return;
+    double* const buf = reinterpret_cast<double*>(scratch.get(need * sizeof(double)));
+    double* dev[7] = {};
+    size_t off = 0;
+    for (int a = 0; a < 7; ++a)
+        if (host[a]) {
+            dev[a] = buf + off;
+            off += (size_t)width[a] * Np;
+        }
+    if (!d_unpack_bad) d_unpack_bad = dalloc<int32_t>(1);
+    SLAB_CUDA(cudaMemsetAsync(d_unpack_bad.get(), 0, sizeof(int32_t), st));
+    const k32::Unpack o{dev[0], dev[1], dev[2], dev[3], dev[4], dev[5], dev[6]};
+    k32::k_unpack_particles<<<std::max(1, std::min(148 * 8, (Np + 255) / 256)), 256, 0, st>>>(host_scn[sid].buf[b], Np, T.dx, rho, o,
+                                                                                        d_unpack_bad.get());
+    SLAB_CUDA(cudaGetLastError());
+    for (int a = 0; a < 7; ++a)
+        if (host[a]) d2h(host[a], dev[a], (size_t)width[a] * Np, st);
+    int32_t bad = 0;
+    d2h(&bad, d_unpack_bad.get(), 1, st);
     SLAB_CUDA(cudaStreamSynchronize(st));
-    const double dx = T.dx;
-    for (int k = 0; k < Np; ++k) {
-        const int q = id[k];
-        if (q < 0 || q >= Np) throw Error{SLAB_E_CUDA, "corrupt particle id"};
-        if (x) {
-            x[2 * q] = ((double)cell_i(cell[k]) + (double)f[k].x) * dx;
-            x[2 * q + 1] = ((double)cell_j(cell[k]) + (double)f[k].y) * dx;
-        }
-        if (v) {
-            v[2 * q] = vv[k].x;
-            v[2 * q + 1] = vv[k].y;
-        }
-        if (vz) vz[q] = vzz[k];
-        if (h) h[q] = hh[k];
-        if (m) m[q] = mm[k];
-        if (A) A[q] = (double)mm[k] / ((double)hh[k] * rho);
-        if (z) z[q] = zz[k];
-    }
+    if (bad) throw Error{SLAB_E_CUDA, "corrupt particle id"};
 }
 
 std::vector<float> Engine32::gather_nodes(int sid, int stepid, int i0, int j0, int nI, int nJ, const std::vector<const float*>& fields,
@@ -966,6 +1029,7 @@ struct Split32 final : Path {
                 const double* z) override {
         (void)A;
         sid = E.add_scenario(prm, dc, hc, Np, x, v, vz, h, m, z);
+        E.tune_key_for(Np);
     }
     void initial_pass() override { E.launch_t0(); }
     void enqueue_steps(int chunk) override { E.enqueue_steps(chunk); }

@@ -819,7 +819,10 @@ struct P2CSmem {
     P2CStage st;
     float nsum[NQ * TN * TN];  // node sums of the tile's window, [q][node]
     int16_t lc[P2C_CAP];   // local cell of each staged candidate (-1: not in the tile)
-    int16_t idx[P2C_CAP];  // sorted position -> candidate index
+    union {
+        int32_t ccell[P2C_CAP];  // phase 1: cell of each staged candidate
+        int16_t idx[P2C_CAP];    // phases 3-4: sorted position -> candidate index
+    };
     float4 dem[(TILE + 1) * (TILE + 1)];
     int wcur[P2C_WARPS][NCELL];  // per-warp cell counts, then per-warp write cursors
     int s_warp[33];
@@ -931,7 +934,9 @@ __device__ __forceinline__ PQ staged_pq(float4 a, float2 v, float vz, int li, in
 }
 
 // Sums of one particle over the 3 nodes of stencil row A of its cell
-// (src/simulation.cpp:758-795); OUTS adds m vz.
+// (src/simulation.cpp:758-795); OUTS adds m vz. Every operation is rounded
+// as written (explicit multiply-adds), so both variants of the cell P2G, and
+// any later change of the code around them, sum the same bits.
 template <bool OUTS, int A>
 __device__ __forceinline__ void add_particle_row(float (&acc)[NQ][3], const PQ& p) {
     float wx[3], wy[3], dwx[3], dwy[3];
@@ -939,15 +944,15 @@ __device__ __forceinline__ void add_particle_row(float (&acc)[NQ][3], const PQ& 
     bspline3(p.fy, wy, dwy);
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
-        const float wgt = wx[A] * wy[b];
+        const float wgt = __fmul_rn(wx[A], wy[b]);
         if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
-            acc[0][b] += p.m * wgt;
-            acc[1][b] += p.mvx * wgt;
-            acc[2][b] += p.mvy * wgt;
-            acc[3][b] += p.mh * wgt;
-            acc[4][b] += p.Khh * (dwx[A] * wy[b]) - p.Kgx * wgt;
-            acc[5][b] += p.Khh * (dwy[b] * wx[A]) - p.Kgy * wgt;
-            if (OUTS) acc[6][b] += p.mvz * wgt;
+            acc[0][b] = __fmaf_rn(p.m, wgt, acc[0][b]);
+            acc[1][b] = __fmaf_rn(p.mvx, wgt, acc[1][b]);
+            acc[2][b] = __fmaf_rn(p.mvy, wgt, acc[2][b]);
+            acc[3][b] = __fmaf_rn(p.mh, wgt, acc[3][b]);
+            acc[4][b] = __fadd_rn(acc[4][b], __fmaf_rn(p.Khh, __fmul_rn(dwx[A], wy[b]), -__fmul_rn(p.Kgx, wgt)));
+            acc[5][b] = __fadd_rn(acc[5][b], __fmaf_rn(p.Khh, __fmul_rn(dwy[b], wx[A]), -__fmul_rn(p.Kgy, wgt)));
+            if (OUTS) acc[6][b] = __fmaf_rn(p.mvz, wgt, acc[6][b]);
         }
     }
 }
@@ -1008,9 +1013,11 @@ __device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const float4*
 // K2: P2G of one tile (src/simulation.cpp:726-798) as a segmented reduction
 // over cell-sorted particles, with no atomics on floats. The tile's
 // descriptor comes from k_prep; then
-//  1. each warp walks a contiguous block of the tile's candidates, loads them
-//     (into shared memory, unless the tile has more than P2C_CAP candidates)
-//     and counts particles per cell (lanes of one cell are grouped by
+//  1. the tile's candidates and terrain window come into shared memory as
+//     per-thread asynchronous copies, all requested in one round (a tile
+//     with more than P2C_CAP candidates reads only their cells, chunk by
+//     chunk); then each warp walks a contiguous block of the candidates and
+//     counts particles per cell (lanes of one cell are grouped by
 //     __match_any_sync);
 //  2. thread = cell: per-warp write cursors and the cell's range (a scan);
 //  3. the warps walk their blocks again and give each particle its place --
@@ -1024,9 +1031,9 @@ __device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const float4*
 //  5. the node sums are the tile's partial window.
 // The candidates of a tile come in an order fixed by the previous step's G2P
 // (ordered placement), so every sum has a fixed order: results are bitwise
-// reproducible and the same alone or inside a batch. A tile costs two
-// dependent rounds of global loads (descriptor, candidates); each CTA takes
-// a contiguous run of work items.
+// reproducible and the same alone or inside a batch. A tile costs one round
+// of global loads (its descriptor is read while the tile before it runs);
+// each CTA takes a contiguous run of work items.
 // With TMA = true the loads of a tile leave its critical path: while tile n
 // is summed (phases 2-5), thread 0 has the TMA engine copy tile n+1's
 // candidate ranges and terrain window into shared memory (p2c_issue_stage),
@@ -1139,10 +1146,11 @@ __global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MI
                     dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
                 }
         } else {
-            dem = sm.dem;
+            dem = sm.dem;  // asynchronous copies, completed with the candidates' before phase 4
             for (int k = tid; k < DEM_W * DEM_W; k += P2C_THREADS) {
                 const int i = ti * TILE + k / DEM_W, j = tj * TILE + k % DEM_W;
-                dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
+                if (i < sh.Nx && j < sh.Ny) cpa::copy16(&dem[k], sh.dem + (int64_t)i * sh.Ny + j);
+                else dem[k] = make_float4(0.f, 0.f, 1.f, 0.f);
             }
         }
         const int ncand = sm.d.rpref[9];
@@ -1185,35 +1193,77 @@ __global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MI
                 }
             }
         };
-        P2CCand nx;
-        load_cand(k_lo + lane, nx);
-        for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
-            const int k = k0 + lane;
-            const P2CCand q = nx;
-            if (k0 + 32 < k_hi) load_cand(k0 + 32 + lane, nx);
-            int lc = -1;
-            if (q.valid) {
-                const int ci = cell_i(q.cell) - ti * TILE, cj = cell_j(q.cell) - tj * TILE;
-                if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
-                else if (q.d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
-                if (staged) {
+        if (!TMA && staged) {
+            // every thread requests its share of the tile's candidates (and the
+            // terrain window above) as asynchronous copies into the stage: the
+            // whole gather is one load round, with no register held per value
+            for (int k = tid; k < ncand; k += P2C_THREADS) {
+                int d;
+                const int src = cand_to_index(k, sm.d, d);
+                cpa::copy4(&sm.ccell[k], B.cell + src);
+                cpa::copy8(&sm.st.sa[k], B.f + src);  // f.x, f.y
+                cpa::copy4(&sm.st.sa[k].z, B.m + src);
+                cpa::copy4(&sm.st.sa[k].w, B.h + src);
+                cpa::copy8(&sm.st.sv[k], B.v + src);
+                if (outs) cpa::copy4(&sm.st.svz[k], B.vz + src);
+            }
+            cpa::wait_all();
+            __syncthreads();
+            // count per (warp, cell) over the warp's block, as below
+            for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+                const int k = k0 + lane;
+                int lc = -1;
+                if (k < k_hi) {
+                    const int32_t cell = sm.ccell[k];
+                    const int ci = cell_i(cell) - ti * TILE, cj = cell_j(cell) - tj * TILE;
+                    if ((unsigned)ci < TILE && (unsigned)cj < TILE) {
+                        lc = ci * TILE + cj;
+                    } else {
+                        int off;
+                        if (cand_range(k, sm.d, off) == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
+                    }
                     sm.lc[k] = (int16_t)lc;
-                    if (lc >= 0) {
-                        sm.st.sa[k] = make_float4(q.f.x, q.f.y, q.m, q.h);
-                        sm.st.sv[k] = q.v;
-                        sm.st.svz[k] = q.vz;
+                }
+                const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
+                if (lc >= 0) {
+                    const unsigned peers = __match_any_sync(vm, lc);
+                    if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
+                }
+                __syncwarp();
+            }
+        } else {
+            P2CCand nx;
+            load_cand(k_lo + lane, nx);
+            for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
+                const int k = k0 + lane;
+                const P2CCand q = nx;
+                if (k0 + 32 < k_hi) load_cand(k0 + 32 + lane, nx);
+                int lc = -1;
+                if (q.valid) {
+                    const int ci = cell_i(q.cell) - ti * TILE, cj = cell_j(q.cell) - tj * TILE;
+                    if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
+                    else if (q.d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
+                    if (staged) {
+                        sm.lc[k] = (int16_t)lc;
+                        if (lc >= 0) {
+                            sm.st.sa[k] = make_float4(q.f.x, q.f.y, q.m, q.h);
+                            sm.st.sv[k] = q.v;
+                            sm.st.svz[k] = q.vz;
+                        }
                     }
                 }
+                const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
+                if (lc >= 0) {
+                    const unsigned peers = __match_any_sync(vm, lc);
+                    if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
+                }
+                __syncwarp();
             }
-            const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
-            if (lc >= 0) {
-                const unsigned peers = __match_any_sync(vm, lc);
-                if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
-            }
-            __syncwarp();
         }
         if constexpr (TMA) {
             if (tid < DESC_WORDS) reinterpret_cast<int*>(&sm.dnext)[tid] = dn;
+        } else {
+            cpa::wait_all();  // the terrain window of an unstaged tile
         }
         __syncthreads();
         if constexpr (TMA) {
@@ -1725,7 +1775,7 @@ __device__ __forceinline__ int dir_of(int ib, int jb, int ti, int tj) {
 }
 
 #ifndef SLAB_G2P_MIN_BLOCKS
-#define SLAB_G2P_MIN_BLOCKS (NCELL == 64 ? 16 : 3)
+#define SLAB_G2P_MIN_BLOCKS (NCELL == 64 ? 14 : 3)
 #endif
 constexpr int G2P_MIN_BLOCKS = SLAB_G2P_MIN_BLOCKS;  // resident G2P CTAs per SM the register budget is cut for
 
@@ -1778,7 +1828,23 @@ __device__ __forceinline__ void g2p_activate(const G2PScn& z, int tt) {
     }
 }
 
+#ifndef SLAB_G2P_CAP
+#define SLAB_G2P_CAP (NCELL == 64 ? 5 * NCELL : 4 * NCELL)
+#endif
+constexpr int G2P_CAP = SLAB_G2P_CAP;  // candidates of a tile staged in shared memory (more are loaded chunk by chunk)
+
+// a tile's candidates, by candidate index
+struct G2PStage {
+    float2 f[G2P_CAP];
+    float2 v[G2P_CAP];
+    int32_t cell[G2P_CAP];
+    float h[G2P_CAP];
+    float m[G2P_CAP];
+    int32_t id[G2P_CAP];
+};
+
 struct G2PSmem {
+    G2PStage st;
     float4 nv[TN * TN];
     float4 dem[(TILE + 1) * (TILE + 1)];
     int front, back;
@@ -1821,6 +1887,28 @@ __device__ __forceinline__ G2PCand load_g2p_cand(const TileDesc& D, const PBuf& 
     return q;
 }
 
+// candidate k of the tile from the stage (as load_g2p_cand)
+__device__ __forceinline__ G2PCand staged_g2p_cand(const G2PStage& st, int k, int ncand, int t, int TY) {
+    G2PCand q;
+    q.valid = k < ncand;
+    q.src = 0;
+    q.cell = 0;
+    q.pid = 0;
+    q.f = make_float2(1.f, 1.f);
+    q.v = make_float2(0.f, 0.f);
+    q.h = q.m = 0.f;
+    if (q.valid) {
+        q.cell = st.cell[k];
+        q.f = st.f[k];
+        q.v = st.v[k];
+        q.h = st.h[k];
+        q.m = st.m[k];
+        q.pid = st.id[k];
+        q.valid = tile_of_cell(q.cell, TY) == t;
+    }
+    return q;
+}
+
 // K4: G2P (src/simulation.cpp:877-940) of one tile: FLIP/PIC blend,
 // advection, depth update, and the write of the particle into the tile's
 // segment of the next buffer -- stayers from the front, particles that moved
@@ -1828,8 +1916,10 @@ __device__ __forceinline__ G2PCand load_g2p_cand(const TileDesc& D, const PBuf& 
 // max of |v|^2 and the particle bounding box feed the next step's dt and
 // remesh box (K5). Latency: the scenario's values stay in shared memory
 // across a run of its tiles, the next tile's descriptor is requested while
-// this one runs, and a tile's neighbour activations (two dependent atomics)
-// are issued while the next tile's loads are in flight.
+// this one runs, a tile's candidates (up to G2P_CAP), node window and terrain
+// come into shared memory by asynchronous copies requested in one round, and
+// a tile's neighbour activations (two dependent atomics) are issued while the
+// next tile's copies are in flight.
 __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const double* __restrict__ z64) {
     __shared__ G2PSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1858,26 +1948,43 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         const bool outs = Z.outs != 0;
         const bool need_vz = Z.need_vz != 0;
         const int ncand = sm.d.rpref[9];
-        // the first chunk's particles, the node window and the terrain are requested together
-        G2PCand pre = load_g2p_cand(sm.d, Z.B, tid, ncand, t, sh.TY);
+        const bool staged = ncand <= G2P_CAP;
+        // the tile's candidates (the first chunk's, for a tile over the stage),
+        // the node window and the terrain are requested together; the stage
+        // and the windows fill by asynchronous copies
+        G2PCand pre = {};
+        if (staged) {
+            const PBuf& B = Z.B;
+            for (int k = tid; k < ncand; k += NCELL) {
+                int r;
+                const int src = cand_to_index(k, sm.d, r);
+                cpa::copy8(&sm.st.f[k], B.f + src);
+                cpa::copy8(&sm.st.v[k], B.v + src);
+                cpa::copy4(&sm.st.cell[k], B.cell + src);
+                cpa::copy4(&sm.st.h[k], B.h + src);
+                cpa::copy4(&sm.st.m[k], B.m + src);
+                cpa::copy4(&sm.st.id[k], B.id + src);
+            }
+        } else {
+            pre = load_g2p_cand(sm.d, Z.B, tid, ncand, t, sh.TY);
+        }
         for (int k = tid; k < TN * TN; k += NCELL) {
             const int a = k / TN, b = k % TN;
             const int i = ti * TILE + a, j = tj * TILE + b;
-            float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (i < sh.Nx && j < sh.Ny) {
-                const int blk = sm.d.blk4[(a >= TILE ? 2 : 0) + (b >= TILE ? 1 : 0)];
-                if (blk >= 0) val = sh.nv[(size_t)blk * NCELL + (a % TILE) * TILE + (b % TILE)];
-            }
-            sm.nv[k] = val;
+            const int blk = (i < sh.Nx && j < sh.Ny) ? sm.d.blk4[(a >= TILE ? 2 : 0) + (b >= TILE ? 1 : 0)] : -1;
+            if (blk >= 0) cpa::copy16(&sm.nv[k], &sh.nv[(size_t)blk * NCELL + (a % TILE) * TILE + (b % TILE)]);
+            else sm.nv[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
         if (need_vz) {
             for (int k = tid; k < (TILE + 1) * (TILE + 1); k += NCELL) {
                 const int i = ti * TILE + k / (TILE + 1), j = tj * TILE + k % (TILE + 1);
-                sm.dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
+                if (i < sh.Nx && j < sh.Ny) cpa::copy16(&sm.dem[k], sh.dem + (int64_t)i * sh.Ny + j);
+                else sm.dem[k] = make_float4(0.f, 0.f, 1.f, 0.f);
             }
         }
         if (pend_tt >= 0) g2p_activate(Z, pend_tt);  // the previous tile's, while the loads above are in flight
         pend_tt = -1;
+        cpa::wait_all();
         __syncthreads();
         const int total = sm.d.total;
         const int base = sm.d.nxt_off;
@@ -1891,8 +1998,13 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         G2PCand nxt = pre;
         for (int k0 = 0; k0 < ncand; k0 += NCELL) {
             // this chunk's candidates, and the next chunk's requested before this one is computed
-            const G2PCand q = nxt;
-            if (k0 + NCELL < ncand) nxt = load_g2p_cand(sm.d, B, k0 + NCELL + tid, ncand, t, sh.TY);
+            G2PCand q;
+            if (staged) {
+                q = staged_g2p_cand(sm.st, k0 + tid, ncand, t, sh.TY);
+            } else {
+                q = nxt;
+                if (k0 + NCELL < ncand) nxt = load_g2p_cand(sm.d, B, k0 + NCELL + tid, ncand, t, sh.TY);
+            }
             const bool valid = q.valid;
             const int32_t cell = q.cell;
             int d = 4, ib = 0, jb = 0;

@@ -66,4 +66,24 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 
 }  // namespace tma
+
+// Per-thread asynchronous copies global -> shared (cp.async): a thread
+// requests many small copies without holding the values in registers, so a
+// whole work item's gather goes out in one round. Each copy is 4, 8 or 16
+// bytes with both addresses aligned to its size; wait_all() completes the
+// thread's own copies, and a CTA barrier after it shows them to the others.
+namespace cpa {
+
+__device__ __forceinline__ void copy4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(tma::smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(tma::smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tma::smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+}  // namespace cpa
 }  // namespace slab

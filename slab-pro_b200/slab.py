@@ -127,6 +127,14 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
 
 
+def _out_array(a, n: int) -> np.ndarray:
+    """A caller's output array as a flat float64 view of at least n values."""
+    a = np.asarray(a)
+    if a.dtype != np.float64 or not a.flags.c_contiguous or a.size < n:
+        raise ValueError(f"output array must be contiguous float64 of at least {n} values")
+    return a.reshape(-1)[:n]
+
+
 def poisson_disk(Lx: float, Ly: float, r: float, seed: int, k: int = 30) -> np.ndarray:
     """Poisson-disk samples (n, 2) in [0,Lx]x[0,Ly] relative to the corner
     (seed 0 reproduces the reference's rand()-driven sampler)."""
@@ -228,10 +236,18 @@ class Slab:
     def synchronize(self):
         self._check(self.L.slab_synchronize(self.h))
 
-    def particles(self) -> dict:
+    def particles(self, out: dict = None) -> dict:
+        """The particles in the reference layout (FP64, upload order). `out`
+        may hold caller-owned contiguous float64 arrays (pinned host memory
+        makes the copy run at full link speed): x and v of 2 n values, the
+        others of n."""
         n = self.Np
-        out = {k: np.zeros(2 * n if k in ("x", "v") else n) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
-        self._check(self.L.slab_download_particles(self.h, *[_dp(out[k]) for k in ("x", "v", "vz", "h", "A", "mass", "z")]))
+        keys = ("x", "v", "vz", "h", "A", "mass", "z")
+        if out is None:
+            out = {k: np.zeros(2 * n if k in ("x", "v") else n) for k in keys}
+        else:
+            out = {k: _out_array(out[k], 2 * n if k in ("x", "v") else n) for k in keys}
+        self._check(self.L.slab_download_particles(self.h, *[_dp(out[k]) for k in keys]))
         out["x"] = out["x"].reshape(n, 2)
         out["v"] = out["v"].reshape(n, 2)
         return out
@@ -253,9 +269,11 @@ class Slab:
         g.update(Nx=gv.Nx, Ny=gv.Ny, i_off=gv.i_off, j_off=gv.j_off)
         return g
 
-    def max_maps(self):
-        hm = np.zeros(self.Nx * self.Ny)
-        vm = np.zeros(self.Nx * self.Ny)
+    def max_maps(self, out=None):
+        """(h_max, v_max) over the whole terrain; `out` may be a caller-owned
+        pair of contiguous float64 arrays of Nx * Ny values."""
+        n = self.Nx * self.Ny
+        hm, vm = (np.zeros(n), np.zeros(n)) if out is None else (_out_array(out[0], n), _out_array(out[1], n))
         self._check(self.L.slab_download_max(self.h, _dp(hm), _dp(vm)))
         return hm.reshape(self.Nx, self.Ny), vm.reshape(self.Nx, self.Ny)
 
