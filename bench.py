@@ -551,14 +551,17 @@ def _stratified(keys, k):
 def _solo_run(s, cfg, P, prec, stream):
     """One scenario alone through a context: (device seconds of the t=0 pass
     and the step loop, wall seconds from upload to max maps on the host, steps,
-    h_max, v_max2)."""
+    h_max, v_max2). P is the particles or a release built on the device."""
     import torch
     import slab
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     w0 = time.perf_counter()
     s.set_params(cfg, prec)
-    s.upload(P)
+    if "type" in P:  # a release, built on the device
+        s.upload_release(P)
+    else:
+        s.upload(P)
     e0.record(stream)
     s.initial_pass()
     n = s.advance_steps(1 << 40)
@@ -566,6 +569,20 @@ def _solo_run(s, cfg, P, prec, stream):
     hm, vm = s.max_maps()
     wall = time.perf_counter() - w0
     return e0.elapsed_time(e1) * 1e-3, wall, n, hm, vm
+
+
+def release_host_particles(z, dx, cfg, rel, stream):
+    """The particles of a release as FP64 host arrays: built on the device
+    (the reference's setup, bit for bit) and read back through the FP64 path,
+    which keeps the uploaded doubles."""
+    import slab
+    s = slab.Slab(z, dx)
+    s.set_stream(stream.cuda_stream)
+    s.set_params(cfg, slab.FP64_PLAIN)
+    s.upload_release(rel)
+    P = s.particles()
+    s.close()
+    return P
 
 
 def ensemble(args, stream, dev):
@@ -577,21 +594,21 @@ def ensemble(args, stream, dev):
     import workloads as W
     import accuracy as Acc
     g0 = time.perf_counter()
-    c = W.config4(args.c4_scenarios)
+    c = W.config4(args.c4_scenarios, particles=False)  # releases: the particles are built on the device
     gen_s = time.perf_counter() - g0
     z, dx, scen = c["z"], c["dx"], c["scenarios"]
     n = len(scen)
-    Nps = np.array([len(P["h"]) for _, P in scen])
-    out = {"workload": c["name"], "scenarios": n, "particles": int(Nps.sum()), "particles_min_max": [int(Nps.min()), int(Nps.max())],
-           "generate_s": round(gen_s, 1)}
     b = slab.Batch(z, dx, n)
     b.set_stream(stream.cuda_stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     w0 = time.perf_counter()
-    for cfg, P in scen:
-        b.add(cfg, P)
+    for cfg, rel in scen:
+        b.add_release(cfg, rel)
     w_add = time.perf_counter()
+    Nps = np.array(b.Np)
+    out = {"workload": c["name"], "scenarios": n, "particles": int(Nps.sum()), "particles_min_max": [int(Nps.min()), int(Nps.max())],
+           "generate_s": round(gen_s, 1), "setup": "RELEASE ellipses built on the device (slab_batch_add_release), UNIFORM 2x2"}
     l0 = b.kernel_launches()
     run_err = None
     with ClockSampler(dev) as clk:
@@ -659,9 +676,9 @@ def ensemble(args, stream, dev):
         import accuracy as Acc2
         rows32, rows_env = [], []
         for i in [ok[q] for q in _stratified(Nps[ok], args.c4_acc_sample)]:
-            cfg, P = scen[i]
+            cfg, rel = scen[i]
             try:
-                a = accuracy_block(z, dx, cfg, P, stream)
+                a = accuracy_block(z, dx, cfg, release_host_particles(z, dx, cfg, rel, stream), stream)
             except slab.SlabError:
                 continue
             rows32.append(a["fp32_vs_fp64"])
@@ -674,7 +691,8 @@ def ensemble(args, stream, dev):
                                          "e2e": round(out["fp32_batched"]["e2e_scenarios_per_s"] / f64["e2e_scenarios_per_s"], 2)}
     out["note"] = ("scenarios/s: completed scenarios / device time of one batched run; sequential rates are the mean over a "
                    "sample of the completed scenarios stratified by particle count, each run in full (t=0 pass to total_time); "
-                   "e2e includes host binning, uploads and max-map downloads; a scenario whose flow leaves the terrain fails")
+                   "e2e includes the device setup of every release, binning and max-map downloads; a scenario whose flow leaves the "
+                   "terrain fails")
     return out
 
 
@@ -689,10 +707,11 @@ def ensemble_sharded(args, stream, dev, rank, world):
     import slab
     import shard
     import workloads as W
-    c = W.config4(args.c4_scenarios)
+    c = W.config4(args.c4_scenarios, particles=False)
     scen = c["scenarios"]
-    shards = shard.assign([len(P["h"]) * cfg["total_time"] for cfg, P in scen], world,
-                          [shard.footprint_bytes(len(P["h"])) for _, P in scen])
+    est = [W.release_particle_estimate(rel, c["dx"]) for _, rel in scen]
+    shards = shard.assign([est[i] * cfg["total_time"] for i, (cfg, _) in enumerate(scen)], world,
+                          [shard.footprint_bytes(e) for e in est])
     mine = shards[rank]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ok, ps, err, dev_s = 0, 0, None, 0.0
@@ -700,7 +719,7 @@ def ensemble_sharded(args, stream, dev, rank, world):
         b = slab.Batch(c["z"], c["dx"], max(1, len(mine)))
         b.set_stream(stream.cuda_stream)
         for i in mine:
-            b.add(*scen[i])
+            b.add_release(*scen[i])
     except Exception as ex:
         b, err = None, f"{type(ex).__name__}: {ex}"
     dist.barrier()

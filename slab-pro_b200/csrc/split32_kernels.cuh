@@ -766,7 +766,8 @@ __global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh, int cls)
 
 // Optional per-phase cycle counters of the P2G kernel (builds with
 // -DSLAB_PHASE_CLOCKS only): thread 0 of each CTA adds the clock64 cycles of
-// each phase of each tile to g_phase_clk[phase]; g_phase_clk[15] counts tiles.
+// each phase of each tile to g_phase_clk[phase] (cell P2G 0-6, G2P 8-12);
+// g_phase_clk[15] and [14] count their tiles.
 #ifdef SLAB_PHASE_CLOCKS
 __device__ unsigned long long g_phase_clk[16];
 #define SLAB_PHASE_BEGIN long long t_prev_ = clock64()
@@ -782,10 +783,15 @@ __device__ unsigned long long g_phase_clk[16];
     do {                                                          \
         if (threadIdx.x == 0) atomicAdd(&g_phase_clk[15], 1ull); \
     } while (0)
+#define SLAB_PHASE_TILE_G2P()                                     \
+    do {                                                          \
+        if (threadIdx.x == 0) atomicAdd(&g_phase_clk[14], 1ull); \
+    } while (0)
 #else
 #define SLAB_PHASE_BEGIN
 #define SLAB_PHASE_MARK(k)
 #define SLAB_PHASE_TILE()
+#define SLAB_PHASE_TILE_G2P()
 #endif
 
 // index of work item w in its scenario's list (pref: the prefix over scenarios)
@@ -1929,9 +1935,11 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
     if (w0 < w1) load_desc(sh.desc + w0, &sm.d);
     if (tid == 0) sm.z.sid = -1;
     int pend_tt = -1;  // threads 0..8: neighbour tile the previous tile activates
+    SLAB_PHASE_BEGIN;
     for (int w = w0; w < w1; ++w) {
         if (tid < 9) sm.dcnt[tid] = 0;
         __syncthreads();
+        SLAB_PHASE_MARK(8);
         int dn = 0;
         if (w + 1 < w1 && tid < DESC_WORDS) dn = reinterpret_cast<const int*>(sh.desc + w + 1)[tid];
         if (sm.d.sid != sm.z.sid) {  // uniform: a new scenario in this CTA's run
@@ -1984,8 +1992,10 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         }
         if (pend_tt >= 0) g2p_activate(Z, pend_tt);  // the previous tile's, while the loads above are in flight
         pend_tt = -1;
+        SLAB_PHASE_MARK(9);
         cpa::wait_all();
         __syncthreads();
+        SLAB_PHASE_MARK(10);
         const int total = sm.d.total;
         const int base = sm.d.nxt_off;
         const PBuf& B = Z.B;
@@ -2118,6 +2128,7 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
                 if (outs) O.z[pos] = (float)zp;
             }
         }
+        SLAB_PHASE_MARK(11);
         if (tid == 0) {
             sm.front = front;
             sm.back = back;
@@ -2166,6 +2177,8 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         }
         __syncthreads();
         if (w + 1 < w1 && tid < DESC_WORDS) reinterpret_cast<int*>(&sm.d)[tid] = dn;
+        SLAB_PHASE_MARK(12);
+        SLAB_PHASE_TILE_G2P();
     }
     if (pend_tt >= 0) g2p_activate(sm.z, pend_tt);  // the last tile's
 }

@@ -454,17 +454,20 @@ def config3_small(seed: int = 2027):
     return {"name": "fractal4096_dx05_ellipse_uniform_mui", "z": z, "dx": dx, "cfg": cfg, "release": rel, "particles": P}
 
 
-def config4(n_scenarios: int = 256, seed: int = 2028):
+def config4(n_scenarios: int = 256, seed: int = 2028, particles: bool = True):
     """Ensemble on a shared 2048^2 DEM at 2 m (fractal-slope construction,
     roughness 7.5 m RMS): elliptical releases with semi-axes U(20, 300) m,
     centres uniform in the upper third, h0 U(0.5, 3) m, UNIFORM 2x2 sampling
     (1.9 k - 265 k particles, 20.7 M in all), Voellmy with mu U(0.1, 0.4),
     xi U(500, 3000), total_time 60 s; the other parameters as the 35-degree
-    slope case (rho 300, C_cfl 0.5, dt_max 0.01 s, flip_ratio 0.95)."""
+    slope case (rho 300, C_cfl 0.5, dt_max 0.01 s, flip_ratio 0.95).
+    Scenarios are (cfg, particles), or (cfg, release) with particles=False
+    (the release is then built where it runs, e.g. on the device; the same
+    random draws give the same releases either way)."""
     dx = 2.0
     n = 2048
     z = fractal_slope_dem(n, dx, seed=seed, rms=7.5, rim_m=RIM_M)
-    gn = terrain_gradient_norm(z, dx)
+    gn = terrain_gradient_norm(z, dx) if particles else None
     rng = np.random.default_rng(seed + 1)
     L = n * dx
     out = []
@@ -478,8 +481,19 @@ def config4(n_scenarios: int = 256, seed: int = 2028):
                    friction="VOELLMY", voellmy_mu=float(rng.uniform(0.1, 0.4)), voellmy_xi=float(rng.uniform(500.0, 3000.0)))
         rel = {"type": "ELLIPSE", "center": (float(cx), float(cy)), "rx": float(rx), "ry": float(ry), "rotation_deg": float(rot),
                "h0": float(rng.uniform(0.5, 3.0))}
-        out.append((cfg, release_particles(z, dx, rel, cfg["rho"], fast_theta=True, grad_norm=gn)))
+        out.append((cfg, release_particles(z, dx, rel, cfg["rho"], fast_theta=True, grad_norm=gn) if particles else rel))
     return {"name": f"ensemble{n_scenarios}_fractal2048_dx2_voellmy", "z": z, "dx": dx, "scenarios": out}
+
+
+def release_particle_estimate(rel: dict, dx: float) -> int:
+    """About how many particles UNIFORM 2x2 sampling gives an ELLIPSE or
+    RECTANGLE release (4 per covered cell), for balancing work before the
+    particles exist."""
+    if rel["type"] == "ELLIPSE":
+        area = np.pi * rel["rx"] * rel["ry"]
+    else:
+        area = rel["Lx"] * rel["Ly"]
+    return int(round(4.0 * area / (dx * dx)))
 
 
 def config5_stream(z: np.ndarray, dx: float, window_s: float, seed: int = 2029, rate: float = 20.0, median: float = 20000.0,
