@@ -810,7 +810,10 @@ __device__ __forceinline__ int cached_work(const Shared& sh, const int32_t* pref
 
 
 constexpr int P2C_THREADS = NCELL;  // one thread per cell of the tile
-constexpr int P2C_MIN_BLOCKS = NCELL == 64 ? 12 : 3;  // resident CTAs per SM the register budget is cut for
+#ifndef SLAB_P2C_MIN_BLOCKS
+#define SLAB_P2C_MIN_BLOCKS (NCELL == 64 ? 12 : 3)
+#endif
+constexpr int P2C_MIN_BLOCKS = SLAB_P2C_MIN_BLOCKS;  // resident CTAs per SM the register budget is cut for
 constexpr int P2C_WARPS = P2C_THREADS / 32;
 constexpr int NSLOT = 9;            // nodes a cell's particles reach (3 x 3)
 constexpr int P2C_CAP = 6 * NCELL;  // candidates of a tile staged in shared memory (more go through global memory)
@@ -939,45 +942,51 @@ __device__ __forceinline__ PQ staged_pq(float4 a, float2 v, float vz, int li, in
     return p;
 }
 
-// Sums of one particle over the 3 nodes of stencil row A of its cell
-// (src/simulation.cpp:758-795); OUTS adds m vz. Every operation is rounded
-// as written (explicit multiply-adds), so both variants of the cell P2G, and
-// any later change of the code around them, sum the same bits.
-template <bool OUTS, int A>
-__device__ __forceinline__ void add_particle_row(float (&acc)[NQ][3], const PQ& p) {
+// Sums of one particle over the 3 nodes of stencil rows A0 .. A0+NA-1 of its
+// cell (src/simulation.cpp:758-795); OUTS adds m vz. Every operation is
+// rounded as written (explicit multiply-adds), so both variants of the cell
+// P2G, and any later change of the code around them, sum the same bits.
+template <bool OUTS, int A0, int NA>
+__device__ __forceinline__ void add_particle_rows(float (&acc)[NA][NQ][3], const PQ& p) {
     float wx[3], wy[3], dwx[3], dwy[3];
     bspline3(p.fx, wx, dwx);
     bspline3(p.fy, wy, dwy);
 #pragma unroll
-    for (int b = 0; b < 3; ++b) {
-        const float wgt = __fmul_rn(wx[A], wy[b]);
-        if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
-            acc[0][b] = __fmaf_rn(p.m, wgt, acc[0][b]);
-            acc[1][b] = __fmaf_rn(p.mvx, wgt, acc[1][b]);
-            acc[2][b] = __fmaf_rn(p.mvy, wgt, acc[2][b]);
-            acc[3][b] = __fmaf_rn(p.mh, wgt, acc[3][b]);
-            acc[4][b] = __fadd_rn(acc[4][b], __fmaf_rn(p.Khh, __fmul_rn(dwx[A], wy[b]), -__fmul_rn(p.Kgx, wgt)));
-            acc[5][b] = __fadd_rn(acc[5][b], __fmaf_rn(p.Khh, __fmul_rn(dwy[b], wx[A]), -__fmul_rn(p.Kgy, wgt)));
-            if (OUTS) acc[6][b] = __fmaf_rn(p.mvz, wgt, acc[6][b]);
+    for (int a = 0; a < NA; ++a) {
+        const int A = A0 + a;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const float wgt = __fmul_rn(wx[A], wy[b]);
+            if (wgt > 3e-3f) {  // the reference's weight cut-off (src/simulation.cpp:780)
+                acc[a][0][b] = __fmaf_rn(p.m, wgt, acc[a][0][b]);
+                acc[a][1][b] = __fmaf_rn(p.mvx, wgt, acc[a][1][b]);
+                acc[a][2][b] = __fmaf_rn(p.mvy, wgt, acc[a][2][b]);
+                acc[a][3][b] = __fmaf_rn(p.mh, wgt, acc[a][3][b]);
+                acc[a][4][b] = __fadd_rn(acc[a][4][b], __fmaf_rn(p.Khh, __fmul_rn(dwx[A], wy[b]), -__fmul_rn(p.Kgx, wgt)));
+                acc[a][5][b] = __fadd_rn(acc[a][5][b], __fmaf_rn(p.Khh, __fmul_rn(dwy[b], wx[A]), -__fmul_rn(p.Kgy, wgt)));
+                if (OUTS) acc[a][6][b] = __fmaf_rn(p.mvz, wgt, acc[a][6][b]);
+            }
         }
     }
 }
 
-// Row-A sums of one cell's particles in sorted order: staged in shared
-// memory, or (tiles over P2C_CAP candidates) read through the sorted index
-// list in global memory.
-template <bool OUTS, int A>
-__device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, const P2CSmem& sm, const float4* dem,
+// Rows A0 .. A0+NA-1 of one cell's particles, summed in sorted order: staged
+// in shared memory, or (tiles over P2C_CAP candidates) read through the
+// sorted index list in global memory.
+template <bool OUTS, int A0, int NA>
+__device__ __forceinline__ void cell_row_sums(float (&acc)[NA][NQ][3], bool staged, const P2CSmem& sm, const float4* dem,
                                               const int32_t* __restrict__ order, int c0, int nn, const PBuf& B, int li, int lj, float g,
                                               float hod) {
 #pragma unroll
-    for (int q = 0; q < NQ; ++q)
+    for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int b = 0; b < 3; ++b) acc[q][b] = 0.f;
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) acc[a][q][b] = 0.f;
     if (staged) {
         for (int r = c0; r < c0 + nn; ++r) {
             const int k = sm.idx[r];
-            add_particle_row<OUTS, A>(acc, staged_pq(sm.st.sa[k], sm.st.sv[k], sm.st.svz[k], li, lj, dem, g, hod));
+            add_particle_rows<OUTS, A0, NA>(acc, staged_pq(sm.st.sa[k], sm.st.sv[k], sm.st.svz[k], li, lj, dem, g, hod));
         }
         return;
     }
@@ -985,35 +994,47 @@ __device__ __forceinline__ void cell_row_sums(float (&acc)[NQ][3], bool staged, 
     for (int r = 0; r < nn; ++r) {
         const int src = nsrc;
         if (r + 1 < nn) nsrc = order[c0 + r + 1];
-        add_particle_row<OUTS, A>(acc, load_pq(B, src, li, lj, dem, g, hod, OUTS));
+        add_particle_rows<OUTS, A0, NA>(acc, load_pq(B, src, li, lj, dem, g, hod, OUTS));
     }
 }
 
-// Stencil row A of every cell into the node sums: in round (A, b) each node
-// receives the row sum of exactly one cell, so the rounds need no atomics and
-// every node adds its <= 9 cells in (a, b) order.
-template <bool OUTS, int A>
-__device__ __forceinline__ void p2c_row(P2CSmem& sm, bool staged, const float4* dem, const int32_t* __restrict__ order, int c0, int nn,
-                                        const PBuf& B,
-                                        int li, int lj, float g, float hod) {
-    float acc[NQ][3];
-    cell_row_sums<OUTS, A>(acc, staged, sm, dem, order, c0, nn, B, li, lj, g, hod);
+// Stencil rows A0 .. A0+NA-1 of every cell into the node sums: in round
+// (A, b) each node receives the row sum of exactly one cell, so the rounds
+// need no atomics and every node adds its <= 9 cells in (a, b) order.
+template <bool OUTS, int A0, int NA>
+__device__ __forceinline__ void p2c_rowset(P2CSmem& sm, bool staged, const float4* dem, const int32_t* __restrict__ order, int c0,
+                                           int nn, const PBuf& B, int li, int lj, float g, float hod) {
+    float acc[NA][NQ][3];
+    cell_row_sums<OUTS, A0, NA>(acc, staged, sm, dem, order, c0, nn, B, li, lj, g, hod);
 #pragma unroll
-    for (int b = 0; b < 3; ++b) {
-        __syncthreads();
-        const int nd = (li + A) * TN + (lj + b);
+    for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int q = 0; q < (OUTS ? NQ : NQ - 1); ++q) sm.nsum[q * TN * TN + nd] += acc[q][b];
-    }
+        for (int b = 0; b < 3; ++b) {
+            __syncthreads();
+            const int nd = (li + A0 + a) * TN + (lj + b);
+#pragma unroll
+            for (int q = 0; q < (OUTS ? NQ : NQ - 1); ++q) sm.nsum[q * TN * TN + nd] += acc[a][q][b];
+        }
 }
 
+// Rows per pass over a cell's particles: each pass evaluates the particles'
+// weights and quantities once; more rows per pass cost accumulator registers.
+#ifndef SLAB_P2C_ROWS
+#define SLAB_P2C_ROWS 2
+#endif
 template <bool OUTS>
 __device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const float4* dem, const int32_t* __restrict__ order, int c0, int nn,
-                                         const PBuf& B,
-                                         int li, int lj, float g, float hod) {
-    p2c_row<OUTS, 0>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
-    p2c_row<OUTS, 1>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
-    p2c_row<OUTS, 2>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+                                         const PBuf& B, int li, int lj, float g, float hod) {
+    if constexpr (SLAB_P2C_ROWS == 3) {
+        p2c_rowset<OUTS, 0, 3>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+    } else if constexpr (SLAB_P2C_ROWS == 2) {
+        p2c_rowset<OUTS, 0, 2>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+        p2c_rowset<OUTS, 2, 1>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+    } else {
+        p2c_rowset<OUTS, 0, 1>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+        p2c_rowset<OUTS, 1, 1>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+        p2c_rowset<OUTS, 2, 1>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
+    }
 }
 
 // K2: P2G of one tile (src/simulation.cpp:726-798) as a segmented reduction
@@ -1203,9 +1224,10 @@ __global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MI
             // every thread requests its share of the tile's candidates (and the
             // terrain window above) as asynchronous copies into the stage: the
             // whole gather is one load round, with no register held per value
+            int d = 0;  // range of candidate k: k only grows, so d is carried (rpref[9] = ncand > k bounds it by 8)
             for (int k = tid; k < ncand; k += P2C_THREADS) {
-                int d;
-                const int src = cand_to_index(k, sm.d, d);
+                while (sm.d.rpref[d + 1] <= k) ++d;
+                const int src = sm.d.rstart[d] + (k - sm.d.rpref[d]);
                 cpa::copy4(&sm.ccell[k], B.cell + src);
                 cpa::copy8(&sm.st.sa[k], B.f + src);  // f.x, f.y
                 cpa::copy4(&sm.st.sa[k].z, B.m + src);
@@ -1963,9 +1985,10 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         G2PCand pre = {};
         if (staged) {
             const PBuf& B = Z.B;
+            int d = 0;  // range of candidate k, carried as k grows (bounded by 8: rpref[9] = ncand > k)
             for (int k = tid; k < ncand; k += NCELL) {
-                int r;
-                const int src = cand_to_index(k, sm.d, r);
+                while (sm.d.rpref[d + 1] <= k) ++d;
+                const int src = sm.d.rstart[d] + (k - sm.d.rpref[d]);
                 cpa::copy8(&sm.st.f[k], B.f + src);
                 cpa::copy8(&sm.st.v[k], B.v + src);
                 cpa::copy4(&sm.st.cell[k], B.cell + src);
