@@ -262,6 +262,11 @@ slab_status slab_work_counters(slab_ctx* ctx, int64_t out[2]);
  * until its next tuning pass). Shapes never change results. */
 slab_status slab_launch_shapes(slab_ctx* ctx, int32_t out[6]);
 
+/* FP32_SPLIT: persistent steps for this context (as
+ * slab_batch_set_persistent); kept across later uploads. SLAB_E_ARG for
+ * FP64_PLAIN parameters. */
+slab_status slab_set_persistent(slab_ctx* ctx, int32_t on, int64_t limit_cycles);
+
 /* Number of kernels this context has launched since creation. */
 int64_t slab_kernel_launches(const slab_ctx* ctx);
 
@@ -332,6 +337,19 @@ slab_status slab_batch_launch_shapes(slab_batch* b, int32_t out[6]);
 /* grids[k] > 0 fixes kernel k's CTA count, 0 leaves it to the tuner (grids
  * NULL: none fixed); tune = 0 stops the tuner (shapes stay as they are). */
 slab_status slab_batch_set_launch_shapes(slab_batch* b, const int32_t grids[5], int32_t tune);
+/* Persistent steps (on = 1): each chunk of up to 32 steps becomes ONE
+ * cooperative launch of a kernel that runs the step's phases (tile
+ * bookkeeping, both P2G classes, grid update, G2P, end of step) for every
+ * scenario, separated by grid-wide barriers instead of kernel boundaries, and
+ * ends early once no scenario has work. The results are bitwise those of the
+ * default path (separate kernels in CUDA graphs). Every barrier wait gives up
+ * after limit_cycles SM clock cycles (0: keep the current limit, by default
+ * 4e9, about two seconds): the waiting CTAs leave the kernel and every
+ * scenario fails with SLAB_E_TIMEOUT, the device stays usable. The launch
+ * shapes are then fixed (as many CTAs as fit on the device at once) and the
+ * tuner does not run. SLAB_E_ARG if the device cannot launch cooperatively.
+ * The environment variable SLAB_PERSIST=1 turns it on for every engine. */
+slab_status slab_batch_set_persistent(slab_batch* b, int32_t on, int64_t limit_cycles);
 const char* slab_batch_last_error(const slab_batch* b);
 void slab_batch_destroy(slab_batch* b);
 

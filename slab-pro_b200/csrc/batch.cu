@@ -68,6 +68,7 @@ slab_status status_of(int e) {
     if (e & ERR_NONFINITE) return SLAB_E_NONFINITE;
     if (e & (ERR_DOMAIN | ERR_MOVE)) return SLAB_E_DOMAIN;
     if (e & ERR_CAPACITY) return SLAB_E_OOM;
+    if (e & ERR_TIMEOUT) return SLAB_E_TIMEOUT;
     return SLAB_OK;
 }
 
@@ -196,8 +197,15 @@ slab_status slab_batch_run(slab_batch* b, int64_t max_steps, int64_t* steps_out)
             done += k;
             b->E->check_capacity();
             pull_all(b);
-            bool all_stopped = true;
-            for (int s = 0; s < b->E->nscn; ++s) all_stopped &= b->h_ctl[s].stop != 0;
+            bool all_stopped = true, gave_up = false;
+            for (int s = 0; s < b->E->nscn; ++s) {
+                all_stopped &= b->h_ctl[s].stop != 0;
+                gave_up |= (b->h_ctl[s].err & ERR_TIMEOUT) != 0;
+            }
+            if (gave_up) {  // a persistent launch left its step half done: no step may follow
+                b->E->dead = true;
+                break;
+            }
             if (all_stopped) break;
         }
         pull_all(b);
@@ -321,6 +329,11 @@ slab_status slab_batch_launch_shapes(slab_batch* b, int32_t out[6]) {
         for (int k = 0; k < 5; ++k) out[k] = g[k];
         out[5] = b->E->tune.tunes;
     });
+}
+
+slab_status slab_batch_set_persistent(slab_batch* b, int32_t on, int64_t limit_cycles) {
+    if (!b || limit_cycles < 0) return SLAB_E_ARG;
+    return bguard(b, [&] { b->E->set_persistent(on != 0, limit_cycles); });
 }
 
 slab_status slab_batch_set_launch_shapes(slab_batch* b, const int32_t grids[5], int32_t tune) {

@@ -45,6 +45,8 @@ struct slab_ctx {
     std::string err;
     int64_t extra_launches = 0;
     int chunk = 32;
+    int persist = -1;              // -1: the engine's default; 0 / 1 set by slab_set_persistent
+    long long persist_limit = 0;
     cudaStream_t copy_stream = nullptr;  // frame copies to the host
     FrameSlot frames[2];
 };
@@ -121,7 +123,7 @@ void raise_device_errors(slab_ctx* c) {
     if (e & ERR_NONFINITE) throw Error{SLAB_E_NONFINITE, "non-finite particle state"};
     if (e & (ERR_DOMAIN | ERR_MOVE)) throw Error{SLAB_E_DOMAIN, "a particle stencil left the terrain"};
     if (e & ERR_CAPACITY) throw Error{SLAB_E_OOM, "device capacity exceeded"};
-    if (e & ERR_TIMEOUT) throw Error{SLAB_E_TIMEOUT, "bounded device wait gave up"};
+    if (e & ERR_TIMEOUT) throw Error{SLAB_E_TIMEOUT, "bounded device wait gave up"};  // the engine takes no further steps
 }
 
 void arm(slab_ctx* c, int64_t steps_left, int stop_at_frame) {
@@ -271,6 +273,7 @@ void upload_arrays(slab_ctx* c, int32_t Np, const double* x, const double* v, co
         c->path = make_plain64(c->terrain, c->params, c->stream, c->d_ctl, c->h_ctl);
     else
         c->path = make_split32(c->terrain, c->params, c->stream, c->d_ctl, c->h_ctl);
+    if (c->persist >= 0 && c->params.precision != SLAB_FP64_PLAIN) c->path->set_persistent(c->persist != 0, c->persist_limit);
     c->path->upload(Np, x, v, vz, h, A, m, z);
     pull_ctl(c);
     raise_device_errors(c);
@@ -510,6 +513,17 @@ slab_status slab_launch_shapes(slab_ctx* c, int32_t out[6]) {
     return guard(c, [&] {
         need(c->uploaded, SLAB_E_STATE, "no particles uploaded");
         c->path->launch_shapes(out);
+    });
+}
+
+slab_status slab_set_persistent(slab_ctx* c, int32_t on, int64_t limit_cycles) {
+    if (!c) return SLAB_E_ARG;
+    return guard(c, [&] {
+        need(limit_cycles >= 0, SLAB_E_ARG, "limit_cycles must be >= 0");
+        need(c->have_params && c->params.precision != SLAB_FP64_PLAIN, SLAB_E_ARG, "persistent steps need FP32_SPLIT parameters");
+        if (c->path) c->path->set_persistent(on != 0, limit_cycles);
+        c->persist = on != 0 ? 1 : 0;
+        if (limit_cycles > 0) c->persist_limit = limit_cycles;
     });
 }
 

@@ -207,6 +207,8 @@ struct Path {
     virtual void set_profiling(bool) {}
     // CTA counts of the work kernels and tuning passes (the FP32 path's tuner)
     virtual void launch_shapes(int32_t out[6]) { for (int k = 0; k < 6; ++k) out[k] = 0; }
+    // chunks of steps as one persistent cooperative launch (FP32_SPLIT)
+    virtual void set_persistent(bool, long long) { throw Error{SLAB_E_ARG, "persistent steps need FP32_SPLIT"}; }
 };
 
 std::unique_ptr<Path> make_plain64(const Terrain& t, const slab_params& p, cudaStream_t s, Ctl* d_ctl, Ctl* h_ctl);

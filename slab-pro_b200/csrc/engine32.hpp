@@ -42,6 +42,16 @@ class Engine32 {
     void launch_p2g(const Shared& sh);
     void launch_p2g_cell(const Shared& sh, int cls);
     bool p2g_tma = false;  // k_p2g_cell<true>: the next tile's loads staged by TMA bulk copies (SLAB_P2G_TMA=1)
+    // persistent steps: a chunk of steps as one cooperative launch of k_persist
+    // (SLAB_PERSIST=1 or set_persistent); its grid waits give up after
+    // persist_limit clock cycles (ERR_TIMEOUT)
+    bool persist = false;
+    long long persist_limit = 4000000000ll;
+    int grid_persist = 0;
+    dptr<unsigned> d_bar;  // k32::GridBar
+    bool dead = false;     // a persistent launch gave up: no further steps
+    void set_persistent(bool on, long long limit_cycles);
+    void launch_persistent(int chunk);
     void arm(int64_t steps_left, int stop_at_frame);
     int acc_mode = 5;  // P2G scheme (k32::ACC_*): dense tiles cell-sorted, sparse tiles fixed point
     int split_min = 3 * NCELL / 4;  // ACC_MIXED: tiles with more particles take the cell-sorted P2G (measured)

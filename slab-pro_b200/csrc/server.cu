@@ -271,6 +271,8 @@ void worker_loop(slab_server* s) {
                     cancel = s->reqs[id].cancel;
                 }
                 const Ctl& c = s->h_ctl[k];
+                if (c.err & ERR_TIMEOUT)  // a persistent launch gave up at a barrier: the engine's step state is incomplete
+                    throw Error{SLAB_E_TIMEOUT, "a bounded device wait gave up; the engine stopped"};
                 if (c.err) {
                     finish(s, k, REQ_FAILED, "device error flags " + std::to_string(c.err));
                 } else if (cancel) {

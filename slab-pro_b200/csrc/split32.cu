@@ -252,6 +252,14 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     const int base[Tuner::NK] = {grid_prep, grid_p2g_cell, grid_p2g_sparse, grid_grid, grid_g2p};
     std::copy(base, base + Tuner::NK, tune.base);
     if (const char* e = std::getenv("SLAB_TUNE")) tune.enabled = std::atoi(e) != 0;
+    // the persistent step kernel: as many CTAs as can be resident at once
+    // (a cooperative launch needs every CTA on the device together)
+    int coop = 0, occ_ps = 0;
+    SLAB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    SLAB_CUDA(cudaFuncSetAttribute(k32::k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k32::PERSIST_SMEM));
+    SLAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ps, k32::k_persist, NCELL, k32::PERSIST_SMEM));
+    grid_persist = coop ? sms * occ_ps : 0;
+    if (const char* e = std::getenv("SLAB_PERSIST")) persist = std::atoi(e) != 0 && grid_persist > 0;
     timer.nk = 5;  // k_prep, P2G, grid update, G2P, k_end
     const int phase_map[5] = {1, 2, 3, 4, 0};
     for (int k = 0; k < 5; ++k) timer.phase_of[k] = phase_map[k];
@@ -718,7 +726,51 @@ void Engine32::tune_pick() {
     tune.next = std::max<int64_t>(4 * tune.steps, tune.steps + 256);
 }
 
+void Engine32::set_persistent(bool on, long long limit_cycles) {
+    if (on && grid_persist <= 0) throw Error{SLAB_E_ARG, "this device cannot run a cooperative launch"};
+    if (!on && persist && d_bar) {  // back to separate kernels: only from a complete step state
+        k32::GridBar b{};
+        d2h(&b, reinterpret_cast<k32::GridBar*>(d_bar.get()), 1, st);
+        SLAB_CUDA(cudaStreamSynchronize(st));
+        if (b.dead) dead = true;
+    }
+    if (on && acc_mode != k32::ACC_MIXED) throw Error{SLAB_E_ARG, "persistent steps run the default P2G scheme only"};
+    persist = on;
+    if (limit_cycles > 0) persist_limit = limit_cycles;
+}
+
+// One cooperative launch of k_persist for `chunk` steps. The barrier state
+// starts from zero at every launch (a launch whose waits ran out leaves it
+// anywhere).
+void Engine32::launch_persistent(int chunk) {
+    if (!d_bar) {
+        d_bar = dalloc<unsigned>(sizeof(k32::GridBar) / sizeof(unsigned));
+        SLAB_CUDA(cudaMemsetAsync(d_bar.get(), 0, sizeof(k32::GridBar), st));
+    }
+    SLAB_CUDA(cudaMemsetAsync(d_bar.get(), 0, 2 * sizeof(unsigned), st));  // count and generation; `dead` stays
+    Shared sh = shared();
+    const double* z64 = T.z.get();
+    int n = chunk;
+    long long lim = persist_limit;
+    k32::GridBar* bar = reinterpret_cast<k32::GridBar*>(d_bar.get());
+    void* args[] = {&sh, &z64, &n, &lim, &bar};
+    SLAB_CUDA(cudaLaunchCooperativeKernel((const void*)k32::k_persist, dim3(grid_persist), dim3(NCELL), args, k32::PERSIST_SMEM, st));
+    nlaunch += 1;
+}
+
 void Engine32::enqueue_steps(int chunk) {
+    if (persist && d_bar && timer.on) {  // profiled steps run the separate kernels: only from a complete step state
+        k32::GridBar b{};
+        d2h(&b, reinterpret_cast<k32::GridBar*>(d_bar.get()), 1, st);
+        SLAB_CUDA(cudaStreamSynchronize(st));
+        if (b.dead) dead = true;
+    }
+    if (dead) throw Error{SLAB_E_TIMEOUT, "an earlier persistent launch gave up at a barrier; the step state is incomplete"};
+    if (persist && acc_mode == k32::ACC_MIXED && !timer.on) {
+        launch_persistent(chunk);
+        tune.steps += chunk;
+        return;
+    }
     if (graph_nscn != nscn) {
         graphs.clear();
         graph_nscn = nscn;
@@ -1061,6 +1113,7 @@ struct Split32 final : Path {
         for (int k = 0; k < 5; ++k) out[k] = g[k];
         out[5] = E.tune.tunes;
     }
+    void set_persistent(bool on, long long limit_cycles) override { E.set_persistent(on, limit_cycles); }
 };
 
 }  // namespace

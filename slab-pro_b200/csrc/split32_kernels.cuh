@@ -252,10 +252,10 @@ static_assert(sizeof(TileDesc) == 28 * 4 && offsetof(TileDesc, rstart) == 4 * 4 
                   offsetof(TileDesc, blk4) == 23 * 4,
               "k_prep writes the descriptor word by word");
 
-__global__ void __launch_bounds__(PREP_THREADS) k_prep(Shared sh) {
+__device__ __forceinline__ void prep_body(const Shared& sh) {
     const int nwork = sh.work_pref[sh.nscn];
     const int lane = threadIdx.x & 31, r = lane & (PREP_LANES - 1);
-    const int per_block = PREP_THREADS / PREP_LANES;
+    const int per_block = (int)blockDim.x / PREP_LANES;
     const int stride = gridDim.x * per_block;
     // whole warps run every iteration (the shuffles need both halves); a half
     // without a tile computes with valid = false
@@ -365,6 +365,8 @@ __global__ void __launch_bounds__(PREP_THREADS) k_prep(Shared sh) {
         }
     }
 }
+
+__global__ void __launch_bounds__(PREP_THREADS) k_prep(Shared sh) { prep_body(sh); }
 
 // ------------------------------------------------------------------- P2G
 
@@ -975,7 +977,7 @@ __device__ __forceinline__ void add_particle_rows(float (&acc)[NA][NQ][3], const
 // sorted index list in global memory.
 template <bool OUTS, int A0, int NA>
 __device__ __forceinline__ void cell_row_sums(float (&acc)[NA][NQ][3], bool staged, const P2CSmem& sm, const float4* dem,
-                                              const int32_t* __restrict__ order, int c0, int nn, const PBuf& B, int li, int lj, float g,
+                                              const int32_t* order, int c0, int nn, const PBuf& B, int li, int lj, float g,
                                               float hod) {
 #pragma unroll
     for (int a = 0; a < NA; ++a)
@@ -1002,7 +1004,7 @@ __device__ __forceinline__ void cell_row_sums(float (&acc)[NA][NQ][3], bool stag
 // (A, b) each node receives the row sum of exactly one cell, so the rounds
 // need no atomics and every node adds its <= 9 cells in (a, b) order.
 template <bool OUTS, int A0, int NA>
-__device__ __forceinline__ void p2c_rowset(P2CSmem& sm, bool staged, const float4* dem, const int32_t* __restrict__ order, int c0,
+__device__ __forceinline__ void p2c_rowset(P2CSmem& sm, bool staged, const float4* dem, const int32_t* order, int c0,
                                            int nn, const PBuf& B, int li, int lj, float g, float hod) {
     float acc[NA][NQ][3];
     cell_row_sums<OUTS, A0, NA>(acc, staged, sm, dem, order, c0, nn, B, li, lj, g, hod);
@@ -1023,7 +1025,7 @@ __device__ __forceinline__ void p2c_rowset(P2CSmem& sm, bool staged, const float
 #define SLAB_P2C_ROWS 2
 #endif
 template <bool OUTS>
-__device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const float4* dem, const int32_t* __restrict__ order, int c0, int nn,
+__device__ __forceinline__ void p2c_rows(P2CSmem& sm, bool staged, const float4* dem, const int32_t* order, int c0, int nn,
                                          const PBuf& B, int li, int lj, float g, float hod) {
     if constexpr (SLAB_P2C_ROWS == 3) {
         p2c_rowset<OUTS, 0, 3>(sm, staged, dem, order, c0, nn, B, li, lj, g, hod);
@@ -1112,9 +1114,8 @@ struct P2CCand {
 };
 
 template <bool TMA>
-__global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MIN_BLOCKS) k_p2g_cell(Shared sh, int cls) {
+__device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigned char* smem_raw) {
     using Sm = typename std::conditional<TMA, P2CSmemTma, P2CSmem>::type;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     Sm& sm = *reinterpret_cast<Sm*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -1366,6 +1367,12 @@ __global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MI
     SLAB_PHASE_MARK(6);
 }
 
+template <bool TMA>
+__global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MIN_BLOCKS) k_p2g_cell(Shared sh, int cls) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    p2g_cell_body<TMA>(sh, cls, smem_raw);
+}
+
 // ----------------------------------------------------- P2G of sparse tiles
 
 // K2 for tiles with at most split_min particles (src/simulation.cpp:726-798).
@@ -1418,8 +1425,7 @@ __device__ __forceinline__ PQ make_pq(float2 f, float2 v, float m, float h, floa
     return p;
 }
 
-__global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shared sh, int cls) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void p2g_sparse_body(const Shared& sh, int cls, unsigned char* smem_raw) {
     P2SSmem& sm = *reinterpret_cast<P2SSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31;
     int i0, i1;
@@ -1594,6 +1600,11 @@ __global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shar
     }
 }
 
+__global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shared sh, int cls) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    p2g_sparse_body(sh, cls, smem_raw);
+}
+
 // ------------------------------------------------------------ grid update
 
 // Values of one scenario that the grid update reads for every grid tile.
@@ -1639,7 +1650,7 @@ __device__ __forceinline__ void load_grid_scn(const Shared& sh, int sid, GridScn
 // the conservation diagnostic.
 // Latency: the scenario's values stay in shared memory across a run of its
 // grid tiles, and thread 0 reads the grid-tile list two entries ahead.
-__global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
+__device__ __forceinline__ void grid_body(const Shared& sh) {
     __shared__ int s_gt, s_blk;
     __shared__ int s_slot[4];
     __shared__ double s_red[NCELL / 32];
@@ -1793,6 +1804,8 @@ __global__ void __launch_bounds__(NCELL) k_grid(Shared sh) {
         __syncthreads();
     }
 }
+
+__global__ void __launch_bounds__(NCELL) k_grid(Shared sh) { grid_body(sh); }
 
 // -------------------------------------------------------------------- G2P
 
@@ -1948,8 +1961,7 @@ __device__ __forceinline__ G2PCand staged_g2p_cand(const G2PStage& st, int k, in
 // come into shared memory by asynchronous copies requested in one round, and
 // a tile's neighbour activations (two dependent atomics) are issued while the
 // next tile's copies are in flight.
-__global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const double* __restrict__ z64) {
-    __shared__ G2PSmem sm;
+__device__ __forceinline__ void g2p_body(const Shared& sh, const double* __restrict__ z64, G2PSmem& sm) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwork = sh.work_pref[sh.nscn];
     int w0, w1;
@@ -1985,10 +1997,9 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
         G2PCand pre = {};
         if (staged) {
             const PBuf& B = Z.B;
-            int d = 0;  // range of candidate k, carried as k grows (bounded by 8: rpref[9] = ncand > k)
             for (int k = tid; k < ncand; k += NCELL) {
-                while (sm.d.rpref[d + 1] <= k) ++d;
-                const int src = sm.d.rstart[d] + (k - sm.d.rpref[d]);
+                int r;
+                const int src = cand_to_index(k, sm.d, r);
                 cpa::copy8(&sm.st.f[k], B.f + src);
                 cpa::copy8(&sm.st.v[k], B.v + src);
                 cpa::copy4(&sm.st.cell[k], B.cell + src);
@@ -2206,10 +2217,15 @@ __global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const 
     if (pend_tt >= 0) g2p_activate(sm.z, pend_tt);  // the last tile's
 }
 
+__global__ void __launch_bounds__(NCELL, G2P_MIN_BLOCKS) k_g2p(Shared sh, const double* __restrict__ z64) {
+    __shared__ G2PSmem sm;
+    g2p_body(sh, z64, sm);
+}
+
 // K5: end of the step for every running scenario (the per-step reductions
 // of G2P into dt, time and the remesh box), then the next step's dt, stop
 // rules and work list. One CTA, after G2P.
-__global__ void k_end(Shared sh) {
+__device__ __forceinline__ void end_body(const Shared& sh) {
     for (int s = threadIdx.x; s < sh.nscn; s += blockDim.x) {
         const Scn& S = sh.scn[s];
         Ctl* c = S.ctl;
@@ -2222,6 +2238,93 @@ __global__ void k_end(Shared sh) {
     }
     __syncthreads();
     begin_scenarios(sh, 0);
+}
+
+__global__ void k_end(Shared sh) { end_body(sh); }
+
+// ------------------------------------------------------- persistent steps
+
+// Barrier of the persistent step kernel: one cooperative launch, every CTA
+// resident. Thread 0 of each CTA arrives on the counter; the last arrival
+// resets it and advances the generation; the others wait for the generation
+// to change -- at most `limit` clock cycles, after which the CTA records
+// ERR_TIMEOUT in every scenario's control block and leaves the kernel. A CTA
+// that left never arrives again, so every later wait of the launch runs out
+// too: the launch always ends, and no phase runs on inputs that a phase
+// before it did not finish (a phase starts only when every CTA arrived).
+// The engine is then dead: its later persistent launches return at once.
+struct GridBar {
+    unsigned count;
+    unsigned gen;
+    int dead;  // a wait ran out: this engine's step state is incomplete, later launches do nothing
+    int pad_;
+};
+
+__device__ __forceinline__ bool grid_sync(const Shared& sh, GridBar* bar, long long limit) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned* vgen = &bar->gen;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
+            *reinterpret_cast<volatile unsigned*>(&bar->count) = 0u;
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (*vgen == g) {
+                if (clock64() - t0 > limit) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            if (!ok) {
+                atomicExch(&bar->dead, 1);
+                for (int s = 0; s < sh.nscn; ++s) atomicOr(&sh.scn[s].ctl->err, ERR_TIMEOUT);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Shared memory of the persistent kernel: the largest phase's, reused by
+// every phase (each phase initialises what it reads).
+constexpr size_t PERSIST_SMEM = sizeof(P2CSmem) > sizeof(P2SSmem) ? (sizeof(P2CSmem) > sizeof(G2PSmem) ? sizeof(P2CSmem) : sizeof(G2PSmem))
+                                                                  : (sizeof(P2SSmem) > sizeof(G2PSmem) ? sizeof(P2SSmem) : sizeof(G2PSmem));
+
+// Up to nsteps whole steps (K1 tile bookkeeping, K2 both P2G classes, K3 grid
+// update, K4 G2P, K5 end of step) in one launch, the phases separated by
+// grid_sync instead of kernel boundaries. The same phase bodies as the
+// separate kernels, over the same work lists and in the same per-tile order,
+// so a step gives the same bits either way. The launch ends early once no
+// scenario has work (every one stopped at its frame, step budget or end).
+__global__ void __launch_bounds__(NCELL, P2C_MIN_BLOCKS) k_persist(Shared sh, const double* __restrict__ z64, int nsteps, long long limit,
+                                                                   GridBar* bar) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // after a launch whose waits ran out, the tile bookkeeping of the step it
+    // left is half done: no phase may run on it again
+    if (*reinterpret_cast<volatile const int*>(&bar->dead)) return;
+    for (int s = 0; s < nsteps; ++s) {
+        prep_body(sh);
+        if (!grid_sync(sh, bar, limit)) return;
+        p2g_cell_body<false>(sh, 0, smem_raw);
+        __syncthreads();  // the shared memory passes to the next phase
+        p2g_sparse_body(sh, 1, smem_raw);
+        if (!grid_sync(sh, bar, limit)) return;
+        grid_body(sh);
+        if (!grid_sync(sh, bar, limit)) return;
+        g2p_body(sh, z64, *reinterpret_cast<G2PSmem*>(smem_raw));
+        if (!grid_sync(sh, bar, limit)) return;
+        if (blockIdx.x == 0) end_body(sh);
+        if (!grid_sync(sh, bar, limit)) return;
+        if (*reinterpret_cast<volatile const int*>(sh.work_pref + sh.nscn) == 0) break;  // the same value in every CTA
+    }
 }
 
 // Particle z and vz at the current positions (for downloads between output

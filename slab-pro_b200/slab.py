@@ -201,6 +201,13 @@ class Slab:
     def set_stream(self, stream_handle: int):
         self._check(self.L.slab_set_stream(self.h, C.c_void_p(stream_handle)))
 
+    def set_persistent(self, on: bool = True, limit_cycles: int = 0):
+        """FP32_SPLIT: run each chunk of steps as one persistent cooperative
+        launch (bitwise the same results); barrier waits give up after
+        limit_cycles SM clocks (0: the current limit)."""
+        self.L.slab_set_persistent.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
+        self._check(self.L.slab_set_persistent(self.h, int(bool(on)), int(limit_cycles)))
+
     def upload(self, P: dict):
         n = len(P["h"])
         arrs = [np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "v", "vz", "h", "A", "mass", "z")]
@@ -399,6 +406,13 @@ class Batch:
         self._check(self.L.slab_batch_add(self.h, C.byref(prm), n, *[_dp(a) for a in arrs], C.byref(sid)))
         self.Np.append(n)
         return sid.value
+
+    def set_persistent(self, on: bool = True, limit_cycles: int = 0):
+        """Run each chunk of steps as one persistent cooperative launch
+        (bitwise the same results as separate kernels); barrier waits give up
+        after limit_cycles SM clocks (0: the current limit)."""
+        self.L.slab_batch_set_persistent.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
+        self._check(self.L.slab_batch_set_persistent(self.h, int(bool(on)), int(limit_cycles)))
 
     def add_release(self, cfg: dict, rel: dict) -> int:
         """A scenario whose particles are built on the device from a release."""
