@@ -1104,6 +1104,32 @@ __device__ __forceinline__ int cand_range(int k, const TileDesc& D, int& off) {
 }
 
 constexpr int P2C_TMA_MIN_BLOCKS = NCELL == 64 ? 6 : 2;  // the stage doubles the shared memory of a CTA
+
+// 8x8 tiles: a staged candidate's entry in sm.lc packs its local cell (6
+// bits) and its rank among the same cell's candidates in its warp's block
+// (the rest, up to 511 > P2C_CAP / 2), so the placement needs no warp votes.
+constexpr bool P2C_PACKED = NCELL == 64;
+
+// Count one chunk of a warp's candidates per cell: lanes of one cell are
+// grouped by __match_any_sync, the group's first lane adds the group to the
+// (warp, cell) count; returns each lane's rank among its cell's candidates
+// so far in this warp (lc < 0: not in the tile, rank 0).
+__device__ __forceinline__ int p2c_count(int (&wcur)[P2C_WARPS][NCELL], int warp, int lane, int lc) {
+    const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
+    int rank = 0;
+    if (lc >= 0) {
+        const unsigned peers = __match_any_sync(vm, lc);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (lane == leader) {
+            base = wcur[warp][lc];
+            wcur[warp][lc] = base + __popc(peers);
+        }
+        rank = __shfl_sync(peers, base, leader) + __popc(peers & ((1u << lane) - 1u));
+    }
+    __syncwarp();
+    return rank;
+}
 // one candidate of phase 1: its range, cell and the quantities to stage
 struct P2CCand {
     int d;
@@ -1251,14 +1277,9 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
                         int off;
                         if (cand_range(k, sm.d, off) == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
                     }
-                    sm.lc[k] = (int16_t)lc;
                 }
-                const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
-                if (lc >= 0) {
-                    const unsigned peers = __match_any_sync(vm, lc);
-                    if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
-                }
-                __syncwarp();
+                const int rank = p2c_count(sm.wcur, warp, lane, lc);
+                if (k < k_hi) sm.lc[k] = (int16_t)(lc < 0 ? -1 : (P2C_PACKED ? (rank << 6) | lc : lc));
             }
         } else {
             P2CCand nx;
@@ -1272,21 +1293,14 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
                     const int ci = cell_i(q.cell) - ti * TILE, cj = cell_j(q.cell) - tj * TILE;
                     if ((unsigned)ci < TILE && (unsigned)cj < TILE) lc = ci * TILE + cj;
                     else if (q.d == 4) atomicOr(&ctl->err, ERR_MOVE);  // a stayer outside its tile
-                    if (staged) {
-                        sm.lc[k] = (int16_t)lc;
-                        if (lc >= 0) {
-                            sm.st.sa[k] = make_float4(q.f.x, q.f.y, q.m, q.h);
-                            sm.st.sv[k] = q.v;
-                            sm.st.svz[k] = q.vz;
-                        }
+                    if (staged && lc >= 0) {
+                        sm.st.sa[k] = make_float4(q.f.x, q.f.y, q.m, q.h);
+                        sm.st.sv[k] = q.v;
+                        sm.st.svz[k] = q.vz;
                     }
                 }
-                const unsigned vm = __ballot_sync(0xffffffffu, lc >= 0);
-                if (lc >= 0) {
-                    const unsigned peers = __match_any_sync(vm, lc);
-                    if ((peers & lt) == 0) sm.wcur[warp][lc] += __popc(peers);
-                }
-                __syncwarp();
+                const int rank = p2c_count(sm.wcur, warp, lane, lc);
+                if (staged && q.valid) sm.lc[k] = (int16_t)(lc < 0 ? -1 : (P2C_PACKED ? (rank << 6) | lc : lc));
             }
         }
         if constexpr (TMA) {
@@ -1314,8 +1328,18 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
         for (int q = 0; q < P2C_WARPS; ++q) sm.wcur[q][tid] += c0;
         __syncthreads();
         SLAB_PHASE_MARK(2);
-        // 3. stable placement by cell
+        // 3. stable placement by cell: (warp, cell) cursor + rank
         int32_t* order = sm.nxt_cell + sm.d.nxt_off;
+        if (P2C_PACKED && staged) {
+            for (int k = k_lo + lane; k < k_hi; k += 32) {
+                const int e = sm.lc[k];
+                if (e >= 0) {
+                    const int pos = sm.wcur[warp][e & 63] + (e >> 6);
+                    if (pos >= total) atomicOr(&ctl->err, ERR_CAPACITY);
+                    else sm.idx[pos] = (int16_t)k;
+                }
+            }
+        } else
         for (int k0 = k_lo; k0 < k_hi; k0 += 32) {
             const int k = k0 + lane;
             int lc = -1, src = 0;
