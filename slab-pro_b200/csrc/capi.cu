@@ -2,6 +2,7 @@
 // argument checks, the host side of the step loop (arming the device control
 // block, replaying step graphs until a frame), and error translation.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -290,10 +291,18 @@ slab_status slab_upload_particles(slab_ctx* c, int32_t Np, const double* x, cons
         need(c->have_params, SLAB_E_STATE, "slab_set_params first");
         need(Np > 0, SLAB_E_ARG, "Np must be > 0");
         need(x && v && vz && h && A && m && z, SLAB_E_ARG, "null particle array");
-        for (int q = 0; q < Np; ++q) {
-            need(std::isfinite(x[2 * q]) && std::isfinite(x[2 * q + 1]), SLAB_E_ARG, "non-finite particle position");
-            need(h[q] > 0 && m[q] > 0, SLAB_E_ARG, "particle h and mass must be > 0");
-        }
+        std::atomic<int> bad_x{0}, bad_hm{0};
+        parallel_ranges(Np, [&](int64_t b, int64_t e) {
+            bool fx = false, fhm = false;
+            for (int64_t q = b; q < e; ++q) {
+                fx |= !(std::isfinite(x[2 * q]) && std::isfinite(x[2 * q + 1]));
+                fhm |= !(h[q] > 0 && m[q] > 0);
+            }
+            if (fx) bad_x = 1;
+            if (fhm) bad_hm = 1;
+        });
+        need(!bad_x, SLAB_E_ARG, "non-finite particle position");
+        need(!bad_hm, SLAB_E_ARG, "particle h and mass must be > 0");
         upload_arrays(c, Np, x, v, vz, h, A, m, z);
     });
 }

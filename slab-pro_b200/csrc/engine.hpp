@@ -4,10 +4,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <functional>
 #include <map>
 #include <memory>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -73,6 +75,25 @@ struct Carve {
         return at;
     }
 };
+
+// Runs f(begin, end) over [0, n) in up to 8 host threads (one for small n):
+// for per-particle host work on millions of particles (input checks).
+template <typename F> void parallel_ranges(int64_t n, F f) {
+    const int64_t min_chunk = 1 << 18;
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(hw, n / min_chunk));
+    if (nt <= 1) {
+        f((int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const int64_t per = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; ++t) {
+        const int64_t b = t * per, e = std::min(n, b + per);
+        if (b < e) th.emplace_back([=] { f(b, e); });
+    }
+    for (auto& x : th) x.join();
+}
 
 // A grid download with no field pointer set only reports the box.
 inline bool grid_view_wants_fields(const slab_grid_view& g) { return g.h || g.mass || g.v || g.vz || g.flip || g.F || g.a; }

@@ -80,6 +80,20 @@ __global__ void k_gather_nodes(const int32_t* __restrict__ blk_of, const int32_t
     }
 }
 
+// The whole-terrain max maps in FP64 (zero where the scenario's blocks never
+// reached), for a download straight into page-locked caller memory.
+__global__ void k_max_full(const int32_t* __restrict__ blk_of, int TY, int Nx, int Ny, const float* __restrict__ hmax,
+                           const float* __restrict__ vmax2, double* __restrict__ oh, double* __restrict__ ov) {
+    const int64_t total = (int64_t)Nx * Ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k / Ny), j = (int)(k % Ny);
+        const int blk = blk_of[(i / TILE) * TY + (j / TILE)];
+        const size_t n = (size_t)blk * NCELL + (i % TILE) * TILE + (j % TILE);
+        oh[k] = blk >= 0 ? (double)hmax[n] : 0.0;
+        ov[k] = blk >= 0 ? (double)vmax2[n] : 0.0;
+    }
+}
+
 // Frame packing (slab_frame_capture). Particle k of the buffer goes to vertex
 // id[k]: x y vx vy vz z h A as float32 (the PLY vertex layout), A = m / (h rho).
 __global__ void k_pack_particles(PBuf B, int Np, double dx, double rho, float* __restrict__ out) {
@@ -993,12 +1007,36 @@ void Engine32::download_grid(int sid, slab_grid_view* gv) {
     }
 }
 
+namespace {
+bool page_locked(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+}  // namespace
+
 void Engine32::download_max(int sid, double* hmax, double* vmax2) {
+    const size_t nn = (size_t)T.Nx * T.Ny;
+    if (hmax && vmax2 && page_locked(hmax) && page_locked(vmax2)) {
+        // page-locked destinations: the whole maps are built on the device and
+        // each is one copy at full link speed (a host-side zero fill of the
+        // untouched nodes would run at host memory speed instead)
+        double* buf = reinterpret_cast<double*>(scratch.get(2 * nn * sizeof(double)));
+        const int blocks = (int)std::min<int64_t>(((int64_t)nn + 255) / 256, 148 * 16);
+        k32::k_max_full<<<blocks, 256, 0, st>>>((*slots[sid]).blk_of.get(), TY, T.Nx, T.Ny, d_hmax.get(), d_vmax2.get(), buf, buf + nn);
+        SLAB_CUDA(cudaGetLastError());
+        d2h(hmax, buf, nn, st);
+        d2h(vmax2, buf + nn, nn, st);
+        SLAB_CUDA(cudaStreamSynchronize(st));
+        return;
+    }
     // nodes outside the box of the scenario's node blocks were never updated:
     // zero; only the box is gathered on the device and copied back
     int box[4];
     box_of_blocks(sid, box);
-    const size_t nn = (size_t)T.Nx * T.Ny;
     zero_fill(hmax, nn);
     zero_fill(vmax2, nn);
     const int nI = box[1] - box[0] + 1, nJ = box[3] - box[2] + 1;

@@ -142,3 +142,26 @@ def test_tma_staged_p2g_equals_load_path(name, monkeypatch):
     for k in P1:
         assert np.array_equal(P1[k], P2[k]), k
     assert np.array_equal(h1, h2) and np.array_equal(v1, v2)
+
+
+@pytest.mark.parametrize("name", ["slope35", "fractal_mui"])
+def test_downloads_into_pinned_buffers_equal_pageable(name):
+    """Particle and max-map downloads into caller-owned page-locked arrays
+    (the max maps are then built whole on the device) give the same values
+    as downloads into pageable numpy arrays."""
+    torch = pytest.importorskip("torch")
+    c = cases.CASES[name]()
+    s = _gpu(c)
+    s.initial_pass()
+    s.advance_to_frame()
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    n = s.Np
+    ob = {k: pin(2 * n if k in ("x", "v") else n) for k in ("x", "v", "vz", "h", "A", "mass", "z")}
+    Pp, Pa = s.particles(out=ob), s.particles()
+    for k in Pa:
+        assert np.array_equal(Pp[k], Pa[k]), k
+    nn = s.Nx * s.Ny
+    (hp, vp), (ha, va) = s.max_maps(out=(pin(nn), pin(nn))), s.max_maps()
+    assert np.array_equal(hp, ha) and np.array_equal(vp, va)
+    assert (ha > 0).any()
+    s.close()
