@@ -835,6 +835,7 @@ struct P2CSmem {
         int16_t idx[P2C_CAP];    // phases 3-4: sorted position -> candidate index
     };
     float4 dem[(TILE + 1) * (TILE + 1)];
+    alignas(8) uint64_t dem_bar;  // completion of the terrain window's bulk copies (k_p2g_cell<false>)
     int wcur[P2C_WARPS][NCELL];  // per-warp cell counts, then per-warp write cursors
     int s_warp[33];
     TileDesc d;
@@ -1156,10 +1157,13 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
         sm.csid = -1;
         if constexpr (TMA) {
             tma::mbar_init(&sm.bar, 1);
-            tma::fence_mbar_init();
+        } else {
+            tma::mbar_init(&sm.dem_bar, 1);
         }
+        tma::fence_mbar_init();
     }
     __syncthreads();
+    uint32_t dem_phase = 0;  // parity of the terrain window's next completion
     if constexpr (TMA) {
         if (tid == 0 && i0 < i1) {  // the first tile's copies
             p2c_load_scenario(sm, sh, sm.d.sid);
@@ -1187,6 +1191,7 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
         const int ti = t / sh.TY, tj = t % sh.TY;
         const bool outs = sm.outs != 0;
         Ctl* const ctl = sm.ctl;
+        const bool dem_in = ti * TILE + TILE < sh.Nx && tj * TILE + TILE < sh.Ny;  // the whole window inside the terrain
         float4* dem;
         bool from_stage = false;
         if constexpr (TMA) {
@@ -1200,11 +1205,23 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
                     dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
                 }
         } else {
-            dem = sm.dem;  // asynchronous copies, completed with the candidates' before phase 4
-            for (int k = tid; k < DEM_W * DEM_W; k += P2C_THREADS) {
-                const int i = ti * TILE + k / DEM_W, j = tj * TILE + k % DEM_W;
-                if (i < sh.Nx && j < sh.Ny) cpa::copy16(&dem[k], sh.dem + (int64_t)i * sh.Ny + j);
-                else dem[k] = make_float4(0.f, 0.f, 1.f, 0.f);
+            // the terrain window: inside the terrain its 9 rows are bulk copies (TMA)
+            // issued by one thread; at the terrain's far edges per-thread copies
+            // and the fill value. Completed before phase 4.
+            dem = sm.dem;
+            if (dem_in) {
+                if (tid == 0) {
+                    tma::fence_proxy_async();  // the previous tile's reads of the window come first
+                    tma::mbar_arrive_expect_tx(&sm.dem_bar, DEM_W * DEM_W * 16);
+                    for (int r = 0; r < DEM_W; ++r)
+                        tma::bulk_g2s(&dem[r * DEM_W], sh.dem + (int64_t)(ti * TILE + r) * sh.Ny + tj * TILE, DEM_W * 16, &sm.dem_bar);
+                }
+            } else {
+                for (int k = tid; k < DEM_W * DEM_W; k += P2C_THREADS) {
+                    const int i = ti * TILE + k / DEM_W, j = tj * TILE + k % DEM_W;
+                    if (i < sh.Nx && j < sh.Ny) cpa::copy16(&dem[k], sh.dem + (int64_t)i * sh.Ny + j);
+                    else dem[k] = make_float4(0.f, 0.f, 1.f, 0.f);
+                }
             }
         }
         const int ncand = sm.d.rpref[9];
@@ -1307,6 +1324,10 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
             if (tid < DESC_WORDS) reinterpret_cast<int*>(&sm.dnext)[tid] = dn;
         } else {
             cpa::wait_all();  // the terrain window of an unstaged tile
+            if (dem_in) {  // uniform: every thread waits for the window's bulk copies
+                if (!tma::mbar_wait(&sm.dem_bar, dem_phase)) atomicOr(&ctl->err, ERR_TIMEOUT);
+                dem_phase ^= 1u;
+            }
         }
         __syncthreads();
         if constexpr (TMA) {
@@ -1389,6 +1410,11 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
         SLAB_PHASE_TILE();
     }
     SLAB_PHASE_MARK(6);
+    __syncthreads();
+    if (tid == 0) {  // every copy was waited for; the memory may serve another purpose next
+        if constexpr (TMA) tma::mbar_inval(&sm.bar);
+        else tma::mbar_inval(&sm.dem_bar);
+    }
 }
 
 template <bool TMA>
@@ -2034,6 +2060,10 @@ __device__ __forceinline__ void g2p_body(const Shared& sh, const double* __restr
         } else {
             pre = load_g2p_cand(sm.d, Z.B, tid, ncand, t, sh.TY);
         }
+        // the node window by per-thread asynchronous copies; a part whose grid tile
+        // has no block this step (or past the terrain edge) is zero. (Bulk copies
+        // of the blocks' rows, issued by warp 0 on an mbarrier, gave the same
+        // bits but made the kernel 6 % slower.)
         for (int k = tid; k < TN * TN; k += NCELL) {
             const int a = k / TN, b = k % TN;
             const int i = ti * TILE + a, j = tj * TILE + b;
