@@ -2,6 +2,8 @@
 // scenarios on a shared terrain and launches their steps together.
 #pragma once
 
+#include <cuda.h>
+
 #include <string>
 
 #include <deque>
@@ -41,6 +43,7 @@ class Engine32 {
     void launch_kernel(int k, const Shared& sh);
     void launch_p2g(const Shared& sh);
     void launch_p2g_cell(const Shared& sh, int cls);
+    CUtensorMap dem_map;   // the FP32 terrain as [Nx][4 Ny] floats, 9 x 9-node boxes (the cell P2G's terrain window)
     bool p2g_tma = false;  // k_p2g_cell<true>: the next tile's loads staged by TMA bulk copies (SLAB_P2G_TMA=1)
     // persistent steps: a chunk of steps as one cooperative launch of k_persist
     // (SLAB_PERSIST=1 or set_persistent); its grid waits give up after

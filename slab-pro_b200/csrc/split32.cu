@@ -197,6 +197,25 @@ void Engine32::pack_frame(int sid, float* d_part, float* d_grid, const int32_t b
     SLAB_CUDA(cudaGetLastError());
 }
 
+namespace {
+// cuTensorMapEncodeTiled, found through the runtime (no link to the driver library)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled() {
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+}  // namespace
+
 Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_cap, bool batch)
     : T(t), st(s), max_scn(max_scn), batch(batch) {
     TX = (t.Nx + TILE - 1) / TILE;
@@ -234,6 +253,22 @@ Engine32::Engine32(const Terrain& t, cudaStream_t s, int max_scn, int64_t blk_ca
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_cell<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2CSmem)));
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_cell<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(k32::P2CSmemTma)));
     if (const char* e = std::getenv("SLAB_P2G_TMA")) p2g_tma = std::atoi(e) != 0;
+    {
+        // the terrain window of the cell P2G as one tensor copy per tile: the
+        // float4 terrain seen as [Nx][4 Ny] floats (rows 16 Ny bytes apart), boxes
+        // of (TILE + 1) nodes by 4 (TILE + 1) floats (a multiple of 16 bytes);
+        // boxes past the far edges read zeros
+        const EncodeTiled enc = encode_tiled();
+        if (!enc) throw Error{SLAB_E_CUDA, "cuTensorMapEncodeTiled is not available"};
+        const cuuint64_t dims[2] = {(cuuint64_t)4 * T.Ny, (cuuint64_t)T.Nx};
+        const cuuint64_t strides[1] = {(cuuint64_t)T.Ny * sizeof(float4)};
+        const cuuint32_t box[2] = {4 * (TILE + 1), TILE + 1};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = enc(&dem_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)T.dem32.get(), dims, strides, box, estr,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) throw Error{SLAB_E_CUDA, "cuTensorMapEncodeTiled failed for the terrain (code " + std::to_string((int)r) + ")"};
+    }
     SLAB_CUDA(cudaFuncSetAttribute(k32::k_p2g_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(k32::P2W_WARPS * sizeof(k32::P2WWarp))));
     if (const char* e = std::getenv("SLAB_P2G_ACC")) acc_mode = std::atoi(e);
@@ -599,9 +634,9 @@ void Engine32::launch_t0() {
 // bulk copies (same sums, in the same order)
 void Engine32::launch_p2g_cell(const Shared& sh, int cls) {
     if (p2g_tma)
-        k32::k_p2g_cell<true><<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmemTma), st>>>(sh, cls);
+        k32::k_p2g_cell<true><<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmemTma), st>>>(sh, cls, dem_map);
     else
-        k32::k_p2g_cell<false><<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, cls);
+        k32::k_p2g_cell<false><<<grid_p2g_cell, k32::P2C_THREADS, sizeof(k32::P2CSmem), st>>>(sh, cls, dem_map);
 }
 
 void Engine32::launch_p2g(const Shared& sh) {
@@ -643,6 +678,7 @@ void Engine32::launch_step() {
 }
 
 constexpr int Engine32::Tuner::FACTOR4[];
+
 
 namespace {
 // Launch shapes picked for single scenarios, by device, tile count and
@@ -767,7 +803,7 @@ void Engine32::launch_persistent(int chunk) {
     int n = chunk;
     long long lim = persist_limit;
     k32::GridBar* bar = reinterpret_cast<k32::GridBar*>(d_bar.get());
-    void* args[] = {&sh, &z64, &n, &lim, &bar};
+    void* args[] = {&sh, &z64, &n, &lim, &bar, &dem_map};
     SLAB_CUDA(cudaLaunchCooperativeKernel((const void*)k32::k_persist, dim3(grid_persist), dim3(NCELL), args, k32::PERSIST_SMEM, st));
     nlaunch += 1;
 }

@@ -439,7 +439,7 @@ __device__ __forceinline__ PQ load_pq(const PBuf& B, int src, int li, int lj, co
 // contributions; the window is converted back and written as the partials.
 template <int ACC>
 __global__ void __launch_bounds__(P2G_THREADS, P2G_MIN_BLOCKS) k_p2g(Shared sh, int cls) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31;
     int i0, i1;
@@ -634,7 +634,7 @@ __device__ __forceinline__ PQ warp_pq(const Shared& sh, const PBuf& B, const Til
 // and the scale is the largest power of two that keeps that below 2^30; the
 // hi word is the rounded contribution, the lo word the rest at 2^-20.
 __global__ void __launch_bounds__(P2W_THREADS, 3) k_p2g_warp(Shared sh, int cls) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     P2WWarp& sw = reinterpret_cast<P2WWarp*>(smem_raw)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * P2W_WARPS + (threadIdx.x >> 5), nw = gridDim.x * P2W_WARPS;
@@ -834,8 +834,8 @@ struct P2CSmem {
         int32_t ccell[P2C_CAP];  // phase 1: cell of each staged candidate
         int16_t idx[P2C_CAP];    // phases 3-4: sorted position -> candidate index
     };
-    float4 dem[(TILE + 1) * (TILE + 1)];
-    alignas(8) uint64_t dem_bar;  // completion of the terrain window's bulk copies (k_p2g_cell<false>)
+    alignas(128) float4 dem[(TILE + 1) * (TILE + 1)];  // a tensor copy's destination: 128-byte aligned
+    alignas(8) uint64_t dem_bar;  // completion of the terrain window's tensor copy (k_p2g_cell<false>)
     int wcur[P2C_WARPS][NCELL];  // per-warp cell counts, then per-warp write cursors
     int s_warp[33];
     TileDesc d;
@@ -1141,7 +1141,7 @@ struct P2CCand {
 };
 
 template <bool TMA>
-__device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigned char* smem_raw) {
+__device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigned char* smem_raw, const CUtensorMap* dem_map) {
     using Sm = typename std::conditional<TMA, P2CSmemTma, P2CSmem>::type;
     Sm& sm = *reinterpret_cast<Sm*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1191,7 +1191,6 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
         const int ti = t / sh.TY, tj = t % sh.TY;
         const bool outs = sm.outs != 0;
         Ctl* const ctl = sm.ctl;
-        const bool dem_in = ti * TILE + TILE < sh.Nx && tj * TILE + TILE < sh.Ny;  // the whole window inside the terrain
         float4* dem;
         bool from_stage = false;
         if constexpr (TMA) {
@@ -1205,23 +1204,16 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
                     dem[k] = (i < sh.Nx && j < sh.Ny) ? sh.dem[(int64_t)i * sh.Ny + j] : make_float4(0.f, 0.f, 1.f, 0.f);
                 }
         } else {
-            // the terrain window: inside the terrain its 9 rows are bulk copies (TMA)
-            // issued by one thread; at the terrain's far edges per-thread copies
-            // and the fill value. Completed before phase 4.
+            // the terrain window: one 2-D tensor copy (TMA) of its 9 x 9 nodes,
+            // issued by one thread, completed before phase 4. The map sees the
+            // terrain as [Nx][4 Ny] floats, so x = 4 tj TILE (a multiple of 16
+            // bytes). Nodes past the terrain's far edges read as zero; no valid
+            // particle uses them (its stencil lies inside the terrain).
             dem = sm.dem;
-            if (dem_in) {
-                if (tid == 0) {
-                    tma::fence_proxy_async();  // the previous tile's reads of the window come first
-                    tma::mbar_arrive_expect_tx(&sm.dem_bar, DEM_W * DEM_W * 16);
-                    for (int r = 0; r < DEM_W; ++r)
-                        tma::bulk_g2s(&dem[r * DEM_W], sh.dem + (int64_t)(ti * TILE + r) * sh.Ny + tj * TILE, DEM_W * 16, &sm.dem_bar);
-                }
-            } else {
-                for (int k = tid; k < DEM_W * DEM_W; k += P2C_THREADS) {
-                    const int i = ti * TILE + k / DEM_W, j = tj * TILE + k % DEM_W;
-                    if (i < sh.Nx && j < sh.Ny) cpa::copy16(&dem[k], sh.dem + (int64_t)i * sh.Ny + j);
-                    else dem[k] = make_float4(0.f, 0.f, 1.f, 0.f);
-                }
+            if (tid == 0) {
+                tma::fence_proxy_async();  // the previous tile's reads of the window come first
+                tma::mbar_arrive_expect_tx(&sm.dem_bar, DEM_W * DEM_W * 16);
+                tma::tensor_g2s_2d(dem, dem_map, 4 * tj * TILE, ti * TILE, &sm.dem_bar);
             }
         }
         const int ncand = sm.d.rpref[9];
@@ -1323,11 +1315,9 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
         if constexpr (TMA) {
             if (tid < DESC_WORDS) reinterpret_cast<int*>(&sm.dnext)[tid] = dn;
         } else {
-            cpa::wait_all();  // the terrain window of an unstaged tile
-            if (dem_in) {  // uniform: every thread waits for the window's bulk copies
-                if (!tma::mbar_wait(&sm.dem_bar, dem_phase)) atomicOr(&ctl->err, ERR_TIMEOUT);
-                dem_phase ^= 1u;
-            }
+            // every thread waits for the terrain window's tensor copy
+            if (!tma::mbar_wait(&sm.dem_bar, dem_phase)) atomicOr(&ctl->err, ERR_TIMEOUT);
+            dem_phase ^= 1u;
         }
         __syncthreads();
         if constexpr (TMA) {
@@ -1418,9 +1408,10 @@ __device__ __forceinline__ void p2g_cell_body(const Shared& sh, int cls, unsigne
 }
 
 template <bool TMA>
-__global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MIN_BLOCKS) k_p2g_cell(Shared sh, int cls) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    p2g_cell_body<TMA>(sh, cls, smem_raw);
+__global__ void __launch_bounds__(P2C_THREADS, TMA ? P2C_TMA_MIN_BLOCKS : P2C_MIN_BLOCKS)
+    k_p2g_cell(Shared sh, int cls, const __grid_constant__ CUtensorMap dem_map) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    p2g_cell_body<TMA>(sh, cls, smem_raw, &dem_map);
 }
 
 // ----------------------------------------------------- P2G of sparse tiles
@@ -1651,7 +1642,7 @@ __device__ __forceinline__ void p2g_sparse_body(const Shared& sh, int cls, unsig
 }
 
 __global__ void __launch_bounds__(P2S_THREADS, P2S_MIN_BLOCKS) k_p2g_sparse(Shared sh, int cls) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     p2g_sparse_body(sh, cls, smem_raw);
 }
 
@@ -2359,15 +2350,15 @@ constexpr size_t PERSIST_SMEM = sizeof(P2CSmem) > sizeof(P2SSmem) ? (sizeof(P2CS
 // so a step gives the same bits either way. The launch ends early once no
 // scenario has work (every one stopped at its frame, step budget or end).
 __global__ void __launch_bounds__(NCELL, P2C_MIN_BLOCKS) k_persist(Shared sh, const double* __restrict__ z64, int nsteps, long long limit,
-                                                                   GridBar* bar) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+                                                                   GridBar* bar, const __grid_constant__ CUtensorMap dem_map) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     // after a launch whose waits ran out, the tile bookkeeping of the step it
     // left is half done: no phase may run on it again
     if (*reinterpret_cast<volatile const int*>(&bar->dead)) return;
     for (int s = 0; s < nsteps; ++s) {
         prep_body(sh);
         if (!grid_sync(sh, bar, limit)) return;
-        p2g_cell_body<false>(sh, 0, smem_raw);
+        p2g_cell_body<false>(sh, 0, smem_raw, &dem_map);
         __syncthreads();  // the shared memory passes to the next phase
         p2g_sparse_body(sh, 1, smem_raw);
         if (!grid_sync(sh, bar, limit)) return;

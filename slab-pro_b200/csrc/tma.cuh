@@ -10,6 +10,8 @@
 // fence_proxy_async(); every wait is bounded.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include <cstdint>
 
 namespace slab {
@@ -68,6 +70,18 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
                  "l"(src), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
+}
+
+// A box of a 2-D tensor (map built on the host by cuTensorMapEncodeTiled)
+// into shared memory (128-byte aligned), completing on bar. x is the inner
+// coordinate in elements; x times the element size must be a multiple of 16.
+// The map is a __grid_constant__ kernel parameter; no multicast.
+__device__ __forceinline__ void tensor_g2s_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
 }
 
 }  // namespace tma
