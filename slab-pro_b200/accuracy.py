@@ -1,8 +1,14 @@
-"""Accuracy measures of a run against an FP64 run of the same scenario.
+"""Accuracy measures of a run against an FP64 run of the same scenario:
+max-flow-height and max-speed maps node by node (within 1 cm or 1 %, within
+0.1 m/s or 1 %), runout, the centre-of-mass trajectory frame by frame, total
+mass.
 
-The bar the FP32 split path is held to: max-flow-height maps within 1 cm or
-1 % node by node (on at least 99.5 % of the wet nodes, never more than 5 cm
-off), runout within one grid cell, total particle mass unchanged."""
+Short runs (the GPU tests' cases, the reference's Brienz example) hold the
+FP32 split path to h_max within 1 cm or 1 % on at least 99.5 % of the wet
+nodes and runout within one grid cell. Whole runs on rough terrain are
+chaotic: there the same measures of FP64 against FP64 started from positions
+moved by 1e-7 cell (the FP64 envelope, bench.py) set the scale the FP32
+error is compared with."""
 from __future__ import annotations
 
 import numpy as np
