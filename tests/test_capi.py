@@ -5,6 +5,9 @@ import glob
 import os
 import re
 
+import numpy as np
+import pytest
+
 import slab
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -55,3 +58,16 @@ def test_null_arguments_are_rejected_without_gpu():
     assert b"NULL" in L.slab_last_error(None)  # a failed create leaves its message for slab_last_error(NULL)
     assert L.slab_set_params(None, None) == 1
     assert L.slab_advance_steps(None, 1, None) == 1
+
+
+def test_caller_output_arrays_are_checked():
+    """slab.py's caller-owned output arrays: contiguous float64 of at least
+    the needed length, else ValueError before any library call."""
+    a = np.zeros(10)
+    assert slab._out_array(a, 8).shape == (8,)
+    with pytest.raises(ValueError):
+        slab._out_array(np.zeros(10, dtype=np.float32), 8)
+    with pytest.raises(ValueError):
+        slab._out_array(np.zeros(4), 8)
+    with pytest.raises(ValueError):
+        slab._out_array(np.zeros((4, 4))[:, 0], 2)

@@ -88,3 +88,32 @@ def test_two_gloo_ranks_run_their_shares_and_gather():
     assert sorted(res) == list(range(6))  # rank 0 gathered every scenario
     assert all(res[i]["rank"] == (0 if i in shards[0] else 1) for i in res)
     assert got[1][2] is None
+
+
+def test_release_estimate_tracks_the_sampled_count():
+    """Sharding a releases-only ensemble balances on the particle count an
+    ELLIPSE / RECTANGLE release will give (4 per covered cell); it must track
+    the count the reference's UNIFORM setup produces."""
+    import workloads as W
+    z = W.fractal_slope_dem(512, 2.0, seed=5, rms=3.0, x_plane_end=600.0, ease_m=200.0)
+    rels = [
+        {"type": "ELLIPSE", "center": (300.0, 500.0), "rx": 80.0, "ry": 40.0, "rotation_deg": 30.0, "h0": 2.0},
+        {"type": "ELLIPSE", "center": (250.0, 300.0), "rx": 25.0, "ry": 60.0, "rotation_deg": 0.0, "h0": 1.0},
+        {"type": "RECTANGLE", "center": (200.0, 700.0), "Lx": 60.0, "Ly": 30.0, "rotation_deg": 10.0, "h0": 1.5},
+    ]
+    for rel in rels:
+        n = len(W.release_particles(z, 2.0, rel, 300.0)["h"])
+        est = W.release_particle_estimate(rel, 2.0)
+        assert abs(est - n) <= 0.05 * n, (rel["type"], est, n)
+
+
+def test_config4_releases_match_its_particle_scenarios():
+    """config4(particles=False) draws the same scenarios as config4(): the
+    same configurations, and releases whose estimates track the particles."""
+    import workloads as W
+    a = W.config4(6)
+    b = W.config4(6, particles=False)
+    for (ca, P), (cb, rel) in zip(a["scenarios"], b["scenarios"]):
+        assert ca == cb
+        n = len(P["h"])
+        assert abs(W.release_particle_estimate(rel, b["dx"]) - n) <= 0.02 * n
